@@ -1,0 +1,439 @@
+"""Benchmark of the plain GPU drop-ins at 4096^2 fp32.
+
+Workload of one step (the reference's headline configuration): on one
+4096 x 4096 fBm heightmap (seed 2, kw 4, 8 octaves, remapped to [0, 1])
+  * thermal: talus map (0.5 + fBm seed 3) / 4096, bedrock 0.3 z,
+    500 iterations, then the border extrapolation;
+  * vpipes: water starts at 0, rain 1e-4 per step, dt 0.1, pipe area 1,
+    gravity 9.81, k_capacity 0.05, k_erode = k_depose = 0.01, evaporation
+    0.01, no volume top-up, no flux diffusion, 1000 iterations.
+Metric: cell-updates/s = cells x (500 + 1000) per step / step time.
+
+value  : inputs resident in HBM, CUDA events on the launch stream, max over
+         ranks.
+e2e    : the same step through the host-buffer C-ABI (hm_thermal, hm_vpipes)
+         from pinned host memory: uploads and downloads inside the timing.
+roofline: the dominant kernel (vpipes, 56 algorithmic bytes per
+         cell-update) timed live with CUDA events inside the timed region.
+cpu_baseline: the reference's kernel text compiled for the CPU
+         (oracle/_ref, all host threads) on a bounded sample, scaled to the
+         same metric.
+
+Multi-GPU: the solvers do not shard (one heightmap per call); every rank
+runs an independent replica (scaling "weak"), value = all ranks' cell
+updates / max-over-ranks time.
+
+`--impl reference` times the reference's CPU implementation of the path
+(oracle/_ref) on the host cores with the same metric; under torchrun only
+rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SIDE = 4096
+THERMAL_ITERS = 500
+VPIPES_ITERS = 1000
+VPIPES_BYTES = 56.0   # algorithmic bytes per vpipes cell-update (7 fields in + out)
+THERMAL_BYTES = 16.0  # z, talus, bedrock in; z out
+CONFIG2_VPIPES = dict(maintain_water_volume=0, flux_diffusion=0, dt=0.1, k_capacity=0.05, k_erode=0.01,
+                      k_depose=0.01, evap_rate=0.01, gravity=9.81, pipe_area=1.0, pipe_length=1.0,
+                      rain_per_step=1e-4, initial_water=0.0, water_height=1e-2)
+METRIC = "cell-updates/s at 4096^2 fp32 (thermal 500 + vpipes 1000 iterations per step)"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=N_SIDE)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    return a
+
+
+def _config(n):
+    return {
+        "workload": "plain drop-ins, %dx%d fp32: thermal (talus map, bedrock 0.3 z) x%d + vpipes x%d"
+                    % (n, n, THERMAL_ITERS, VPIPES_ITERS),
+        "grid": [n, n],
+        "thermal": {"iterations": THERMAL_ITERS, "talus": "(0.5 + fbm seed 3) / nx", "bedrock": "0.3 z",
+                    "bedrock_mode": "intended"},
+        "vpipes": dict(CONFIG2_VPIPES, iterations=VPIPES_ITERS),
+        "inputs": "fBm seed 2 remapped to [0,1] (synthetic, seeded)",
+        "l2": "inputs larger than L2 (state 7 x 64 MiB for vpipes, 4 x 64 MiB for thermal)",
+        "parallelism": "replicas",
+    }
+
+
+def _inputs(n):
+    import numpy as np
+
+    from highmap_b200.inputs import fbm
+    z = fbm(n, n, seed=2)
+    talus = ((0.5 + fbm(n, n, seed=3)) / n).astype(np.float32)
+    bed = (0.3 * z).astype(np.float32)
+    return z, talus, bed
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples of the benchmark GPU during the timed region."""
+
+    Q = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9 or (self.uuid and f[0] != self.uuid):
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                smax.append(float(f[2].split()[0]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic():
+    """dram bytes per vpipes launch from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            t = json.load(f)
+        return t.get("vpipes_bytes_per_step_4096")
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------- cpu
+
+def _cpu_rates(n, budget_s=12.0, use_ref=True):
+    """Cell-update rates of the CPU implementation on a bounded sample:
+    a few thermal and vpipes iterations on the full n x n inputs."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+    z, talus, bed = _inputs(n)
+    if use_ref and po.ref_available():
+        kind, th, vp, cores = "reference", po.ref_thermal, po.ref_vpipes, None
+    else:
+        kind, th, vp, cores = "port", po.thermal, po.vpipes, None
+
+    def t_thermal(k):
+        t = time.perf_counter()
+        th(z, talus, k, bedrock=bed) if kind == "reference" else th(z, talus, k, bedrock=bed)
+        return time.perf_counter() - t
+
+    def t_vpipes(k):
+        p = po.VpipesParams.make(**dict(CONFIG2_VPIPES, iterations=k))
+        t = time.perf_counter()
+        vp(z, p)
+        return time.perf_counter() - t
+
+    # one iteration each to size the sample, then the sample itself
+    t1 = max(t_thermal(1), 1e-3)
+    v1 = max(t_vpipes(1), 1e-3)
+    kt = max(1, int(0.35 * budget_s / t1))
+    kv = max(1, int(0.65 * budget_s / v1))
+    tt = t_thermal(kt)
+    tv = t_vpipes(kv)
+    cells = float(n) * n
+    rate_t = cells * kt / tt
+    rate_v = cells * kv / tv
+    cores = po.num_threads()
+    return kind, cores, rate_t, rate_v, kt, kv, tt + tv
+
+
+def _composite(cells, rate_t, rate_v):
+    step_s = cells * THERMAL_ITERS / rate_t + cells * VPIPES_ITERS / rate_v
+    return cells * (THERMAL_ITERS + VPIPES_ITERS) / step_s
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np
+
+    from oracle import pyoracle as po
+    n = a.size
+    cells = float(n) * n
+    z, talus, bed = _inputs(n)
+    use_ref = po.ref_available()
+    kind = "reference" if use_ref else "port"
+    th = po.ref_thermal if use_ref else po.thermal
+    vp = po.ref_vpipes if use_ref else po.vpipes
+    p1 = po.VpipesParams.make(**dict(CONFIG2_VPIPES, iterations=1))
+
+    def step():
+        t0 = time.perf_counter()
+        th(z, talus, 1, bedrock=bed)
+        t1 = time.perf_counter()
+        vp(z, p1)
+        t2 = time.perf_counter()
+        return t1 - t0, t2 - t1
+
+    for _ in range(a.warmup):
+        step()
+    tt = tv = 0.0
+    for _ in range(a.steps):
+        x, y = step()
+        tt += x
+        tv += y
+    rate_t = cells * a.steps / tt
+    rate_v = cells * a.steps / tv
+    value = _composite(cells, rate_t, rate_v)
+    ms = 1e3 * cells * (THERMAL_ITERS + VPIPES_ITERS) / value
+    cores = po.num_threads()
+    sample = ("each step: 1 thermal + 1 vpipes iteration on the full %dx%d inputs, extrapolated to %d + %d "
+              "iterations" % (n, n, THERMAL_ITERS, VPIPES_ITERS))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": _config(n),
+        "per_solver": {"thermal_cell_updates_per_s": rate_t, "vpipes_cell_updates_per_s": rate_v},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- ours
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from highmap_b200 import gpu as G
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    if not G.init_opencl():
+        raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
+    ctx = G.Context(local)
+    n = a.size
+    cells = float(n) * n
+    z, talus, bed = _inputs(n)
+    dev = torch.device("cuda", local)
+    z0_d = torch.from_numpy(z).to(dev)
+    talus_d = torch.from_numpy(talus).to(dev)
+    bed_d = torch.from_numpy(bed).to(dev)
+    z_th = torch.empty_like(z0_d)
+    z_vp = torch.empty_like(z0_d)
+    pv = G.vpipes_params(**dict(CONFIG2_VPIPES, iterations=VPIPES_ITERS))
+    stream = torch.cuda.Stream(device=dev)
+
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(a.steps)]
+
+    def step(e=None):
+        if e:
+            e[0].record(stream)
+        z_th.copy_(z0_d)
+        G.thermal_device(z_th, talus_d, THERMAL_ITERS, bedrock=bed_d, ctx=ctx, stream=stream.cuda_stream)
+        if e:
+            e[1].record(stream)
+        z_vp.copy_(z0_d)
+        G.hydraulic_vpipes_device(z_vp, pv, ctx=ctx, stream=stream.cuda_stream)
+        if e:
+            e[2].record(stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            step()
+    torch.cuda.synchronize()
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        if not uuid.startswith("GPU-"):
+            uuid = "GPU-" + uuid
+    except Exception:
+        uuid = None
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.5)
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    G.launch_count_reset()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        t_start.record(stream)
+        for k in range(a.steps):
+            step(ev[k])
+        t_end.record(stream)
+    torch.cuda.synchronize()
+    launches = G.launch_count()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+
+    elapsed_ms = t_start.elapsed_time(t_end)
+    th_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    vp_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
+    if world > 1:
+        t = torch.tensor([elapsed_ms, th_ms, vp_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms, th_ms, vp_ms = [float(x) for x in t.tolist()]
+
+    total_updates = world * a.steps * cells * (THERMAL_ITERS + VPIPES_ITERS)
+    value = total_updates / (elapsed_ms * 1e-3)
+    ms_per_step = elapsed_ms / a.steps
+
+    peak, peak_kind = _peaks()
+    vp_step_s = vp_ms * 1e-3 / (a.steps * VPIPES_ITERS)
+    th_step_s = th_ms * 1e-3 / (a.steps * THERMAL_ITERS)
+    achieved = VPIPES_BYTES * cells / vp_step_s / 1e9
+    th_achieved = THERMAL_BYTES * cells / th_step_s / 1e9
+    traffic = _traffic()
+
+    # e2e through the host-buffer C-ABI, pinned host memory
+    e2e = None
+    if not a.no_e2e:
+        zp = torch.empty((n, n), dtype=torch.float32, pin_memory=True).numpy()
+        tp = torch.empty((n, n), dtype=torch.float32, pin_memory=True).numpy()
+        bp = torch.empty((n, n), dtype=torch.float32, pin_memory=True).numpy()
+        tp[...] = talus
+        bp[...] = bed
+        vkw = dict(CONFIG2_VPIPES)
+
+        def e2e_step():
+            zp[...] = z
+            t0 = time.perf_counter()
+            G.thermal(zp, tp, THERMAL_ITERS, bedrock=bp, ctx=ctx)
+            t1 = time.perf_counter()
+            zp[...] = z
+            t2 = time.perf_counter()
+            G.hydraulic_vpipes(zp, iterations=VPIPES_ITERS, ctx=ctx, **vkw)
+            t3 = time.perf_counter()
+            return (t1 - t0) + (t3 - t2)
+
+        for _ in range(a.warmup):
+            e2e_step()
+        if world > 1:
+            dist.barrier()
+        tot = sum(e2e_step() for _ in range(a.steps))
+        if world > 1:
+            t = torch.tensor([tot], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot = float(t.item())
+        e2e = {"value": world * a.steps * cells * (THERMAL_ITERS + VPIPES_ITERS) / tot, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": int(4 * cells * 4), "d2h_bytes_per_step": int(2 * cells * 4),
+               "ms_per_step": 1e3 * tot / a.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        kind, cores, rt, rv, kt, kv, secs = _cpu_rates(n)
+        cpu = {"value": _composite(cells, rt, rv), "unit": "cell-updates/s", "cores": cores, "kind": kind,
+               "sample": "%d thermal + %d vpipes iterations on the full %dx%d inputs (%.1f s of CPU time), "
+                         "scaled to %d + %d iterations" % (kt, kv, n, n, secs, THERMAL_ITERS, VPIPES_ITERS),
+               "thermal_cell_updates_per_s": rt, "vpipes_cell_updates_per_s": rv}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": _config(n),
+            "per_solver": {
+                "thermal_cell_updates_per_s": world * a.steps * cells * THERMAL_ITERS / (th_ms * 1e-3),
+                "vpipes_cell_updates_per_s": world * a.steps * cells * VPIPES_ITERS / (vp_ms * 1e-3),
+                "thermal_roofline": {"bound": "hbm", "achieved": th_achieved, "peak": peak, "unit": "GB/s",
+                                     "frac": th_achieved / peak, "bytes_per_cell_update": THERMAL_BYTES},
+            },
+            "roofline": {"bound": "hbm", "kernel": "vpipes step", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "bytes_per_cell_update": VPIPES_BYTES},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,117 @@
+"""Loader of libhm_erosion.so and its ctypes signatures.
+
+The library is the only compute path: if it is missing or cannot load,
+every call raises; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libhm_erosion.so")
+
+HM_OK = 0
+HM_ERR_INVALID_ARGUMENT = 1
+HM_ERR_NO_DEVICE = 2
+HM_ERR_OUT_OF_MEMORY = 3
+HM_ERR_CUDA = 4
+HM_ERR_TIMEOUT = 5
+HM_ERR_BUSY = 6
+
+HM_BEDROCK_INTENDED = 0
+HM_BEDROCK_LITERAL = 1
+
+# every symbol include/hm_erosion.h declares (checked by the CPU tests)
+EXPORTED = (
+    "hm_init", "hm_context_create", "hm_context_destroy", "hm_context_trim",
+    "hm_status_string", "hm_last_error", "hm_thermal_default_options",
+    "hm_thermal", "hm_thermal_scalar", "hm_thermal_masked", "hm_thermal_device",
+    "hm_vpipes_default_params", "hm_vpipes", "hm_vpipes_device",
+    "hm_launch_count", "hm_launch_count_reset",
+)
+
+
+class HMError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__("%s (status %d)" % (message, status))
+        self.status = status
+
+
+class ThermalOptions(C.Structure):
+    _fields_ = [("bedrock_mode", C.c_int), ("time_block", C.c_int)]
+
+
+class VpipesParams(C.Structure):
+    """hm_vpipes_params: the reference's hydraulic_vpipes parameters
+    (HighMap/include/highmap/erosion.hpp:1206-1223) and the extensions."""
+
+    _fields_ = [
+        ("water_height", C.c_float),
+        ("maintain_water_volume", C.c_int),
+        ("evap_rate", C.c_float),
+        ("iterations", C.c_int),
+        ("dt", C.c_float),
+        ("k_capacity", C.c_float),
+        ("k_erode", C.c_float),
+        ("k_depose", C.c_float),
+        ("k_discharge_exp", C.c_float),
+        ("downcutting_max_depth_ratio", C.c_float),
+        ("flux_diffusion", C.c_int),
+        ("flux_diffusion_strength", C.c_float),
+        ("gravity", C.c_float),
+        ("pipe_length", C.c_float),
+        ("pipe_area", C.c_float),
+        ("rain_per_step", C.c_float),
+        ("initial_water", C.c_float),
+    ]
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _declare(lib):
+    vp = C.c_void_p
+    i = C.c_int
+    f = C.c_float
+    lib.hm_init.restype = i
+    lib.hm_context_create.argtypes = [C.POINTER(vp), i]
+    lib.hm_context_destroy.argtypes = [vp]
+    lib.hm_context_trim.argtypes = [vp]
+    lib.hm_status_string.restype = C.c_char_p
+    lib.hm_status_string.argtypes = [i]
+    lib.hm_last_error.restype = C.c_char_p
+    lib.hm_thermal_default_options.argtypes = [vp]
+    lib.hm_thermal.argtypes = [vp, vp, i, i, vp, i, vp, vp, vp]
+    lib.hm_thermal_scalar.argtypes = [vp, vp, i, i, f, i, vp, vp, vp]
+    lib.hm_thermal_masked.argtypes = [vp, vp, i, i, vp, vp, i, vp, vp, vp]
+    lib.hm_thermal_device.argtypes = [vp, vp, i, i, vp, f, i, vp, vp, vp, vp, vp]
+    lib.hm_vpipes_default_params.argtypes = [vp]
+    lib.hm_vpipes.argtypes = [vp, vp, i, i, vp, vp, vp, vp, vp, vp]
+    lib.hm_vpipes_device.argtypes = [vp, vp, i, i, vp, vp, vp, vp, vp, vp, vp]
+    lib.hm_launch_count.restype = C.c_ulonglong
+    for name in EXPORTED:
+        getattr(lib, name)  # raises AttributeError if a symbol is missing
+    return lib
+
+
+def lib():
+    """The loaded library; raises if it is not built."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise RuntimeError(
+                        "libhm_erosion.so is not built (expected at %s); run "
+                        "`python -m highmap_b200.build`" % LIB_PATH)
+                _lib = _declare(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != HM_OK:
+        msg = lib().hm_last_error().decode(errors="replace") or lib().hm_status_string(status).decode()
+        raise HMError(status, msg)

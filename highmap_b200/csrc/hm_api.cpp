@@ -1,0 +1,175 @@
+/*
+ * hm_api.cpp - the C-ABI entry points of include/hm_erosion.h.
+ *
+ * Host-pointer calls reproduce the reference drivers' boundary
+ * (HighMap/src/erosion/thermal_gpu.cpp:30-46 uploads z, talus and bedrock,
+ * runs the steps, reads z back): one upload of each input, the whole solve
+ * on the device, one download of each output, all ordered on the context's
+ * stream and finished before the call returns.
+ */
+#include <cstring>
+
+#include "hm_internal.h"
+#include "hm_thermal.h"
+#include "hm_vpipes.h"
+
+namespace
+{
+
+using hm::align_up;
+
+struct Slab
+{
+  char  *base;
+  size_t off = 0;
+  float *take(size_t nfloats)
+  {
+    float *p = (float *)(base + off);
+    off += align_up(nfloats * sizeof(float), 256);
+    return p;
+  }
+};
+
+int thermal_host(hm_context *ctx, float *z, int nx, int ny, const float *talus, float talus_value,
+                 int iterations, const float *bedrock, float *depo, const float *mask,
+                 const hm_thermal_options *opts)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "thermal: ctx is NULL");
+  int st = hm::thermal_check_args(z, nx, ny, iterations, opts);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const size_t n = (size_t)nx * ny;
+  const size_t nbytes = n * sizeof(float);
+  const bool   need_z0 = depo || mask;
+  size_t       fields = 1 + (talus ? 1 : 0) + (bedrock ? 1 : 0) + (depo ? 1 : 0) + (mask ? 1 : 0);
+  size_t total = fields * align_up(nbytes, 256) + align_up(hm::thermal_scratch_floats(nx, ny, need_z0) * 4, 256);
+  void  *ws = nullptr;
+  if ((st = hm::workspace(ctx, total, &ws))) return st;
+  Slab         sl{(char *)ws};
+  float       *dz = sl.take(n);
+  float       *dt = talus ? sl.take(n) : nullptr;
+  float       *db = bedrock ? sl.take(n) : nullptr;
+  float       *dd = depo ? sl.take(n) : nullptr;
+  float       *dm = mask ? sl.take(n) : nullptr;
+  float       *scr = sl.take(hm::thermal_scratch_floats(nx, ny, need_z0));
+  cudaStream_t s = ctx->stream;
+  HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
+  if (dt) HM_CUDA_TRY(cudaMemcpyAsync(dt, talus, nbytes, cudaMemcpyHostToDevice, s));
+  if (db) HM_CUDA_TRY(cudaMemcpyAsync(db, bedrock, nbytes, cudaMemcpyHostToDevice, s));
+  if (dm) HM_CUDA_TRY(cudaMemcpyAsync(dm, mask, nbytes, cudaMemcpyHostToDevice, s));
+  st = hm::thermal_core(ctx->device, dz, nx, ny, dt, talus_value, iterations, db, dd, dm, opts, scr, s);
+  if (st)
+  {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  HM_CUDA_TRY(cudaMemcpyAsync(z, dz, nbytes, cudaMemcpyDeviceToHost, s));
+  if (dd) HM_CUDA_TRY(cudaMemcpyAsync(depo, dd, nbytes, cudaMemcpyDeviceToHost, s));
+  HM_CUDA_TRY(cudaStreamSynchronize(s));
+  return HM_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int hm_thermal(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
+               const float *bedrock, float *deposition_map, const hm_thermal_options *opts)
+{
+  if (!talus) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal: talus is NULL");
+  return thermal_host(ctx, z, nx, ny, talus, 0.f, iterations, bedrock, deposition_map, nullptr, opts);
+}
+
+int hm_thermal_scalar(hm_context *ctx, float *z, int nx, int ny, float talus, int iterations,
+                      const float *bedrock, float *deposition_map, const hm_thermal_options *opts)
+{
+  return thermal_host(ctx, z, nx, ny, nullptr, talus, iterations, bedrock, deposition_map, nullptr, opts);
+}
+
+int hm_thermal_masked(hm_context *ctx, float *z, int nx, int ny, const float *mask, const float *talus,
+                      int iterations, const float *bedrock, float *deposition_map,
+                      const hm_thermal_options *opts)
+{
+  if (!talus) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_masked: talus is NULL");
+  return thermal_host(ctx, z, nx, ny, talus, 0.f, iterations, bedrock, deposition_map, mask, opts);
+}
+
+int hm_thermal_device(hm_context *ctx, float *z, int nx, int ny, const float *talus, float talus_value,
+                      int iterations, const float *bedrock, float *deposition_map, const float *mask,
+                      const hm_thermal_options *opts, void *stream)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_device: ctx is NULL");
+  int st = hm::thermal_check_args(z, nx, ny, iterations, opts);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const bool need_z0 = deposition_map || mask;
+  void      *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::thermal_scratch_floats(nx, ny, need_z0) * sizeof(float), &ws))) return st;
+  return hm::thermal_core(ctx->device, z, nx, ny, talus, talus_value, iterations, bedrock, deposition_map, mask,
+                          opts, (float *)ws, (cudaStream_t)stream);
+}
+
+int hm_vpipes(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_params *params, const float *rain_map,
+              float *water_depth, float *sediment, float *vel_u, float *vel_v)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes: ctx is NULL");
+  hm_vpipes_params p;
+  hm_vpipes_default_params(&p);
+  if (params) p = *params;
+  int st = hm::vpipes_check_args(z, nx, ny, &p);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const size_t n = (size_t)nx * ny;
+  const size_t nbytes = n * sizeof(float);
+  size_t       fields = 1 + (rain_map ? 1 : 0) + (water_depth ? 1 : 0) + (sediment ? 1 : 0) + (vel_u ? 1 : 0) +
+                  (vel_v ? 1 : 0);
+  size_t total = fields * align_up(nbytes, 256) + align_up(hm::vpipes_scratch_bytes(nx, ny), 256);
+  void  *ws = nullptr;
+  if ((st = hm::workspace(ctx, total, &ws))) return st;
+  Slab         sl{(char *)ws};
+  float       *dz = sl.take(n);
+  float       *dr = rain_map ? sl.take(n) : nullptr;
+  float       *dd = water_depth ? sl.take(n) : nullptr;
+  float       *ds = sediment ? sl.take(n) : nullptr;
+  float       *du = vel_u ? sl.take(n) : nullptr;
+  float       *dv = vel_v ? sl.take(n) : nullptr;
+  void        *scr = sl.take(hm::vpipes_scratch_bytes(nx, ny) / sizeof(float) + 1);
+  cudaStream_t s = ctx->stream;
+  HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
+  if (dr) HM_CUDA_TRY(cudaMemcpyAsync(dr, rain_map, nbytes, cudaMemcpyHostToDevice, s));
+  st = hm::vpipes_core(dz, nx, ny, p, dr, dd, ds, du, dv, scr, s);
+  if (st)
+  {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  HM_CUDA_TRY(cudaMemcpyAsync(z, dz, nbytes, cudaMemcpyDeviceToHost, s));
+  if (dd) HM_CUDA_TRY(cudaMemcpyAsync(water_depth, dd, nbytes, cudaMemcpyDeviceToHost, s));
+  if (ds) HM_CUDA_TRY(cudaMemcpyAsync(sediment, ds, nbytes, cudaMemcpyDeviceToHost, s));
+  if (du) HM_CUDA_TRY(cudaMemcpyAsync(vel_u, du, nbytes, cudaMemcpyDeviceToHost, s));
+  if (dv) HM_CUDA_TRY(cudaMemcpyAsync(vel_v, dv, nbytes, cudaMemcpyDeviceToHost, s));
+  HM_CUDA_TRY(cudaStreamSynchronize(s));
+  return HM_OK;
+}
+
+int hm_vpipes_device(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_params *params,
+                     const float *rain_map, float *water_depth, float *sediment, float *vel_u, float *vel_v,
+                     void *stream)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes_device: ctx is NULL");
+  hm_vpipes_params p;
+  hm_vpipes_default_params(&p);
+  if (params) p = *params;
+  int st = hm::vpipes_check_args(z, nx, ny, &p);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::vpipes_scratch_bytes(nx, ny), &ws))) return st;
+  return hm::vpipes_core(z, nx, ny, p, rain_map, water_depth, sediment, vel_u, vel_v, ws, (cudaStream_t)stream);
+}
+
+} // extern "C"

@@ -1,0 +1,20 @@
+/* hm_thermal.h - internal entry points of hm_thermal.cu */
+#ifndef HM_THERMAL_H
+#define HM_THERMAL_H
+
+#include <cuda_runtime.h>
+
+#include "hm_erosion.h"
+
+namespace hm
+{
+int    thermal_check_args(const float *z, int nx, int ny, int iterations, const hm_thermal_options *o);
+/* floats of workspace thermal_core needs (one grid, two with a z0 copy) */
+size_t thermal_scratch_floats(int nx, int ny, bool need_z0);
+/* Device pointers; ordered on s.  talus NULL selects talus_value. */
+int    thermal_core(int device, float *z, int nx, int ny, const float *talus, float talus_value, int iterations,
+                    const float *bedrock, float *depo, const float *mask, const hm_thermal_options *opts,
+                    float *scratch_buf, cudaStream_t s);
+} // namespace hm
+
+#endif

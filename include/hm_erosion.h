@@ -1,0 +1,219 @@
+/*
+ * hm_erosion.h - C-ABI of the B200 erosion solvers (libhm_erosion.so).
+ *
+ * Drop-in replacement for HighMap's GPU thermal and virtual-pipes erosion:
+ * every entry point below replaces one reference interface, cited beside
+ * it.  Grids are float32, element (i, j) at [j * nx + i] (x fastest), the
+ * layout of hmap::Array (HighMap/include/highmap/array.hpp:236-252).
+ *
+ * Semantics of the reference that are decided here:
+ *  - Thermal steps are Jacobi: step t+1 is computed from the whole step-t
+ *    field.  The reference kernel updates z in place from racing
+ *    work-items (HighMap/src/gpu_opencl/kernels/thermal.cl:26-58), which
+ *    is not reproducible; Jacobi is its deterministic form.
+ *  - Bedrock: HM_BEDROCK_INTENDED (default) applies the talus update and
+ *    then clamps to bedrock; HM_BEDROCK_LITERAL reproduces thermal.cl:96-99,
+ *    where the update is overwritten by max(z_before, bedrock).
+ *  - The advection pass samples sediment with OpenCL's linear filter and
+ *    mirrored-repeat addressing at unnormalised coordinates
+ *    (hydraulic_vpipes.cl:201-208), defined here as the specification's
+ *    normalised rule in texel units, fp32 weights.
+ *
+ * Every function returns an hm_status (0 = success).  On failure the
+ * output buffers are left unmodified where the failure is detected before
+ * any device work (argument checks), and hm_last_error() describes it.
+ * Contexts are not shared between threads; one context serialises its own
+ * calls on its stream.
+ */
+#ifndef HM_EROSION_H
+#define HM_EROSION_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define HM_OK 0
+#define HM_ERR_INVALID_ARGUMENT 1
+#define HM_ERR_NO_DEVICE 2
+#define HM_ERR_OUT_OF_MEMORY 3
+#define HM_ERR_CUDA 4
+#define HM_ERR_TIMEOUT 5
+#define HM_ERR_BUSY 6
+
+/* bedrock handling of the thermal step */
+#define HM_BEDROCK_INTENDED 0
+#define HM_BEDROCK_LITERAL 1
+
+typedef struct hm_context hm_context;
+
+/* Replaces hmap::gpu::init_opencl() (HighMap/include/highmap/opencl/
+ * gpu_opencl.hpp:166, HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134):
+ * returns HM_OK when a CUDA device of compute capability 10.x is ready and
+ * the kernels of this library can run on it. */
+int hm_init(void);
+
+/* Context: a CUDA stream for the host-pointer calls and a grow-only device
+ * workspace.  Replaces the OpenCL device/queue singleton that the reference
+ * keeps inside CLWrapper (gpu_opencl.cpp:34). */
+int hm_context_create(hm_context **ctx, int device);
+int hm_context_destroy(hm_context *ctx);
+/* Release the workspace (it grows again on demand). */
+int hm_context_trim(hm_context *ctx);
+
+const char *hm_status_string(int status);
+/* Message of the last failure on the calling thread ("" if none). */
+const char *hm_last_error(void);
+
+typedef struct hm_thermal_options
+{
+  int bedrock_mode; /* HM_BEDROCK_INTENDED or HM_BEDROCK_LITERAL */
+  int time_block;   /* steps advanced per sweep: 0 = tuned default, 1 = one launch per step */
+} hm_thermal_options;
+
+void hm_thermal_default_options(hm_thermal_options *opts);
+
+/* ---- thermal, host buffers ------------------------------------------- */
+
+/* Replaces hmap::gpu::thermal(Array &z, const Array &talus, int iterations,
+ * Array *p_bedrock, Array *p_deposition_map)
+ * (HighMap/include/highmap/erosion.hpp:1784-1788,
+ *  HighMap/src/erosion/thermal_gpu.cpp:17-72).
+ * z: nx*ny, in/out.  talus: nx*ny.  bedrock, deposition_map: nullable.
+ * After the iterations the outer ring is linearly extrapolated
+ * (extrapolate_borders, HighMap/src/boundary/boundary.cpp:19-41) and the
+ * deposition map is max(z_out - z_in, 0).  opts may be NULL.
+ * nx, ny >= 3, iterations >= 0. */
+int hm_thermal(hm_context               *ctx,
+               float                    *z,
+               int                       nx,
+               int                       ny,
+               const float              *talus,
+               int                       iterations,
+               const float              *bedrock,
+               float                    *deposition_map,
+               const hm_thermal_options *opts);
+
+/* Replaces hmap::gpu::thermal(Array &z, float talus, int iterations,
+ * Array *p_bedrock, Array *p_deposition_map) (erosion.hpp:1797-1801,
+ * thermal_gpu.cpp:88-96).  The uniform talus is passed to the kernel as a
+ * scalar instead of being expanded into a map. */
+int hm_thermal_scalar(hm_context               *ctx,
+                      float                    *z,
+                      int                       nx,
+                      int                       ny,
+                      float                     talus,
+                      int                       iterations,
+                      const float              *bedrock,
+                      float                    *deposition_map,
+                      const hm_thermal_options *opts);
+
+/* Replaces hmap::gpu::thermal(Array &z, const Array *p_mask,
+ * const Array &talus, int iterations, Array *p_bedrock,
+ * Array *p_deposition_map) (erosion.hpp:1790-1795, thermal_gpu.cpp:74-86):
+ * z = lerp(z, thermal(z), mask) (operator.hpp:405-418).  mask NULL means no
+ * mask. */
+int hm_thermal_masked(hm_context               *ctx,
+                      float                    *z,
+                      int                       nx,
+                      int                       ny,
+                      const float              *mask,
+                      const float              *talus,
+                      int                       iterations,
+                      const float              *bedrock,
+                      float                    *deposition_map,
+                      const hm_thermal_options *opts);
+
+/* ---- thermal, device-resident buffers --------------------------------- */
+
+/* All pointers are device pointers; the call is ordered on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) and returns without
+ * synchronising.  talus NULL selects the scalar talus_value.  mask,
+ * bedrock and deposition_map are nullable. */
+int hm_thermal_device(hm_context               *ctx,
+                      float                    *z,
+                      int                       nx,
+                      int                       ny,
+                      const float              *talus,
+                      float                     talus_value,
+                      int                       iterations,
+                      const float              *bedrock,
+                      float                    *deposition_map,
+                      const float              *mask,
+                      const hm_thermal_options *opts,
+                      void                     *stream);
+
+/* ---- virtual pipes ----------------------------------------------------- */
+
+typedef struct hm_vpipes_params
+{
+  /* the reference's parameters, erosion.hpp:1206-1223 (same defaults) */
+  float water_height;
+  int   maintain_water_volume;
+  float evap_rate;
+  int   iterations;
+  float dt;
+  float k_capacity;
+  float k_erode;
+  float k_depose;
+  float k_discharge_exp;
+  float downcutting_max_depth_ratio;
+  int   flux_diffusion;
+  float flux_diffusion_strength;
+  /* extensions; the defaults 1, 1, 1, 0, -1 reproduce the reference */
+  float gravity;       /* hydraulic_vpipes.cl:31 hard-codes 1                  */
+  float pipe_length;   /* hydraulic_vpipes.cl:30 hard-codes 1                  */
+  float pipe_area;     /* pipe cross-section, scales the flux update            */
+  float rain_per_step; /* depth added (times rain map) before every flow pass  */
+  float initial_water; /* < 0: water_height (reference); else initial depth     */
+} hm_vpipes_params;
+
+void hm_vpipes_default_params(hm_vpipes_params *p);
+
+/* Replaces hmap::gpu::hydraulic_vpipes(Array &z, float water_height,
+ * bool maintain_water_volume, float evap_rate, int iterations, float dt,
+ * float k_capacity, float k_erode, float k_depose, float k_discharge_exp,
+ * float downcutting_max_depth_ratio, bool flux_diffusion,
+ * float flux_diffusion_strength, Array *p_rain_map, Array *p_water_depth,
+ * Array *p_sediment, Array *p_vel_u, Array *p_vel_v)
+ * (erosion.hpp:1206-1223, HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178).
+ * Host buffers; rain_map and the four outputs are nullable.  params NULL
+ * means the reference defaults. */
+int hm_vpipes(hm_context             *ctx,
+              float                  *z,
+              int                     nx,
+              int                     ny,
+              const hm_vpipes_params *params,
+              const float            *rain_map,
+              float                  *water_depth,
+              float                  *sediment,
+              float                  *vel_u,
+              float                  *vel_v);
+
+/* Device-pointer form of hm_vpipes, ordered on `stream`. */
+int hm_vpipes_device(hm_context             *ctx,
+                     float                  *z,
+                     int                     nx,
+                     int                     ny,
+                     const hm_vpipes_params *params,
+                     const float            *rain_map,
+                     float                  *water_depth,
+                     float                  *sediment,
+                     float                  *vel_u,
+                     float                  *vel_v,
+                     void                   *stream);
+
+/* ---- instrumentation --------------------------------------------------- */
+
+/* Number of kernel launches issued by this library on the calling thread
+ * since the last reset (counted on the host at each launch). */
+unsigned long long hm_launch_count(void);
+void               hm_launch_count_reset(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,196 @@
+"""ctypes front-end of the CPU oracle and of the reference checker.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+CPU-baseline legs of bench.py, always as the checker or the timed CPU
+baseline, never as the product path.  Grids are 2-D numpy arrays of shape
+(ny, nx), C order, so element (i, j) of the reference's hmap::Array is
+``a[j, i]``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build_oracle as _b
+
+BEDROCK_INTENDED = 0
+BEDROCK_LITERAL = 1
+
+
+class VpipesParams(C.Structure):
+    """Mirror of hmo_vpipes_params (hm_oracle.h) and of the product's
+    hm_vpipes_params: the reference parameters of erosion.hpp:1206-1223 plus
+    the extensions gravity, pipe_length, pipe_area, rain_per_step and
+    initial_water (defaults reproduce the reference)."""
+
+    _fields_ = [
+        ("water_height", C.c_float),
+        ("maintain_water_volume", C.c_int),
+        ("evap_rate", C.c_float),
+        ("iterations", C.c_int),
+        ("dt", C.c_float),
+        ("k_capacity", C.c_float),
+        ("k_erode", C.c_float),
+        ("k_depose", C.c_float),
+        ("k_discharge_exp", C.c_float),
+        ("downcutting_max_depth_ratio", C.c_float),
+        ("flux_diffusion", C.c_int),
+        ("flux_diffusion_strength", C.c_float),
+        ("gravity", C.c_float),
+        ("pipe_length", C.c_float),
+        ("pipe_area", C.c_float),
+        ("rain_per_step", C.c_float),
+        ("initial_water", C.c_float),
+    ]
+
+    @classmethod
+    def make(cls, **kw):
+        p = cls()
+        _lib().hmo_vpipes_default_params(C.byref(p))
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise KeyError(k)
+            setattr(p, k, v)
+        return p
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_LIB = None
+_REF = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = C.CDLL(_b.build_oracle())
+        _LIB.hmo_vpipes_default_params.argtypes = [C.c_void_p]
+        _LIB.hmo_sample_linear_mirror_f32.restype = C.c_float
+        _LIB.hmo_sample_linear_mirror_f32.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
+    return _LIB
+
+
+def ref_available() -> bool:
+    return os.path.exists(_b.REF_SO) or _b.build_ref() is not None
+
+
+def _ref():
+    global _REF
+    if _REF is None:
+        path = _b.build_ref()
+        if path is None:
+            raise RuntimeError("reference checker oracle/_ref/libhm_ref.so is not built")
+        _REF = C.CDLL(path)
+    return _REF
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _grid(a, dtype):
+    a = np.ascontiguousarray(a, dtype=dtype)
+    if a.ndim != 2:
+        raise ValueError("expected a 2-D grid")
+    return a
+
+
+def _out(like, want):
+    return np.empty_like(like) if want else None
+
+
+def thermal(z, talus, iterations, bedrock=None, mask=None, deposition=False,
+            bedrock_mode=BEDROCK_INTENDED, dtype=np.float32):
+    """Oracle thermal; returns (z, deposition_map or None)."""
+    z = _grid(z, dtype).copy()
+    ny, nx = z.shape
+    if np.isscalar(talus):
+        talus = np.full_like(z, talus)
+    talus = _grid(talus, dtype)
+    bedrock = None if bedrock is None else _grid(bedrock, dtype)
+    mask = None if mask is None else _grid(mask, dtype)
+    depo = _out(z, deposition)
+    fn = _lib().hmo_thermal_f32 if dtype == np.float32 else _lib().hmo_thermal_f64
+    rc = fn(_p(z), nx, ny, _p(talus), int(iterations), _p(bedrock), _p(depo), _p(mask), int(bedrock_mode))
+    if rc:
+        raise ValueError("oracle thermal rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
+def thermal_auto_bedrock(z, talus, iterations, deposition=False):
+    z = _grid(z, np.float32).copy()
+    ny, nx = z.shape
+    if np.isscalar(talus):
+        talus = np.full_like(z, talus)
+    talus = _grid(talus, np.float32)
+    depo = _out(z, deposition)
+    rc = _lib().hmo_thermal_auto_bedrock_f32(_p(z), nx, ny, _p(talus), int(iterations), _p(depo))
+    if rc:
+        raise ValueError("oracle thermal_auto_bedrock rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
+def vpipes(z, params: VpipesParams, rain_map=None, dtype=np.float32):
+    """Oracle vpipes; returns (z, water_depth, sediment, vel_u, vel_v)."""
+    z = _grid(z, dtype).copy()
+    ny, nx = z.shape
+    rain = None if rain_map is None else _grid(rain_map, dtype)
+    outs = [np.empty_like(z) for _ in range(4)]
+    fn = _lib().hmo_vpipes_f32 if dtype == np.float32 else _lib().hmo_vpipes_f64
+    rc = fn(_p(z), nx, ny, C.byref(params), _p(rain), *[_p(o) for o in outs])
+    if rc:
+        raise ValueError("oracle vpipes rejected its arguments (status %d)" % rc)
+    return (z, *outs)
+
+
+def sample_linear_mirror(s, x, y):
+    s = _grid(s, np.float32)
+    ny, nx = s.shape
+    return float(_lib().hmo_sample_linear_mirror_f32(_p(s), nx, ny, float(x), float(y)))
+
+
+def ref_thermal(z, talus, iterations, bedrock=None, mask=None, deposition=False):
+    """The reference's thermal / thermal_with_bedrock kernel text, Jacobi form."""
+    z = _grid(z, np.float32).copy()
+    ny, nx = z.shape
+    if np.isscalar(talus):
+        talus = np.full_like(z, talus)
+    talus = _grid(talus, np.float32)
+    bedrock = None if bedrock is None else _grid(bedrock, np.float32)
+    mask = None if mask is None else _grid(mask, np.float32)
+    depo = _out(z, deposition)
+    rc = _ref().ref_thermal(_p(z), nx, ny, _p(talus), int(iterations), _p(bedrock), _p(depo), _p(mask))
+    if rc:
+        raise ValueError("ref thermal rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
+def ref_thermal_auto_bedrock(z, talus, iterations, deposition=False):
+    z = _grid(z, np.float32).copy()
+    ny, nx = z.shape
+    if np.isscalar(talus):
+        talus = np.full_like(z, talus)
+    talus = _grid(talus, np.float32)
+    depo = _out(z, deposition)
+    rc = _ref().ref_thermal_auto_bedrock(_p(z), nx, ny, _p(talus), int(iterations), _p(depo))
+    if rc:
+        raise ValueError("ref thermal_auto_bedrock rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
+def ref_vpipes(z, params: VpipesParams, rain_map=None):
+    z = _grid(z, np.float32).copy()
+    ny, nx = z.shape
+    rain = None if rain_map is None else _grid(rain_map, np.float32)
+    outs = [np.empty_like(z) for _ in range(4)]
+    rc = _ref().ref_vpipes(_p(z), nx, ny, C.byref(params), _p(rain), *[_p(o) for o in outs])
+    if rc:
+        raise ValueError("ref vpipes rejected its arguments (status %d)" % rc)
+    return (z, *outs)
+
+
+def num_threads() -> int:
+    return int(_lib().hmo_num_threads())

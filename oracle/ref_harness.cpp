@@ -1,0 +1,299 @@
+/*
+ * ref_harness.cpp - host driver around the reference's own kernel text
+ * compiled for the CPU (see ref_shim.h and build_oracle.py).
+ *
+ * TEST INFRASTRUCTURE ONLY: pins the oracle and serves as the timed CPU
+ * baseline of the benchmark's reference arm.  Built into oracle/_ref/.
+ *
+ * The host drivers of the reference (thermal_gpu.cpp, hydraulic_vpipes_gpu.cpp)
+ * need glm and the absent CLWrapper submodule, so their loops are restated
+ * here around the compiled kernels:
+ *   ref_thermal    : HighMap/src/erosion/thermal_gpu.cpp:17-96
+ *   ref_thermal_auto_bedrock : thermal_gpu.cpp:98-130
+ *   ref_vpipes     : HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
+ *
+ * Work-items run as a host loop (OpenMP over rows).  The in-place thermal
+ * kernels are given a private copy of the three rows around the work-item,
+ * restored after each call, so every work-item reads step t and the result
+ * is the Jacobi (deterministic) form of the racing in-place update.
+ */
+#include <algorithm>
+#include <cfloat>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "hm_oracle.h"
+#include "ref_shim.h"
+
+namespace hmref
+{
+thread_local int g_gid0 = 0;
+thread_local int g_gid1 = 0;
+
+/* compiled from the reference's kernel text (ref_kernels.o) */
+void thermal(float *z, const float *talus, const int nx, const int ny, const int it);
+void thermal_with_bedrock(float       *z,
+                          const float *talus,
+                          const float *bedrock,
+                          const int    nx,
+                          const int    ny,
+                          const int    it);
+void thermal_auto_bedrock(float       *z,
+                          const float *talus,
+                          float       *bedrock,
+                          const float *z0,
+                          const int    nx,
+                          const int    ny,
+                          const int    it);
+void hydraulic_vpipes_flow_pass(image2d_t, image2d_t, image2d_t, image2d_t, image2d_t, image2d_t,
+                                image2d_t, image2d_t, image2d_t, image2d_t, const int, const int,
+                                const float, const int, const float);
+void hydraulic_vpipes_water_pass(image2d_t, image2d_t, image2d_t, image2d_t, image2d_t, image2d_t,
+                                 image2d_t, image2d_t, image2d_t, const int, const int, const float,
+                                 const float);
+void hydraulic_vpipes_erosion_pass(image2d_t, image2d_t, image2d_t, image2d_t, image2d_t, image2d_t,
+                                   image2d_t, const int, const int, const float, const float,
+                                   const float, const float, const float, const float);
+void hydraulic_vpipes_sediment_transport_pass(image2d_t, image2d_t, image2d_t, image2d_t, const int,
+                                              const int, const float);
+} // namespace hmref
+
+namespace
+{
+
+/* extrapolate_borders(z, nbuffer=1, sigma=0), boundary.cpp:19-41 */
+void extrapolate_borders(float *z, int ni, int nj)
+{
+  auto at = [&](int i, int j) -> float & { return z[(long)j * ni + i]; };
+  for (int j = 0; j < nj; j++)
+  {
+    at(0, j) = 2.f * at(1, j) - at(2, j);
+    at(ni - 1, j) = 2.f * at(ni - 2, j) - at(ni - 3, j);
+  }
+  for (int i = 0; i < ni; i++)
+  {
+    at(i, 0) = 2.f * at(i, 1) - at(i, 2);
+    at(i, nj - 1) = 2.f * at(i, nj - 2) - at(i, nj - 3);
+  }
+}
+
+/* One launch of an in-place thermal kernel over the nx x ny NDRange,
+ * Jacobi form: a is step t, b receives step t+1.  `launch(zw)` runs the
+ * kernel for the current work-item with zw addressing the row window. */
+template <class Launch>
+void run_inplace(const float *a, float *b, float *bed, int nx, int ny, Launch launch)
+{
+  (void)bed;
+#pragma omp parallel
+  {
+    std::vector<float> win((size_t)3 * nx, NAN);
+#pragma omp for schedule(static)
+    for (int j = 0; j < ny; j++)
+    {
+      for (int r = -1; r <= 1; r++)
+        if (j + r >= 0 && j + r < ny)
+          std::memcpy(&win[(size_t)(r + 1) * nx], a + (size_t)(j + r) * nx, sizeof(float) * nx);
+        else
+          std::fill(win.begin() + (size_t)(r + 1) * nx, win.begin() + (size_t)(r + 2) * nx, NAN);
+      /* zw[(j + r) * nx + i] == win[(r + 1) * nx + i] */
+      float *zw = win.data() - ((ptrdiff_t)j - 1) * (ptrdiff_t)nx;
+      hmref::g_gid1 = j;
+      for (int i = 0; i < nx; i++)
+      {
+        hmref::g_gid0 = i;
+        launch(zw);
+        b[(size_t)j * nx + i] = win[(size_t)nx + i];
+        win[(size_t)nx + i] = a[(size_t)j * nx + i];
+      }
+    }
+  }
+}
+
+} // namespace
+
+extern "C" {
+
+/* thermal_gpu.cpp:17-72 (and :74-86 when mask != NULL).  The bedrock
+ * variant is the literal thermal_with_bedrock kernel. */
+int ref_thermal(float       *z,
+                int          nx,
+                int          ny,
+                const float *talus,
+                int          iterations,
+                const float *bedrock,
+                float       *deposition_map,
+                const float *mask)
+{
+  if (!z || !talus || nx < 3 || ny < 3 || iterations < 0) return 1;
+  const size_t       n = (size_t)nx * ny;
+  std::vector<float> z0(z, z + n), a(z, z + n), b(n);
+  for (int it = 0; it < iterations; it++)
+  {
+    if (bedrock)
+      run_inplace(a.data(), b.data(), nullptr, nx, ny, [&](float *zw)
+                  { hmref::thermal_with_bedrock(zw, talus, bedrock, nx, ny, it); });
+    else
+      run_inplace(a.data(), b.data(), nullptr, nx, ny,
+                  [&](float *zw) { hmref::thermal(zw, talus, nx, ny, it); });
+    std::swap(a, b);
+  }
+  extrapolate_borders(a.data(), nx, ny);
+  if (deposition_map)
+    for (size_t k = 0; k < n; k++) deposition_map[k] = std::max(a[k] - z0[k], 0.f);
+  if (mask)
+    for (size_t k = 0; k < n; k++) z[k] = z0[k] * (1.f - mask[k]) + a[k] * mask[k];
+  else
+    std::memcpy(z, a.data(), n * sizeof(float));
+  return 0;
+}
+
+/* thermal_gpu.cpp:98-130 */
+int ref_thermal_auto_bedrock(float       *z,
+                             int          nx,
+                             int          ny,
+                             const float *talus,
+                             int          iterations,
+                             float       *deposition_map)
+{
+  if (!z || !talus || nx < 3 || ny < 3 || iterations < 0) return 1;
+  const size_t       n = (size_t)nx * ny;
+  std::vector<float> z0(z, z + n), a(z, z + n), b(n), bed(n, 0.f);
+  for (int it = 0; it < iterations; it++)
+  {
+    run_inplace(a.data(), b.data(), bed.data(), nx, ny, [&](float *zw)
+                { hmref::thermal_auto_bedrock(zw, talus, bed.data(), z0.data(), nx, ny, it); });
+    std::swap(a, b);
+  }
+  extrapolate_borders(a.data(), nx, ny);
+  if (deposition_map)
+    for (size_t k = 0; k < n; k++) deposition_map[k] = std::max(a[k] - z0[k], 0.f);
+  std::memcpy(z, a.data(), n * sizeof(float));
+  return 0;
+}
+
+/* hydraulic_vpipes_gpu.cpp:15-178.  Separate input and output images per
+ * pass, as the driver binds them; Array::sum is the serial float
+ * accumulate of methods.cpp:428-431.  The kernels hard-code gravity and
+ * pipe length to 1, so p->gravity, p->pipe_length and p->pipe_area are
+ * not used here; the driver-level extensions rain_per_step and
+ * initial_water are. */
+int ref_vpipes(float                   *z,
+               int                      nx,
+               int                      ny,
+               const hmo_vpipes_params *p,
+               const float             *rain_map,
+               float                   *water_depth,
+               float                   *sediment,
+               float                   *vel_u,
+               float                   *vel_v)
+{
+  if (!z || !p || nx < 1 || ny < 1 || p->iterations < 0) return 1;
+  const size_t       n = (size_t)nx * ny;
+  std::vector<float> rain(n, 1.f);
+  if (rain_map) rain.assign(rain_map, rain_map + n);
+  const float        init_depth = p->initial_water < 0.f ? p->water_height : p->initial_water;
+  std::vector<float> d(n, init_depth), d1(n), d2(n), s(n, 0.f), fl(n, 0.f), fr(n, 0.f), ft(n, 0.f),
+      fb(n, 0.f), u(n, 0.f), v(n, 0.f);
+  std::vector<float> fl_o(n), fr_o(n), ft_o(n), fb_o(n), z_o(n), s_o(n);
+  for (size_t k = 0; k < n; k++) d[k] *= rain[k];
+  const float water_volume_init = std::accumulate(d.begin(), d.end(), 0.f);
+  const float rain_map_volume = std::accumulate(rain.begin(), rain.end(), 0.f);
+
+  auto img = [&](std::vector<float> &a) { return hmref::hm_image{a.data(), nx, ny}; };
+
+  for (int it = 0; it < p->iterations; it++)
+  {
+    for (size_t k = 0; k < n; k++) d1[k] = d[k] + p->rain_per_step * rain[k];
+
+    hmref::hm_image iz{z, nx, ny}, i_fl = img(fl), i_fr = img(fr), i_ft = img(ft), i_fb = img(fb),
+                    i_d1 = img(d1), o_fl = img(fl_o), o_fr = img(fr_o), o_ft = img(ft_o), o_fb = img(fb_o),
+                    i_d2 = img(d2), i_u = img(u), i_v = img(v), i_s = img(s), o_z = img(z_o),
+                    o_s = img(s_o);
+
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < ny; j++)
+    {
+      hmref::g_gid1 = j;
+      for (int i = 0; i < nx; i++)
+      {
+        hmref::g_gid0 = i;
+        hmref::hydraulic_vpipes_flow_pass(&iz, &i_fl, &i_fr, &i_ft, &i_fb, &i_d1, &o_fl, &o_fr, &o_ft,
+                                          &o_fb, nx, ny, p->dt, p->flux_diffusion ? 1 : 0,
+                                          p->flux_diffusion_strength);
+      }
+    }
+    fl.swap(fl_o);
+    fr.swap(fr_o);
+    ft.swap(ft_o);
+    fb.swap(fb_o);
+    i_fl = img(fl), i_fr = img(fr), i_ft = img(ft), i_fb = img(fb);
+
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < ny; j++)
+    {
+      hmref::g_gid1 = j;
+      for (int i = 0; i < nx; i++)
+      {
+        hmref::g_gid0 = i;
+        hmref::hydraulic_vpipes_water_pass(&iz, &i_fl, &i_fr, &i_ft, &i_fb, &i_d1, &i_d2, &i_u, &i_v,
+                                           nx, ny, p->dt, p->water_height);
+      }
+    }
+
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < ny; j++)
+    {
+      hmref::g_gid1 = j;
+      for (int i = 0; i < nx; i++)
+      {
+        hmref::g_gid0 = i;
+        hmref::hydraulic_vpipes_erosion_pass(&iz, &i_d2, &i_u, &i_v, &i_s, &o_z, &o_s, nx, ny,
+                                             p->water_height, p->k_capacity, p->k_erode, p->k_depose,
+                                             p->k_discharge_exp, p->downcutting_max_depth_ratio);
+      }
+    }
+    std::memcpy(z, z_o.data(), n * sizeof(float));
+    o_s = img(s_o);
+
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < ny; j++)
+    {
+      hmref::g_gid1 = j;
+      for (int i = 0; i < nx; i++)
+      {
+        hmref::g_gid0 = i;
+        hmref::hydraulic_vpipes_sediment_transport_pass(&i_u, &i_v, &o_s, &i_s, nx, ny, p->dt);
+      }
+    }
+
+    const float keep = 1.f - p->dt * p->evap_rate;
+    for (size_t k = 0; k < n; k++) d[k] = d2[k] * keep;
+    if (p->maintain_water_volume)
+    {
+      float water_to_add = water_volume_init - std::accumulate(d.begin(), d.end(), 0.f);
+      for (size_t k = 0; k < n; k++) d[k] += water_to_add * rain[k] / rain_map_volume;
+    }
+  }
+
+  if (water_depth) std::memcpy(water_depth, d.data(), n * sizeof(float));
+  if (sediment) std::memcpy(sediment, s.data(), n * sizeof(float));
+  if (vel_u) std::memcpy(vel_u, u.data(), n * sizeof(float));
+  if (vel_v) std::memcpy(vel_v, v.data(), n * sizeof(float));
+  return 0;
+}
+
+int ref_num_threads(void)
+{
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+} // extern "C"

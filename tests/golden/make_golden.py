@@ -1,0 +1,95 @@
+"""Generate tests/golden/*.npz from the reference's own kernel text.
+
+The reference has no golden vectors or known-answer tests for either
+solver, so these fixtures are outputs of the reference's OpenCL kernels
+(HighMap/src/gpu_opencl/kernels/thermal.cl, hydraulic_vpipes.cl) compiled
+for the CPU by oracle/build_oracle.py and driven by oracle/ref_harness.cpp
+(Jacobi form).  Run in a checkout where the reference tree is present:
+
+    python tests/golden/make_golden.py
+
+Each .npz holds the inputs, the parameters and the outputs of one case.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from highmap_b200.inputs import fbm  # noqa: E402
+from oracle import pyoracle as po  # noqa: E402
+
+
+def _save(name, **arrays):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **arrays)
+    print("wrote", path)
+
+
+def thermal_cases():
+    nx, ny = 64, 48
+    z = fbm(nx, ny, seed=1)
+    talus = (0.5 + fbm(nx, ny, seed=3)) / nx
+    talus_u = np.full_like(z, 1.0 / nx)
+    mask = fbm(nx, ny, seed=5)
+
+    zo, depo = po.ref_thermal(z, talus_u, 100, deposition=True)
+    _save("thermal_uniform", z=z, talus=talus_u, iterations=np.int32(100), out_z=zo, out_depo=depo)
+
+    zo, depo = po.ref_thermal(z, talus, 60, deposition=True)
+    _save("thermal_talus_map", z=z, talus=talus, iterations=np.int32(60), out_z=zo, out_depo=depo)
+
+    bed = (0.3 * z).astype(np.float32)
+    zo, depo = po.ref_thermal(z, talus, 40, bedrock=bed, deposition=True)
+    _save("thermal_bedrock_literal", z=z, talus=talus, bedrock=bed, iterations=np.int32(40), out_z=zo,
+          out_depo=depo)
+
+    zo, depo = po.ref_thermal(z, talus, 40, mask=mask, deposition=True)
+    _save("thermal_masked", z=z, talus=talus, mask=mask, iterations=np.int32(40), out_z=zo, out_depo=depo)
+
+    zo, depo = po.ref_thermal_auto_bedrock(z, talus_u * 4, 60, deposition=True)
+    _save("thermal_auto_bedrock", z=z, talus=talus_u * 4, iterations=np.int32(60), out_z=zo, out_depo=depo)
+
+    # odd, non-square, minimal sizes
+    for (nx2, ny2) in ((3, 3), (5, 17), (33, 7)):
+        z2 = fbm(nx2, ny2, seed=7, kw=2.0)
+        zo, depo = po.ref_thermal(z2, np.full_like(z2, 0.01), 9, deposition=True)
+        _save("thermal_small_%dx%d" % (nx2, ny2), z=z2, talus=np.full_like(z2, 0.01), iterations=np.int32(9),
+              out_z=zo, out_depo=depo)
+
+
+def vpipes_cases():
+    nx, ny = 48, 40
+    z = fbm(nx, ny, seed=2)
+    rain = (0.5 + fbm(nx, ny, seed=9)).astype(np.float32)
+    cases = {
+        # defaults of erosion.hpp:1206-1223, 25 iterations
+        "vpipes_defaults": (dict(iterations=25), None),
+        "vpipes_rain_map": (dict(iterations=25), rain),
+        "vpipes_no_maintain": (dict(iterations=30, maintain_water_volume=0), None),
+        "vpipes_rain_per_step": (dict(iterations=40, maintain_water_volume=0, flux_diffusion=0, dt=0.1,
+                                      k_capacity=0.05, k_erode=0.01, k_depose=0.01, evap_rate=0.01,
+                                      rain_per_step=1e-4, initial_water=0.0), None),
+        "vpipes_exp_half": (dict(iterations=20, maintain_water_volume=0, k_discharge_exp=0.5), None),
+    }
+    for name, (kw, rmap) in cases.items():
+        p = po.VpipesParams.make(**kw)
+        zo, d, s, u, v = po.ref_vpipes(z, p, rain_map=rmap)
+        arrays = dict(z=z, params=np.array(json.dumps(p.as_dict())), out_z=zo, out_water=d, out_sediment=s,
+                      out_u=u, out_v=v)
+        if rmap is not None:
+            arrays["rain_map"] = rmap
+        _save(name, **arrays)
+
+
+if __name__ == "__main__":
+    if not po.ref_available():
+        sys.exit("the reference checker oracle/_ref/libhm_ref.so could not be built")
+    thermal_cases()
+    vpipes_cases()

@@ -1,0 +1,79 @@
+"""CPU tests of the C-ABI library: it builds for sm_100a, loads, exports
+every function include/hm_erosion.h declares, and rejects bad arguments
+before touching a device."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = set(re.findall(r"\b(hm_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    lib = C.CDLL(built_lib)
+    declared = _declared("hm_erosion.h")
+    assert declared, "no declarations parsed"
+    missing = [n for n in sorted(declared) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header(built_lib):
+    from highmap_b200 import _lib as L
+    assert _declared("hm_erosion.h") <= set(L.EXPORTED)
+
+
+def test_library_is_sm100a(built_lib):
+    import subprocess
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", built_lib], capture_output=True,
+                         text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_argument_checks_without_device(built_lib):
+    from highmap_b200 import _lib as L
+    lib = L.lib()
+    z = np.zeros((4, 4), np.float32)
+    # NULL context is rejected before any CUDA call
+    assert lib.hm_thermal_scalar(None, C.c_void_p(z.ctypes.data), 4, 4, C.c_float(0.1), 1, None, None,
+                                 None) == L.HM_ERR_INVALID_ARGUMENT
+    assert lib.hm_vpipes(None, C.c_void_p(z.ctypes.data), 4, 4, None, None, None, None, None,
+                         None) == L.HM_ERR_INVALID_ARGUMENT
+    assert b"NULL" in lib.hm_last_error()
+    assert lib.hm_status_string(L.HM_ERR_OUT_OF_MEMORY) == b"out of device memory"
+
+
+def test_defaults_match_reference_signature(built_lib):
+    """hm_vpipes_default_params carries the defaults of
+    HighMap/include/highmap/erosion.hpp:1206-1223."""
+    from highmap_b200 import gpu as G
+    p = G.vpipes_params()
+    assert p.water_height == pytest.approx(1e-2)
+    assert p.maintain_water_volume == 1
+    assert p.evap_rate == pytest.approx(0.1)
+    assert p.iterations == 50
+    assert p.dt == pytest.approx(0.5)
+    assert p.k_capacity == pytest.approx(0.5)
+    assert p.k_erode == pytest.approx(0.001)
+    assert p.k_depose == pytest.approx(0.01)
+    assert p.k_discharge_exp == 1.0
+    assert p.downcutting_max_depth_ratio == 10.0
+    assert p.flux_diffusion == 1
+    assert p.flux_diffusion_strength == pytest.approx(0.01)
+    assert (p.gravity, p.pipe_length, p.pipe_area, p.rain_per_step, p.initial_water) == (1, 1, 1, 0, -1)
+
+
+def test_no_cpu_fallback_when_library_missing(monkeypatch, tmp_path):
+    from highmap_b200 import _lib as L
+    monkeypatch.setattr(L, "_lib", None)
+    monkeypatch.setattr(L, "LIB_PATH", str(tmp_path / "missing.so"))
+    with pytest.raises(RuntimeError, match="not built"):
+        L.lib()

@@ -1,0 +1,178 @@
+"""CPU tests of the oracle: pinned to the reference's kernel text.
+
+1. Against the golden fixtures (tests/golden/, made from the reference's
+   own OpenCL kernels compiled for the CPU): bit-exact wherever the oracle
+   and the reference evaluate the same fp32 operations; within a tight
+   tolerance where they differ by construction (the reference sums the
+   water volume serially in float, the oracle in fp64).
+2. Against the reference checker on fresh seeded inputs, when it is built.
+3. Property tests in the style of the reference's unit tests
+   (tests/src/test_smooth_cpulse.cpp and friends): flat field unchanged,
+   slopes under talus unchanged, a spike relaxes symmetrically, interior
+   mass conservation, no water means no erosion.
+"""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+from highmap_b200.inputs import fbm
+from oracle import pyoracle as po
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _load(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def _params(g):
+    return po.VpipesParams.make(**json.loads(str(g["params"])))
+
+
+@pytest.mark.parametrize("name", ["thermal_uniform", "thermal_talus_map", "thermal_masked", "thermal_small_3x3",
+                                  "thermal_small_5x17", "thermal_small_33x7"])
+def test_thermal_golden_bit_exact(name):
+    g = _load(name)
+    z, depo = po.thermal(g["z"], g["talus"], int(g["iterations"]), mask=g.get("mask"), deposition=True)
+    assert np.array_equal(z, g["out_z"])
+    assert np.array_equal(depo, g["out_depo"])
+
+
+def test_thermal_bedrock_literal_golden():
+    g = _load("thermal_bedrock_literal")
+    z, depo = po.thermal(g["z"], g["talus"], int(g["iterations"]), bedrock=g["bedrock"], deposition=True,
+                         bedrock_mode=po.BEDROCK_LITERAL)
+    assert np.array_equal(z, g["out_z"])
+    assert np.array_equal(depo, g["out_depo"])
+
+
+def test_thermal_auto_bedrock_golden():
+    g = _load("thermal_auto_bedrock")
+    z, depo = po.thermal_auto_bedrock(g["z"], g["talus"], int(g["iterations"]), deposition=True)
+    assert np.array_equal(z, g["out_z"])
+    assert np.array_equal(depo, g["out_depo"])
+
+
+@pytest.mark.parametrize("name", ["vpipes_no_maintain", "vpipes_rain_per_step", "vpipes_exp_half"])
+def test_vpipes_golden_bit_exact(name):
+    g = _load(name)
+    out = po.vpipes(g["z"], _params(g), rain_map=g.get("rain_map"))
+    for got, key in zip(out, ("out_z", "out_water", "out_sediment", "out_u", "out_v")):
+        assert np.array_equal(got, g[key]), key
+
+
+@pytest.mark.parametrize("name", ["vpipes_defaults", "vpipes_rain_map"])
+def test_vpipes_golden_volume_sum(name):
+    """maintain_water_volume: the reference sums the depth serially in
+    float (Array::sum); the oracle sums in fp64.  The outputs agree to well
+    inside the 1e-3 height-range tolerance."""
+    g = _load(name)
+    out = po.vpipes(g["z"], _params(g), rain_map=g.get("rain_map"))
+    rng = float(g["z"].max() - g["z"].min())
+    assert np.abs(out[0] - g["out_z"]).max() <= 1e-4 * rng
+    assert np.abs(out[1] - g["out_water"]).max() <= 1e-4 * float(g["out_water"].max())
+    assert np.abs(out[2] - g["out_sediment"]).max() <= 1e-4 * rng
+
+
+def test_golden_files_present():
+    names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))}
+    assert {"thermal_uniform", "vpipes_defaults", "vpipes_rain_per_step"} <= names
+
+
+ref_only = pytest.mark.skipif(not po.ref_available(), reason="reference checker not built here")
+
+
+@ref_only
+@pytest.mark.parametrize("seed", [11, 12])
+def test_thermal_matches_reference_text(seed):
+    z = fbm(71, 53, seed=seed)
+    talus = (0.5 + fbm(71, 53, seed=seed + 100)) / 71
+    bed = (0.5 * z).astype(np.float32)
+    for kw in (dict(), dict(bedrock=bed)):
+        a, da = po.thermal(z, talus, 30, deposition=True, bedrock_mode=po.BEDROCK_LITERAL, **kw)
+        b, db = po.ref_thermal(z, talus, 30, deposition=True, **kw)
+        assert np.array_equal(a, b) and np.array_equal(da, db)
+
+
+@ref_only
+def test_vpipes_matches_reference_text():
+    z = fbm(40, 56, seed=21)
+    p = po.VpipesParams.make(iterations=15, maintain_water_volume=0, flux_diffusion=1, dt=0.3)
+    a = po.vpipes(z, p)
+    b = po.ref_vpipes(z, p)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_flat_field_unchanged():
+    z = np.full((20, 24), 0.5, np.float32)
+    out, depo = po.thermal(z, 0.01, 50, deposition=True)
+    assert np.array_equal(out, z)
+    assert not depo.any()
+
+
+def test_slope_below_talus_unchanged():
+    ny, nx = 30, 40
+    z = (np.arange(nx, dtype=np.float32)[None, :] * 0.001 + np.zeros((ny, 1), np.float32)).astype(np.float32)
+    out, _ = po.thermal(z, 0.0011, 20)
+    # interior unchanged; the border is extrapolated linearly, which keeps a plane
+    np.testing.assert_allclose(out, z, atol=1e-6)
+
+
+def test_spike_relaxes_symmetrically():
+    n = 33
+    z = np.zeros((n, n), np.float32)
+    z[n // 2, n // 2] = 1.0
+    out, _ = po.thermal(z, 0.0, 8)
+    inner = out[2:-2, 2:-2]
+    assert np.allclose(inner, inner.T, atol=1e-7)
+    assert np.allclose(inner, inner[::-1, :], atol=1e-7)
+    assert out[n // 2, n // 2] < 1.0
+
+
+def test_interior_mass_conserved_uniform_talus():
+    """With a uniform talus every exchange is antisymmetric between the two
+    cells, so the sum over cells far from the border (where the border
+    copy rule cannot reach in a few steps) changes only by rounding."""
+    n = 64
+    z = np.zeros((n, n), np.float32)
+    z[24:40, 24:40] = fbm(16, 16, seed=4)
+    out, _ = po.thermal(z, 0.001, 6, dtype=np.float64)
+    assert abs(out.sum() - z.astype(np.float64).sum()) < 1e-9
+
+
+def test_vpipes_dry_leaves_terrain():
+    z = fbm(32, 24, seed=5)
+    p = po.VpipesParams.make(iterations=10, water_height=1e-2, initial_water=0.0, maintain_water_volume=0)
+    zo, d, s, u, v = po.vpipes(z, p)
+    assert np.array_equal(zo, z)
+    assert not s.any() and not d.any() and not u.any() and not v.any()
+
+
+def test_sampler_half_texel_shift():
+    """At zero velocity the linear sampler blends (i-1, i) with weights 1/2:
+    texel centres are at k + 0.5 (hydraulic_vpipes.cl:207-208)."""
+    s = np.arange(12, dtype=np.float32).reshape(3, 4)
+    assert po.sample_linear_mirror(s, 2.0, 1.5) == pytest.approx(0.5 * (s[1, 1] + s[1, 2]))
+    # mirrored repeat at the left edge: texel -1 reads texel 0
+    assert po.sample_linear_mirror(s, 0.0, 1.5) == pytest.approx(s[1, 0])
+    # far outside: mirror with period 2 * width
+    assert po.sample_linear_mirror(s, 8.5 + 0.0, 1.5) == pytest.approx(po.sample_linear_mirror(s, 0.5, 1.5))
+
+
+def test_float_vs_double_thermal_error_small():
+    z = fbm(64, 64, seed=1)
+    a, _ = po.thermal(z, 1 / 64, 100)
+    b, _ = po.thermal(z.astype(np.float64), 1 / 64, 100, dtype=np.float64)
+    assert np.abs(a - b).max() <= 1e-4 * float(z.max() - z.min())
+
+
+def test_float_vs_double_vpipes_error_small():
+    z = fbm(48, 48, seed=2)
+    p = po.VpipesParams.make(iterations=30)
+    a = po.vpipes(z, p)
+    b = po.vpipes(z.astype(np.float64), p, dtype=np.float64)
+    assert np.abs(a[0] - b[0]).max() <= 1e-3 * float(z.max() - z.min())

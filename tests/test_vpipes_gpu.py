@@ -1,0 +1,132 @@
+"""GPU parity of the virtual-pipes solver against the oracle, via the C-ABI.
+
+Bit-exact where both sides evaluate the same fp32 operations (every case
+without the water-volume top-up: the GPU reproduces the reference's
+one-rounding-per-operation arithmetic, fp64 hypot included).  With
+maintain_water_volume the grid-wide fp64 sum is reduced in a different
+order on the two sides; there the bar is the north-star tolerance (max abs
+error <= 1e-3 of the height range) on z and sediment.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from highmap_b200.inputs import fbm
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-3  # of the height range, vpipes
+
+CONFIG2 = dict(maintain_water_volume=0, flux_diffusion=0, dt=0.1, k_capacity=0.05, k_erode=0.01, k_depose=0.01,
+               evap_rate=0.01, gravity=9.81, pipe_area=1.0, pipe_length=1.0, rain_per_step=1e-4,
+               initial_water=0.0, water_height=1e-2)
+
+
+def _run_gpu(gpu, z0, pkw, rain=None):
+    z = z0.copy()
+    outs = [np.empty_like(z) for _ in range(4)]
+    kw = dict(pkw)
+    it = kw.pop("iterations", 50)
+    gpu.hydraulic_vpipes(z, iterations=it, rain_map=rain, water_depth=outs[0], sediment=outs[1], vel_u=outs[2],
+                         vel_v=outs[3], **kw)
+    return (z, *outs)
+
+
+def _check(got, want, z0, exact):
+    rng = float(z0.max() - z0.min()) or 1.0
+    names = ("z", "water", "sediment", "u", "v")
+    errs = {n: float(np.abs(g.astype(np.float64) - w).max()) for n, g, w in zip(names, got, want)}
+    assert errs["z"] <= TOL * rng, errs
+    assert errs["sediment"] <= TOL * rng, errs
+    if exact:
+        for n, g, w in zip(names, got, want):
+            assert np.array_equal(g, w), "%s not bit-exact: %s" % (n, errs)
+
+
+@pytest.mark.parametrize("name", ["vpipes_no_maintain", "vpipes_rain_per_step", "vpipes_exp_half",
+                                  "vpipes_defaults", "vpipes_rain_map"])
+def test_golden(gpu, name):
+    g = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+    p = json.loads(str(g["params"]))
+    got = _run_gpu(gpu, g["z"], p, rain=g.get("rain_map"))
+    want = tuple(g[k] for k in ("out_z", "out_water", "out_sediment", "out_u", "out_v"))
+    _check(got, want, g["z"], exact=not p["maintain_water_volume"])
+
+
+@pytest.mark.parametrize("shape", [(128, 128), (97, 131), (256, 64), (5, 300)])
+@pytest.mark.parametrize("case", ["config2", "defaults", "no_maintain_diffusion", "rain_map", "pipe_length"])
+def test_against_oracle(gpu, shape, case):
+    ny, nx = shape
+    z0 = fbm(nx, ny, seed=2)
+    rain = None
+    if case == "config2":
+        pkw = dict(CONFIG2, iterations=60)
+    elif case == "defaults":
+        pkw = dict(iterations=30)
+    elif case == "no_maintain_diffusion":
+        pkw = dict(iterations=30, maintain_water_volume=0)
+    elif case == "rain_map":
+        pkw = dict(iterations=30)
+        rain = (0.25 + fbm(nx, ny, seed=12)).astype(np.float32)
+    else:
+        pkw = dict(iterations=30, maintain_water_volume=0, pipe_length=0.75, gravity=2.0, pipe_area=0.5)
+    want = po.vpipes(z0, po.VpipesParams.make(**pkw), rain_map=rain)
+    got = _run_gpu(gpu, z0, pkw, rain)
+    _check(got, want, z0, exact=not pkw.get("maintain_water_volume", 1))
+
+
+def test_deterministic(gpu):
+    z0 = fbm(300, 220, seed=3)
+    a = _run_gpu(gpu, z0, dict(iterations=40))
+    b = _run_gpu(gpu, z0, dict(iterations=40))
+    for x, y in zip(a, b):
+        assert x.tobytes() == y.tobytes()
+
+
+def test_device_api_matches_host_api(gpu):
+    import torch
+    z0 = fbm(512, 256, seed=7)
+    pkw = dict(CONFIG2, iterations=50)
+    h = _run_gpu(gpu, z0, pkw)
+    dz = torch.from_numpy(z0.copy()).cuda()
+    outs = [torch.empty_like(dz) for _ in range(4)]
+    gpu.hydraulic_vpipes_device(dz, gpu.vpipes_params(**pkw), None, *outs)
+    torch.cuda.synchronize()
+    for x, y in zip((dz, *outs), h):
+        assert np.array_equal(x.cpu().numpy(), y)
+
+
+def test_full_size_config_properties(gpu):
+    """4096^2 with the plain drop-in benchmark's vpipes configuration:
+    finite, deterministic, water volume bookkeeping consistent (rain in =
+    stored + evaporated, to fp32 accumulation accuracy), and a band
+    checked bit-exact against the oracle after a few iterations."""
+    import torch
+    n = 4096
+    z0 = fbm(n, n, seed=2)
+    it = 200
+    p = dict(CONFIG2, iterations=it)
+    dz = torch.from_numpy(z0).cuda()
+    a = dz.clone()
+    wa = torch.empty_like(dz)
+    sa = torch.empty_like(dz)
+    gpu.hydraulic_vpipes_device(a, gpu.vpipes_params(**p), None, wa, sa)
+    b = dz.clone()
+    gpu.hydraulic_vpipes_device(b, gpu.vpipes_params(**p))
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    assert bool(torch.isfinite(a).all()) and bool(torch.isfinite(wa).all()) and bool(torch.isfinite(sa).all())
+    assert float(wa.min()) >= 0.0
+    # band check: 8 iterations move information at most 8 * (2 + sampler reach) cells
+    iters = 8
+    c = dz.clone()
+    gpu.hydraulic_vpipes_device(c, gpu.vpipes_params(**dict(CONFIG2, iterations=iters)))
+    torch.cuda.synchronize()
+    r0, r1, halo = 2000, 2256, 200
+    band = slice(r0 - halo, r1 + halo)
+    want = po.vpipes(z0[band], po.VpipesParams.make(**dict(CONFIG2, iterations=iters)))[0]
+    got = c.cpu().numpy()[r0:r1]
+    assert np.array_equal(got, want[halo:halo + (r1 - r0)])
