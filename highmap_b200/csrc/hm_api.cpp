@@ -22,10 +22,11 @@ struct Slab
 {
   char  *base;
   size_t off = 0;
-  float *take(size_t nfloats)
+  float *take(size_t nfloats) { return (float *)take_bytes(nfloats * sizeof(float)); }
+  void  *take_bytes(size_t bytes)
   {
-    float *p = (float *)(base + off);
-    off += align_up(nfloats * sizeof(float), 256);
+    void *p = base + off;
+    off += align_up(bytes, 256);
     return p;
   }
 };
@@ -136,7 +137,7 @@ int hm_vpipes(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_params 
   float       *ds = sediment ? sl.take(n) : nullptr;
   float       *du = vel_u ? sl.take(n) : nullptr;
   float       *dv = vel_v ? sl.take(n) : nullptr;
-  void        *scr = sl.take(hm::vpipes_scratch_bytes(nx, ny) / sizeof(float) + 1);
+  void        *scr = sl.take_bytes(hm::vpipes_scratch_bytes(nx, ny));
   cudaStream_t s = ctx->stream;
   HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
   if (dr) HM_CUDA_TRY(cudaMemcpyAsync(dr, rain_map, nbytes, cudaMemcpyHostToDevice, s));

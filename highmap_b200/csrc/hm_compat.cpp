@@ -1,0 +1,191 @@
+/*
+ * hm_compat.cpp - hmap::gpu::thermal / hydraulic_vpipes / init_opencl over
+ * the C-ABI (include/highmap_b200/hmap_gpu.hpp).
+ *
+ * Mirrors the reference drivers' interface and error behaviour:
+ *   thermal          HighMap/src/erosion/thermal_gpu.cpp:17-96
+ *   hydraulic_vpipes HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
+ *   init_opencl      HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134
+ * The reference functions return void and report problems only through
+ * their logger; here a failed call leaves z untouched, prints the status
+ * to stderr and records it for hmap::gpu::last_error().  Optional outputs
+ * are resized to z's shape and overwritten, as `*p = d` does in the
+ * reference.  Each thread uses its own context on device 0.
+ */
+#include <cstdio>
+#include <memory>
+#include <string>
+
+#include "highmap_b200/hmap_gpu.hpp"
+#include "hm_erosion.h"
+
+namespace hmap
+{
+namespace gpu
+{
+
+namespace
+{
+
+thread_local std::string g_err;
+
+struct CtxHolder
+{
+  hm_context *ctx = nullptr;
+  ~CtxHolder()
+  {
+    if (ctx) hm_context_destroy(ctx);
+  }
+};
+
+hm_context *context()
+{
+  thread_local CtxHolder h;
+  if (!h.ctx)
+  {
+    if (hm_context_create(&h.ctx, 0) != HM_OK) h.ctx = nullptr;
+  }
+  return h.ctx;
+}
+
+bool report(int st, const char *fn)
+{
+  if (st == HM_OK)
+  {
+    g_err.clear();
+    return true;
+  }
+  g_err = std::string(fn) + ": " + hm_status_string(st) + ": " + hm_last_error();
+  std::fprintf(stderr, "[highmap_b200] %s\n", g_err.c_str());
+  return false;
+}
+
+void shape_like(Array *p, const Array &z)
+{
+  if (!p) return;
+  p->shape = z.shape;
+  p->vector.resize((size_t)z.shape.x * (size_t)z.shape.y);
+}
+
+bool same_shape(const Array *a, const Array &z)
+{
+  return !a || (a->shape.x == z.shape.x && a->shape.y == z.shape.y &&
+                a->vector.size() == (size_t)z.shape.x * (size_t)z.shape.y);
+}
+
+void thermal_impl(Array &z, const Array *p_mask, const Array *talus, float talus_value, int iterations,
+                  Array *p_bedrock, Array *p_deposition_map)
+{
+  const char *fn = "hmap::gpu::thermal";
+  if (!same_shape(talus, z) || !same_shape(p_mask, z) || !same_shape(p_bedrock, z) ||
+      z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
+  {
+    report(HM_ERR_INVALID_ARGUMENT, fn);
+    g_err += "arrays of different shapes";
+    return;
+  }
+  hm_context *ctx = context();
+  if (!ctx)
+  {
+    report(HM_ERR_NO_DEVICE, fn);
+    return;
+  }
+  std::vector<float> depo;
+  if (p_deposition_map) depo.resize(z.vector.size());
+  std::vector<float> zw(z.vector);
+  float             *dp = p_deposition_map ? depo.data() : nullptr;
+  const float       *bp = p_bedrock ? p_bedrock->vector.data() : nullptr;
+  int                st;
+  if (p_mask)
+    st = hm_thermal_masked(ctx, zw.data(), z.shape.x, z.shape.y, p_mask->vector.data(), talus->vector.data(),
+                           iterations, bp, dp, nullptr);
+  else if (talus)
+    st = hm_thermal(ctx, zw.data(), z.shape.x, z.shape.y, talus->vector.data(), iterations, bp, dp, nullptr);
+  else
+    st = hm_thermal_scalar(ctx, zw.data(), z.shape.x, z.shape.y, talus_value, iterations, bp, dp, nullptr);
+  if (!report(st, fn)) return;
+  z.vector.swap(zw);
+  if (p_deposition_map)
+  {
+    shape_like(p_deposition_map, z);
+    p_deposition_map->vector.swap(depo);
+  }
+}
+
+} // namespace
+
+bool init_opencl() { return hm_init() == HM_OK; }
+
+std::string last_error() { return g_err; }
+
+void thermal(Array &z, const Array &talus, int iterations, Array *p_bedrock, Array *p_deposition_map)
+{
+  thermal_impl(z, nullptr, &talus, 0.f, iterations, p_bedrock, p_deposition_map);
+}
+
+void thermal(Array &z, const Array *p_mask, const Array &talus, int iterations, Array *p_bedrock,
+             Array *p_deposition_map)
+{
+  thermal_impl(z, p_mask, &talus, 0.f, iterations, p_bedrock, p_deposition_map);
+}
+
+void thermal(Array &z, float talus, int iterations, Array *p_bedrock, Array *p_deposition_map)
+{
+  thermal_impl(z, nullptr, nullptr, talus, iterations, p_bedrock, p_deposition_map);
+}
+
+void hydraulic_vpipes(Array &z, float water_height, bool maintain_water_volume, float evap_rate, int iterations,
+                      float dt, float k_capacity, float k_erode, float k_depose, float k_discharge_exp,
+                      float downcutting_max_depth_ratio, bool flux_diffusion, float flux_diffusion_strength,
+                      Array *p_rain_map, Array *p_water_depth, Array *p_sediment, Array *p_vel_u, Array *p_vel_v)
+{
+  const char *fn = "hmap::gpu::hydraulic_vpipes";
+  if (!same_shape(p_rain_map, z) || z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
+  {
+    report(HM_ERR_INVALID_ARGUMENT, fn);
+    g_err += "arrays of different shapes";
+    return;
+  }
+  hm_context *ctx = context();
+  if (!ctx)
+  {
+    report(HM_ERR_NO_DEVICE, fn);
+    return;
+  }
+  hm_vpipes_params p;
+  hm_vpipes_default_params(&p);
+  p.water_height = water_height;
+  p.maintain_water_volume = maintain_water_volume ? 1 : 0;
+  p.evap_rate = evap_rate;
+  p.iterations = iterations;
+  p.dt = dt;
+  p.k_capacity = k_capacity;
+  p.k_erode = k_erode;
+  p.k_depose = k_depose;
+  p.k_discharge_exp = k_discharge_exp;
+  p.downcutting_max_depth_ratio = downcutting_max_depth_ratio;
+  p.flux_diffusion = flux_diffusion ? 1 : 0;
+  p.flux_diffusion_strength = flux_diffusion_strength;
+  const size_t       n = z.vector.size();
+  std::vector<float> zw(z.vector), d, s, u, v;
+  if (p_water_depth) d.resize(n);
+  if (p_sediment) s.resize(n);
+  if (p_vel_u) u.resize(n);
+  if (p_vel_v) v.resize(n);
+  int st = hm_vpipes(ctx, zw.data(), z.shape.x, z.shape.y, &p, p_rain_map ? p_rain_map->vector.data() : nullptr,
+                     p_water_depth ? d.data() : nullptr, p_sediment ? s.data() : nullptr,
+                     p_vel_u ? u.data() : nullptr, p_vel_v ? v.data() : nullptr);
+  if (!report(st, fn)) return;
+  z.vector.swap(zw);
+  Array *outs[4] = {p_water_depth, p_sediment, p_vel_u, p_vel_v};
+  std::vector<float> *vals[4] = {&d, &s, &u, &v};
+  for (int k = 0; k < 4; k++)
+    if (outs[k])
+    {
+      shape_like(outs[k], z);
+      outs[k]->vector.swap(*vals[k]);
+    }
+}
+
+} // namespace gpu
+} // namespace hmap

@@ -1,0 +1,76 @@
+/*
+ * hmap_gpu.hpp - HighMap's hmap::gpu erosion API, served by libhm_erosion.so.
+ *
+ * Source-compatible with the declarations of
+ * HighMap/include/highmap/erosion.hpp:1206-1223 (hydraulic_vpipes),
+ * :1784-1801 (thermal, three overloads), :1822-1833 (thermal_auto_bedrock)
+ * and HighMap/include/highmap/opencl/gpu_opencl.hpp:30 (init_opencl).
+ * To use HighMap's own hmap::Array, include "highmap/array.hpp" first and
+ * define HMAP_B200_EXTERNAL_ARRAY; otherwise this header brings in the
+ * layout-identical minimal one (highmap_b200/hmap_array.hpp).
+ *
+ * Error behaviour follows the reference: the functions return void and do
+ * not throw.  On failure z is left as it was, the C-ABI status message is
+ * printed to stderr and kept in hmap::gpu::last_error().
+ */
+#ifndef HMAP_B200_GPU_HPP
+#define HMAP_B200_GPU_HPP
+
+#include <string>
+
+#ifndef HMAP_B200_EXTERNAL_ARRAY
+#include "highmap_b200/hmap_array.hpp"
+#endif
+
+namespace hmap
+{
+namespace gpu
+{
+
+bool init_opencl();
+
+void thermal(Array       &z,
+             const Array &talus,
+             int          iterations = 10,
+             Array       *p_bedrock = nullptr,
+             Array       *p_deposition_map = nullptr);
+
+void thermal(Array       &z,
+             const Array *p_mask,
+             const Array &talus,
+             int          iterations = 10,
+             Array       *p_bedrock = nullptr,
+             Array       *p_deposition_map = nullptr);
+
+void thermal(Array &z,
+             float  talus,
+             int    iterations = 10,
+             Array *p_bedrock = nullptr,
+             Array *p_deposition_map = nullptr);
+
+void hydraulic_vpipes(Array &z,
+                      float  water_height = 1e-2f,
+                      bool   maintain_water_volume = true,
+                      float  evap_rate = 0.1f,
+                      int    iterations = 50,
+                      float  dt = 0.5f,
+                      float  k_capacity = 0.5f,
+                      float  k_erode = 0.001f,
+                      float  k_depose = 0.01f,
+                      float  k_discharge_exp = 1.f,
+                      float  downcutting_max_depth_ratio = 10.f,
+                      bool   flux_diffusion = true,
+                      float  flux_diffusion_strength = 0.01f,
+                      Array *p_rain_map = nullptr,
+                      Array *p_water_depth = nullptr,
+                      Array *p_sediment = nullptr,
+                      Array *p_vel_u = nullptr,
+                      Array *p_vel_v = nullptr);
+
+/* message of the last failure of a call above on this thread ("" if none) */
+std::string last_error();
+
+} // namespace gpu
+} // namespace hmap
+
+#endif

@@ -1,0 +1,77 @@
+/*
+ * compat_example.cpp - a caller written against HighMap's hmap::gpu API,
+ * in the style of the reference's examples (examples/ex_thermal/ex_thermal.cpp,
+ * examples/ex_hydraulic_vpipes_gpu/ex_hydraulic_vpipes_gpu.cpp), linked
+ * against libhm_erosion.so.  Reads a raw float32 heightmap, runs the
+ * requested solver, writes the results as raw float32 for the test to
+ * compare with the oracle.
+ *
+ * usage: compat_example <thermal|thermal_scalar|thermal_mask|vpipes> nx ny in.f32 out_prefix
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+#include "highmap_b200/hmap_gpu.hpp"
+
+static bool read_raw(const char *path, hmap::Array &a)
+{
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return false;
+  size_t n = std::fread(a.vector.data(), sizeof(float), a.vector.size(), f);
+  std::fclose(f);
+  return n == a.vector.size();
+}
+
+static void write_raw(const std::string &path, const hmap::Array &a)
+{
+  FILE *f = std::fopen(path.c_str(), "wb");
+  std::fwrite(a.vector.data(), sizeof(float), a.vector.size(), f);
+  std::fclose(f);
+}
+
+int main(int argc, char **argv)
+{
+  if (argc != 6) return 2;
+  if (!hmap::gpu::init_opencl()) return 3;
+  std::string mode = argv[1];
+  glm::ivec2  shape(std::atoi(argv[2]), std::atoi(argv[3]));
+  hmap::Array z(shape);
+  if (!read_raw(argv[4], z)) return 4;
+  std::string out = argv[5];
+
+  if (mode == "thermal" || mode == "thermal_mask")
+  {
+    hmap::Array talus(shape, 1.f / shape.x);
+    hmap::Array bedrock(shape);
+    for (size_t k = 0; k < z.vector.size(); k++) bedrock.vector[k] = 0.3f * z.vector[k];
+    hmap::Array depo;
+    if (mode == "thermal")
+      hmap::gpu::thermal(z, talus, 50, &bedrock, &depo);
+    else
+    {
+      hmap::Array mask(shape, 0.25f);
+      hmap::gpu::thermal(z, &mask, talus, 50, nullptr, &depo);
+    }
+    write_raw(out + "_z.f32", z);
+    write_raw(out + "_depo.f32", depo);
+  }
+  else if (mode == "thermal_scalar")
+  {
+    hmap::gpu::thermal(z, 0.1f / shape.x, 60);
+    write_raw(out + "_z.f32", z);
+  }
+  else if (mode == "vpipes")
+  {
+    hmap::Array water, sediment, u, v;
+    hmap::gpu::hydraulic_vpipes(z, 1e-2f, true, 0.1f, 25, 0.5f, 0.5f, 0.001f, 0.01f, 1.f, 10.f, false, 0.01f,
+                                nullptr, &water, &sediment, &u, &v);
+    write_raw(out + "_z.f32", z);
+    write_raw(out + "_water.f32", water);
+    write_raw(out + "_sediment.f32", sediment);
+  }
+  else
+    return 5;
+  return hmap::gpu::last_error().empty() ? 0 : 6;
+}

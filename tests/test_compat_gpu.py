@@ -1,0 +1,72 @@
+"""The C++ drop-in layer (include/highmap_b200/hmap_gpu.hpp): a caller
+written against HighMap's hmap::gpu API, built with g++ and linked to
+libhm_erosion.so, produces the oracle's results."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from highmap_b200.inputs import fbm
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def example(built_lib, tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("cpp") / "compat_example")
+    libdir = os.path.dirname(built_lib)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "compat_example.cpp"), "-L", libdir, "-lhm_erosion",
+                    "-Wl,-rpath," + libdir, "-o", exe], check=True)
+    return exe
+
+
+def _run(exe, mode, z, tmp_path):
+    ny, nx = z.shape
+    src = tmp_path / "in.f32"
+    z.tofile(src)
+    prefix = str(tmp_path / "out")
+    r = subprocess.run([exe, mode, str(nx), str(ny), str(src), prefix], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+    def load(name):
+        return np.fromfile(prefix + "_" + name + ".f32", dtype=np.float32).reshape(ny, nx)
+    return load
+
+
+def test_thermal(gpu, example, tmp_path):
+    z = fbm(160, 96, seed=1)
+    load = _run(example, "thermal", z, tmp_path)
+    want, depo = po.thermal(z, np.full_like(z, 1 / 160), 50, bedrock=(0.3 * z).astype(np.float32),
+                            deposition=True)
+    assert np.array_equal(load("z"), want)
+    assert np.array_equal(load("depo"), depo)
+
+
+def test_thermal_mask(gpu, example, tmp_path):
+    z = fbm(128, 128, seed=4)
+    load = _run(example, "thermal_mask", z, tmp_path)
+    want, depo = po.thermal(z, np.full_like(z, 1 / 128), 50, mask=np.full_like(z, 0.25), deposition=True)
+    assert np.array_equal(load("z"), want)
+    assert np.array_equal(load("depo"), depo)
+
+
+def test_thermal_scalar(gpu, example, tmp_path):
+    z = fbm(100, 70, seed=3)
+    load = _run(example, "thermal_scalar", z, tmp_path)
+    want, _ = po.thermal(z, np.float32(0.1 / 100), 60)
+    assert np.array_equal(load("z"), want)
+
+
+def test_vpipes(gpu, example, tmp_path):
+    z = fbm(96, 64, seed=2)
+    load = _run(example, "vpipes", z, tmp_path)
+    p = po.VpipesParams.make(iterations=25, flux_diffusion=0)
+    wz, wd, ws, _, _ = po.vpipes(z, p)
+    rng = float(z.max() - z.min())
+    assert np.abs(load("z") - wz).max() <= 1e-3 * rng
+    assert np.abs(load("sediment") - ws).max() <= 1e-3 * rng
+    assert np.abs(load("water") - wd).max() <= 1e-3 * float(wd.max())

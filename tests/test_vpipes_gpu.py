@@ -1,11 +1,14 @@
 """GPU parity of the virtual-pipes solver against the oracle, via the C-ABI.
 
 Bit-exact where both sides evaluate the same fp32 operations (every case
-without the water-volume top-up: the GPU reproduces the reference's
-one-rounding-per-operation arithmetic, fp64 hypot included).  With
-maintain_water_volume the grid-wide fp64 sum is reduced in a different
-order on the two sides; there the bar is the north-star tolerance (max abs
-error <= 1e-3 of the height range) on z and sediment.
+without the water-volume top-up and with discharge exponent 1: the GPU
+reproduces the reference's one-rounding-per-operation arithmetic, fp64
+hypot included).  Two cases differ by construction and are held to the
+north-star tolerance (max abs error <= 1e-3 of the height range) on z and
+sediment instead: maintain_water_volume, whose grid-wide fp64 sum is
+reduced in a different order on the two sides, and exponents other than 1,
+where the C library's powf (not correctly rounded) and the GPU's fp64 pow
+can differ in the last bit.
 """
 import json
 import os
@@ -53,7 +56,7 @@ def test_golden(gpu, name):
     p = json.loads(str(g["params"]))
     got = _run_gpu(gpu, g["z"], p, rain=g.get("rain_map"))
     want = tuple(g[k] for k in ("out_z", "out_water", "out_sediment", "out_u", "out_v"))
-    _check(got, want, g["z"], exact=not p["maintain_water_volume"])
+    _check(got, want, g["z"], exact=not p["maintain_water_volume"] and p["k_discharge_exp"] == 1.0)
 
 
 @pytest.mark.parametrize("shape", [(128, 128), (97, 131), (256, 64), (5, 300)])
@@ -101,9 +104,8 @@ def test_device_api_matches_host_api(gpu):
 
 def test_full_size_config_properties(gpu):
     """4096^2 with the plain drop-in benchmark's vpipes configuration:
-    finite, deterministic, water volume bookkeeping consistent (rain in =
-    stored + evaporated, to fp32 accumulation accuracy), and a band
-    checked bit-exact against the oracle after a few iterations."""
+    finite, deterministic, water depth non-negative, and a band checked
+    bit-exact against the oracle after a few iterations."""
     import torch
     n = 4096
     z0 = fbm(n, n, seed=2)
