@@ -122,13 +122,16 @@ def test_full_size_config_properties(gpu):
     assert torch.equal(a, b)
     assert bool(torch.isfinite(a).all()) and bool(torch.isfinite(wa).all()) and bool(torch.isfinite(sa).all())
     assert float(wa.min()) >= 0.0
-    # band check: 8 iterations move information at most 8 * (2 + sampler reach) cells
+    # band check: the top 712 rows run alone reach the same values in their
+    # first 512 rows after 8 iterations (influence of the band's artificial
+    # bottom edge travels about one row per iteration).  The band starts at
+    # row 0 so every cell keeps its coordinates: the advection pass samples at
+    # j - dt * v, whose rounding depends on the magnitude of j.
     iters = 8
     c = dz.clone()
     gpu.hydraulic_vpipes_device(c, gpu.vpipes_params(**dict(CONFIG2, iterations=iters)))
     torch.cuda.synchronize()
-    r0, r1, halo = 2000, 2256, 200
-    band = slice(r0 - halo, r1 + halo)
-    want = po.vpipes(z0[band], po.VpipesParams.make(**dict(CONFIG2, iterations=iters)))[0]
-    got = c.cpu().numpy()[r0:r1]
-    assert np.array_equal(got, want[halo:halo + (r1 - r0)])
+    rows, band = 512, 712
+    want = po.vpipes(z0[:band], po.VpipesParams.make(**dict(CONFIG2, iterations=iters)))[0]
+    got = c.cpu().numpy()[:rows]
+    assert np.array_equal(got, want[:rows])
