@@ -145,6 +145,31 @@ int hm_thermal_device(hm_context               *ctx,
                       const hm_thermal_options *opts,
                       void                     *stream);
 
+/* No counterpart in the reference (which allocates its OpenCL buffers on
+ * every call).  Thermal erosion on device buffers for callers that cannot
+ * allocate device memory when they run it (an application whose own pool
+ * allocator owns the device memory, or a loop that must not stall on
+ * cudaMalloc/cudaFree): the same solve as hm_thermal_device without the
+ * deposition map and mask, with the Jacobi scratch grid taken from a
+ * statically reserved device array of HM_NOALLOC_MAX_CELLS floats that
+ * every GPU loading the library holds until exit.  No allocation, no
+ * context.  Grids larger than HM_NOALLOC_MAX_CELLS cells are refused with
+ * HM_ERR_INVALID_ARGUMENT.  Runs on the calling thread's current device;
+ * the first call on a device looks up the array's address and should come
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller.  talus NULL selects
+ * talus_value; bedrock is nullable. */
+#define HM_NOALLOC_MAX_CELLS (1 << 22)
+int hm_thermal_device_noalloc(float       *z,
+                              int          nx,
+                              int          ny,
+                              const float *talus,
+                              float        talus_value,
+                              int          iterations,
+                              const float *bedrock,
+                              int          bedrock_mode,
+                              void        *stream);
+
 /* ---- virtual pipes ----------------------------------------------------- */
 
 typedef struct hm_vpipes_params

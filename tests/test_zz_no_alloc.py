@@ -1,0 +1,85 @@
+"""The no-allocation thermal entry point, hm_thermal_device_noalloc.
+
+It serves callers that cannot allocate device memory when they run
+erosion: an application whose own pool allocator owns the device memory,
+or a loop that must not stall on cudaMalloc/cudaFree.  Its Jacobi scratch
+grid is a statically reserved device array instead of workspace memory.
+
+Checked through the C-ABI against the allocating entry point
+hm_thermal_device on two calls in a row (the array keeps the first call's
+contents when the second starts), within the thermal tests' bar: max abs
+error <= 1e-4 of the height range, and bit-exact.  Also: a grid larger than
+the array is refused before any device work.  This file is collected last
+so a stop-at-first-failure run has already run every other test; it also
+passes on its own in a fresh process (the first call does the per-device
+set-up).
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from highmap_b200.inputs import fbm
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+TOL = 1e-4  # of the height range, as the thermal parity tests
+
+
+def _max_cells():
+    text = open(os.path.join(ROOT, "include", "hm_erosion.h")).read()
+    return eval(re.search(r"#define HM_NOALLOC_MAX_CELLS \((.*?)\)", text).group(1))
+
+
+def _p(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def test_noalloc_matches_allocating_entry_point(gpu):
+    import torch
+    from highmap_b200 import _lib as L
+
+    lib = L.lib()
+    ctx = gpu.Context(torch.cuda.current_device())
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    # two calls in a row: a talus map with bedrock, then a larger grid with a scalar talus
+    cases = [(512, 384, True, True, 41), (2048, 2048, False, False, 30)]
+    assert cases[1][0] * cases[1][1] <= _max_cells()
+    for nx, ny, tmap, bed, iters in cases:
+        z0 = torch.from_numpy(fbm(nx, ny, seed=nx + ny)).cuda()
+        talus = torch.from_numpy(((0.5 + fbm(nx, ny, seed=7)) / nx).astype(np.float32)).cuda() if tmap else None
+        tv = 0.0 if tmap else 1.0 / nx
+        bedrock = (0.3 * z0).contiguous() if bed else None
+        opts = gpu.thermal_options(gpu.BEDROCK_INTENDED)
+
+        want = z0.clone()
+        L.check(lib.hm_thermal_device(ctx.handle, _p(want), nx, ny, _p(talus), C.c_float(tv), iters, _p(bedrock),
+                                      None, None, C.byref(opts), stream))
+        got = z0.clone()
+        L.check(lib.hm_thermal_device_noalloc(_p(got), nx, ny, _p(talus), C.c_float(tv), iters, _p(bedrock),
+                                              gpu.BEDROCK_INTENDED, stream))
+        torch.cuda.synchronize()
+        rng = float(z0.max() - z0.min())
+        err = float((got - want).abs().max())
+        assert err <= TOL * rng, err
+        assert torch.equal(got, want)
+    ctx.close()
+
+
+def test_noalloc_refuses_oversized_grid(gpu):
+    import torch
+    from highmap_b200 import _lib as L
+
+    lib = L.lib()
+    nx, ny = 2049, 2048
+    assert nx * ny > _max_cells()
+    z = torch.rand((ny, nx), device="cuda")
+    before = z.clone()
+    st = lib.hm_thermal_device_noalloc(_p(z), nx, ny, None, C.c_float(0.01), 5, None, gpu.BEDROCK_INTENDED,
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert st == L.HM_ERR_INVALID_ARGUMENT
+    assert b"no-allocation limit" in lib.hm_last_error()
+    assert torch.equal(z, before)
