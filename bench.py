@@ -61,6 +61,8 @@ def _args():
     ap.add_argument("--size", type=int, default=N_SIDE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--vpipes-launch", default=None,
+                    help="fused vpipes launch shape 'tpb,radius,rows' (default: built-in choice)")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -285,6 +287,8 @@ def run_ours(a):
     if not G.init_opencl():
         raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
     ctx = G.Context(local)
+    if a.vpipes_launch:
+        G.vpipes_set_launch(*[int(x) for x in a.vpipes_launch.split(",")])
     n = a.size
     cells = float(n) * n
     z, talus, bed = _inputs(n)

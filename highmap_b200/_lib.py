@@ -30,7 +30,7 @@ EXPORTED = (
     "hm_thermal", "hm_thermal_scalar", "hm_thermal_masked", "hm_thermal_device",
     "hm_vpipes_default_params", "hm_vpipes", "hm_vpipes_device",
     "hm_launch_count", "hm_launch_count_reset",
-    "hm_thermal_device_noalloc",
+    "hm_thermal_device_noalloc", "hm_vpipes_set_launch",
 )
 
 
@@ -94,6 +94,7 @@ def _declare(lib):
     lib.hm_vpipes_device.argtypes = [vp, vp, i, i, vp, vp, vp, vp, vp, vp, vp]
     lib.hm_launch_count.restype = C.c_ulonglong
     lib.hm_thermal_device_noalloc.argtypes = [vp, i, i, vp, f, i, vp, i, vp]
+    lib.hm_vpipes_set_launch.argtypes = [i, i, i]
     for name in EXPORTED:
         getattr(lib, name)  # raises AttributeError if a symbol is missing
     return lib

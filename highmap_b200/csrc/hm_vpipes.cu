@@ -8,21 +8,17 @@
  * evaporation and volume top-up on the host; here all state stays in HBM
  * for the whole call and every step is device work only.
  *
- * State in HBM (fp32, nx*ny each, SoA): z (ping-pong with one workspace
- * grid), d (evaporated depth, before the volume top-up), s (sediment),
- * fl, fr, ft, fb (outflow fluxes), u, v (velocities), and s1 (sediment
- * after erosion, before advection).  The volume top-up (V0 - sum d) * rain
- * / R is applied lazily: the step that follows reads the stored depth plus
- * the top-up, and the grid-wide sum is a deterministic fp64 reduction
- * finished by the last block of the water/erosion kernel.
+ * State in HBM (fp32, nx*ny each, SoA), two copies that alternate between
+ * steps: z, d (evaporated depth, before the volume top-up), s (sediment)
+ * and fl, fr, ft, fb (outflow fluxes); copy A's z is the caller's z.  The
+ * volume top-up (V0 - sum d) * rain / R is applied lazily: the step that
+ * follows reads the stored depth plus the top-up, and the grid-wide sum is
+ * a deterministic fp64 reduction finished by the last block of the step.
  *
- * Kernels per step
- *   k_vp_flow          flow pass (:5-69); reads z, d (radius 1), f;
- *                      writes f in place.
- *   k_vp_water_erosion water pass (:71-116) and erosion pass (:118-184);
- *                      reads f (radius 1), d, z, s (radius 1); writes z',
- *                      s1, u, v, d.
- *   k_vp_transport     advection (:186-211): s = bilinear(s1, x - dt u).
+ * Kernels
+ *   k_vp_init          initial depth, zero sediment and fluxes, V0 and R.
+ *   k_vp_fused         one whole step (hm_vpipes_fused.cuh).
+ *   k_vp_final_depth   water-depth output with the last top-up applied.
  */
 #include <cuda_runtime.h>
 
@@ -31,40 +27,33 @@
 #include "hm_internal.h"
 #include "hm_reduce.cuh"
 #include "hm_vpipes.h"
+#include "hm_vpipes_fused.cuh"
 #include "hm_vpipes_math.cuh"
 
 namespace hm
 {
 
-struct VpScalars
-{
-  float    v0;     /* initial water volume (float of the fp64 sum)  */
-  float    rvol;   /* rain map volume                               */
-  float    add[2]; /* V0 - sum(d) of the previous step, ping-pong   */
-  unsigned ticket;
-  unsigned pad[3];
-};
+constexpr int VP_NT = 256;
+constexpr unsigned VP_INIT_BLOCKS = 296;
 
-constexpr int VP_BX = 64;
-constexpr int VP_BY = 4;
-constexpr int VP_NT = VP_BX * VP_BY;
-
+/* one copy of the solver state (SoA grids) */
 struct VpFields
 {
-  float *z, *zn, *d, *s, *s1, *fl, *fr, *ft, *fb, *u, *v;
-  const float *rain; /* nullable */
+  float *z, *d, *s, *fl, *fr, *ft, *fb;
 };
 
 /* ---- init --------------------------------------------------------- */
 
+/* d = initial depth * rain, s = f = 0; fp64 partial sums of d and rain
+ * (hydraulic_vpipes_gpu.cpp:36-55). */
 __global__ void __launch_bounds__(VP_NT)
-    k_vp_init(VpFields f, size_t n, float init_depth, VpScalars *sc, double *partials)
+    k_vp_init(VpFields f, const float *rain, size_t n, float init_depth, double *partials)
 {
   const unsigned bid = blockIdx.x;
   double         sd = 0.0, sr = 0.0;
   for (size_t k = bid * (size_t)VP_NT + threadIdx.x; k < n; k += (size_t)gridDim.x * VP_NT)
   {
-    float r = f.rain ? f.rain[k] : 1.f;
+    float r = rain ? rain[k] : 1.f;
     float d = fmul(init_depth, r);
     f.d[k] = d;
     f.s[k] = 0.f;
@@ -72,12 +61,9 @@ __global__ void __launch_bounds__(VP_NT)
     f.fr[k] = 0.f;
     f.ft[k] = 0.f;
     f.fb[k] = 0.f;
-    f.u[k] = 0.f;
-    f.v[k] = 0.f;
     sd += (double)d;
     sr += (double)r;
   }
-  /* two sums: partials[0 .. G) for d, partials[G .. 2G) for rain */
   __shared__ double sm[VP_NT / 32];
   double            bd = block_sum<VP_NT>(sd, sm);
   double            br = block_sum<VP_NT>(sr, sm);
@@ -106,113 +92,15 @@ __global__ void __launch_bounds__(VP_NT) k_vp_init_finish(VpScalars *sc, const d
     sc->add[0] = 0.f;
     sc->add[1] = 0.f;
     sc->ticket = 0u;
+    sc->slow = 0u;
+    sc->defer_count[0] = 0u;
+    sc->defer_count[1] = 0u;
   }
-}
-
-/* ---- flow pass ------------------------------------------------------ */
-
-template <bool MAINTAIN, bool DIFFUSION, bool PL_ONE>
-__global__ void __launch_bounds__(VP_NT)
-    k_vp_flow(VpFields f, VpConst c, const VpScalars *__restrict__ sc, int parity)
-{
-  const int i = blockIdx.x * VP_BX + threadIdx.x;
-  const int j = blockIdx.y * VP_BY + threadIdx.y;
-  if (i >= c.nx || j >= c.ny) return;
-  const int   nx = c.nx;
-  const int   im = i > 0 ? i - 1 : 0, ip = i < nx - 1 ? i + 1 : nx - 1;
-  const int   jm = j > 0 ? j - 1 : 0, jp = j < c.ny - 1 ? j + 1 : c.ny - 1;
-  const float add = MAINTAIN ? sc->add[parity] : 0.f;
-  const float rvol = MAINTAIN ? sc->rvol : 1.f;
-  const bool  rain_step = c.rps != 0.f;
-
-  auto d1 = [&](int ii, int jj) -> float
-  {
-    size_t k = (size_t)jj * nx + ii;
-    float  r = f.rain ? __ldg(f.rain + k) : 1.f;
-    float  dd = __ldg(f.d + k);
-    return rain_step ? depth_d1<MAINTAIN, true>(dd, r, add, rvol, c.rps)
-                     : depth_d1<MAINTAIN, false>(dd, r, add, rvol, c.rps);
-  };
-  auto zz = [&](int ii, int jj) -> float { return __ldg(f.z + (size_t)jj * nx + ii); };
-
-  const size_t k = (size_t)j * nx + i;
-  float        fl = f.fl[k], fr = f.fr[k], ft = f.ft[k], fb = f.fb[k];
-  flow_cell<DIFFUSION, PL_ONE>(c, zz(i, j), d1(i, j), zz(im, j), d1(im, j), zz(ip, j), d1(ip, j),
-                               zz(i, jp), d1(i, jp), zz(i, jm), d1(i, jm), fl, fr, ft, fb);
-  f.fl[k] = fl;
-  f.fr[k] = fr;
-  f.ft[k] = ft;
-  f.fb[k] = fb;
-}
-
-/* ---- water + erosion ------------------------------------------------ */
-
-template <bool MAINTAIN, bool PL_ONE, bool KEXP_ONE>
-__global__ void __launch_bounds__(VP_NT)
-    k_vp_water_erosion(VpFields f, VpConst c, VpScalars *sc, int parity, double *partials)
-{
-  const int i = blockIdx.x * VP_BX + threadIdx.x;
-  const int j = blockIdx.y * VP_BY + threadIdx.y;
-  const int nx = c.nx;
-  double    part = 0.0;
-  if (i < nx && j < c.ny)
-  {
-    const int    im = i > 0 ? i - 1 : 0, ip = i < nx - 1 ? i + 1 : nx - 1;
-    const int    jm = j > 0 ? j - 1 : 0, jp = j < c.ny - 1 ? j + 1 : c.ny - 1;
-    const size_t k = (size_t)j * nx + i;
-    const float  add = MAINTAIN ? sc->add[parity] : 0.f;
-    const float  rvol = MAINTAIN ? sc->rvol : 1.f;
-    const float  r = f.rain ? __ldg(f.rain + k) : 1.f;
-    const float  d1c = c.rps != 0.f ? depth_d1<MAINTAIN, true>(__ldg(f.d + k), r, add, rvol, c.rps)
-                                    : depth_d1<MAINTAIN, false>(__ldg(f.d + k), r, add, rvol, c.rps);
-    float d2, u, v;
-    water_cell<PL_ONE>(c, d1c, __ldg(f.fl + k), __ldg(f.fr + k), __ldg(f.ft + k), __ldg(f.fb + k),
-                       __ldg(f.fr + (size_t)j * nx + im), __ldg(f.fl + (size_t)j * nx + ip),
-                       __ldg(f.ft + (size_t)jm * nx + i), __ldg(f.fb + (size_t)jp * nx + i), d2, u, v);
-    const float *z = f.z, *s = f.s;
-    float        zo, so;
-    erosion_cell<KEXP_ONE>(c, __ldg(z + k), __ldg(s + k), __ldg(z + (size_t)j * nx + im),
-                           __ldg(z + (size_t)j * nx + ip), __ldg(z + (size_t)jm * nx + i),
-                           __ldg(z + (size_t)jp * nx + i), __ldg(s + (size_t)j * nx + im),
-                           __ldg(s + (size_t)j * nx + ip), __ldg(s + (size_t)jm * nx + i),
-                           __ldg(s + (size_t)jp * nx + i), d2, u, v, zo, so);
-    const float de = fmul(d2, c.keep);
-    f.zn[k] = zo;
-    f.s1[k] = so;
-    f.u[k] = u;
-    f.v[k] = v;
-    f.d[k] = de;
-    part = (double)de;
-  }
-  if (MAINTAIN)
-  {
-    const unsigned nb = gridDim.x * gridDim.y;
-    const unsigned bid = blockIdx.y * gridDim.x + blockIdx.x;
-    const float    v0 = sc->v0;
-    float         *out = &sc->add[parity ^ 1];
-    grid_sum_commit<VP_NT>(part, partials, &sc->ticket, nb, bid,
-                           [&](double total) { *out = fsub(v0, (float)total); });
-  }
-}
-
-/* ---- advection ------------------------------------------------------ */
-
-__global__ void __launch_bounds__(VP_NT) k_vp_transport(VpFields f, VpConst c)
-{
-  const int i = blockIdx.x * VP_BX + threadIdx.x;
-  const int j = blockIdx.y * VP_BY + threadIdx.y;
-  if (i >= c.nx || j >= c.ny) return;
-  const size_t k = (size_t)j * c.nx + i;
-  const float  x = fsub((float)i, fmul(c.dt, __ldg(f.u + k)));
-  const float  y = fsub((float)j, fmul(c.dt, __ldg(f.v + k)));
-  const Tap    t = linear_tap(x, y, c.nx, c.ny);
-  const float *s1 = f.s1;
-  const size_t r0 = (size_t)t.j0 * c.nx, r1 = (size_t)t.j1 * c.nx;
-  f.s[k] = blend(t, __ldg(s1 + r0 + t.i0), __ldg(s1 + r0 + t.i1), __ldg(s1 + r1 + t.i0), __ldg(s1 + r1 + t.i1));
 }
 
 /* ---- outputs -------------------------------------------------------- */
 
+/* water depth output: the stored depth plus the last step's top-up */
 template <bool MAINTAIN>
 __global__ void k_vp_final_depth(const float *__restrict__ d,
                                  const float *__restrict__ rain,
@@ -234,6 +122,39 @@ __global__ void k_vp_final_depth(const float *__restrict__ d,
 /* host side                                                          */
 /* ------------------------------------------------------------------ */
 
+/* launch shapes of the fused step kernel (threads per CTA = strip width
+ * including the halo, sampler radius R) */
+struct FusedCfg
+{
+  int tpb, r, h;
+};
+
+static FusedCfg g_cfg_override = {0, 0, 0};
+
+FusedCfg vpipes_pick_config(int nx, int ny)
+{
+  if (g_cfg_override.tpb) return g_cfg_override;
+  (void)nx;
+  (void)ny;
+  return FusedCfg{128, 3, 128};
+}
+
+static int fused_w(const FusedCfg &c) { return c.tpb - 2 * (c.r + 2); }
+
+static dim3 fused_grid(const FusedCfg &c, int nx, int ny)
+{
+  const int w = fused_w(c);
+  return dim3((nx + w - 1) / w, (ny + c.h - 1) / c.h);
+}
+
+static size_t partials_bytes(int nx, int ny)
+{
+  /* the smallest strip and chunk any configuration uses bound the grid */
+  size_t blocks = (size_t)((nx + 63) / 64 + 1) * ((ny + 31) / 32 + 1);
+  if (blocks < 2 * VP_INIT_BLOCKS) blocks = 2 * VP_INIT_BLOCKS;
+  return align_up(blocks * sizeof(double), 256);
+}
+
 int vpipes_check_args(const float *z, int nx, int ny, const hm_vpipes_params *p)
 {
   if (!z) return fail(HM_ERR_INVALID_ARGUMENT, "vpipes: z is NULL");
@@ -246,21 +167,21 @@ int vpipes_check_args(const float *z, int nx, int ny, const hm_vpipes_params *p)
   return HM_OK;
 }
 
-constexpr unsigned VP_INIT_BLOCKS = 296;
-
-/* fp64 partial sums: one per block of the step grid, and two per block of
- * the init grid */
-static size_t partials_bytes(int nx, int ny)
+/* capacity of the deferred-advection list (cells per step); a step that
+ * defers more cells resolves the excess inline */
+static size_t defer_cap(int nx, int ny)
 {
-  size_t grid_blocks = (size_t)((nx + VP_BX - 1) / VP_BX) * ((ny + VP_BY - 1) / VP_BY);
-  if (grid_blocks < 2 * VP_INIT_BLOCKS) grid_blocks = 2 * VP_INIT_BLOCKS;
-  return align_up(grid_blocks * sizeof(double), 256);
+  size_t cap = (size_t)nx * ny / 32;
+  return cap < 4096 ? 4096 : cap;
 }
 
 size_t vpipes_scratch_bytes(int nx, int ny)
 {
   const size_t n = align_up((size_t)nx * ny, 64);
-  return n * sizeof(float) * 10 + partials_bytes(nx, ny) + align_up(sizeof(VpScalars), 256);
+  /* state copy B (7 grids), state A's d, s and fluxes (6 grids), u and v,
+   * fp64 partials, the scalar block, the deferred list */
+  return n * sizeof(float) * 15 + partials_bytes(nx, ny) + align_up(sizeof(VpScalars), 256) +
+         align_up(defer_cap(nx, ny) * sizeof(Deferred), 256);
 }
 
 VpConst vpipes_consts(int nx, int ny, const hm_vpipes_params &p)
@@ -288,36 +209,39 @@ VpConst vpipes_consts(int nx, int ny, const hm_vpipes_params &p)
   return c;
 }
 
-template <bool M>
-static void launch_flow(const VpFields &f, const VpConst &c, const VpScalars *sc, int parity, bool diff,
-                        bool pl1, dim3 g, dim3 b, cudaStream_t s)
+template <int TPB, int R>
+static int launch_fused(const VpStep &st, const VpConst &c, VpScalars *sc, double *partials, const VpDefer &df,
+                        dim3 grid, cudaStream_t s)
 {
-  if (diff)
+  using L = FusedLayout<TPB, R>;
+  static bool attr_set[64] = {};
+  int         dev = 0;
+  HM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !attr_set[dev])
   {
-    if (pl1) k_vp_flow<M, true, true><<<g, b, 0, s>>>(f, c, sc, parity);
-    else k_vp_flow<M, true, false><<<g, b, 0, s>>>(f, c, sc, parity);
+    HM_CUDA_TRY(cudaFuncSetAttribute(k_vp_fused<TPB, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)L::SMEM));
+    HM_CUDA_TRY(cudaFuncSetAttribute(k_vp_fused<TPB, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)L::SMEM));
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
   }
-  else
-  {
-    if (pl1) k_vp_flow<M, false, true><<<g, b, 0, s>>>(f, c, sc, parity);
-    else k_vp_flow<M, false, false><<<g, b, 0, s>>>(f, c, sc, parity);
-  }
+  if (st.maintain) k_vp_fused<TPB, R, true><<<grid, TPB, L::SMEM, s>>>(st, c, sc, partials, df);
+  else k_vp_fused<TPB, R, false><<<grid, TPB, L::SMEM, s>>>(st, c, sc, partials, df);
+  HM_LAUNCH_CHECK("k_vp_fused");
+  k_vp_fixup<128><<<2 * 148, 128, 0, s>>>(st, c, sc, df);
+  HM_LAUNCH_CHECK("k_vp_fixup");
+  return HM_OK;
 }
 
-template <bool M>
-static void launch_we(const VpFields &f, const VpConst &c, VpScalars *sc, int parity, double *partials, bool pl1,
-                      bool k1, dim3 g, dim3 b, cudaStream_t s)
+static int launch_step(const FusedCfg &cfg, const VpStep &st, const VpConst &c, VpScalars *sc, double *partials,
+                       const VpDefer &df, cudaStream_t s)
 {
-  if (pl1)
-  {
-    if (k1) k_vp_water_erosion<M, true, true><<<g, b, 0, s>>>(f, c, sc, parity, partials);
-    else k_vp_water_erosion<M, true, false><<<g, b, 0, s>>>(f, c, sc, parity, partials);
-  }
-  else
-  {
-    if (k1) k_vp_water_erosion<M, false, true><<<g, b, 0, s>>>(f, c, sc, parity, partials);
-    else k_vp_water_erosion<M, false, false><<<g, b, 0, s>>>(f, c, sc, parity, partials);
-  }
+  const dim3 grid = fused_grid(cfg, c.nx, c.ny);
+  if (cfg.tpb == 128 && cfg.r == 2) return launch_fused<128, 2>(st, c, sc, partials, df, grid, s);
+  if (cfg.tpb == 256 && cfg.r == 2) return launch_fused<256, 2>(st, c, sc, partials, df, grid, s);
+  if (cfg.tpb == 128 && cfg.r == 3) return launch_fused<128, 3>(st, c, sc, partials, df, grid, s);
+  if (cfg.tpb == 256 && cfg.r == 3) return launch_fused<256, 3>(st, c, sc, partials, df, grid, s);
+  return fail(HM_ERR_INVALID_ARGUMENT, "vpipes: unsupported fused configuration");
 }
 
 int vpipes_core(float *z,
@@ -335,69 +259,98 @@ int vpipes_core(float *z,
   const size_t n = (size_t)nx * ny;
   const size_t na = align_up(n, 64);
   float       *base = (float *)scratch_buf;
-  VpFields     f;
-  f.z = z;
-  f.zn = base + 0 * na;
-  f.d = base + 1 * na;
-  f.s = base + 2 * na;
-  f.s1 = base + 3 * na;
-  f.fl = base + 4 * na;
-  f.fr = base + 5 * na;
-  f.ft = base + 6 * na;
-  f.fb = base + 7 * na;
-  f.u = base + 8 * na;
-  f.v = base + 9 * na;
-  f.rain = rain;
-  double      *partials = (double *)(base + 10 * na);
-  VpScalars   *sc = (VpScalars *)((char *)partials + partials_bytes(nx, ny));
+  VpFields     A, B;
+  A.z = z;
+  A.d = base + 0 * na;
+  A.s = base + 1 * na;
+  A.fl = base + 2 * na;
+  A.fr = base + 3 * na;
+  A.ft = base + 4 * na;
+  A.fb = base + 5 * na;
+  B.z = base + 6 * na;
+  B.d = base + 7 * na;
+  B.s = base + 8 * na;
+  B.fl = base + 9 * na;
+  B.fr = base + 10 * na;
+  B.ft = base + 11 * na;
+  B.fb = base + 12 * na;
+  float     *u_buf = base + 13 * na, *v_buf = base + 14 * na;
+  double    *partials = (double *)(base + 15 * na);
+  VpScalars *sc = (VpScalars *)((char *)partials + partials_bytes(nx, ny));
+  VpDefer    df;
+  df.list = (Deferred *)((char *)sc + align_up(sizeof(VpScalars), 256));
+  df.count = sc->defer_count;
+  df.cap = (unsigned)defer_cap(nx, ny);
 
   const VpConst c = vpipes_consts(nx, ny, p);
   const float   init_depth = p.initial_water < 0.f ? p.water_height : p.initial_water;
 
-  /* init: fields and the two volumes (deterministic: fixed grid) */
-  const unsigned gi = VP_INIT_BLOCKS;
-  k_vp_init<<<gi, VP_NT, 0, s>>>(f, n, init_depth, sc, partials);
+  k_vp_init<<<VP_INIT_BLOCKS, VP_NT, 0, s>>>(A, rain, n, init_depth, partials);
   HM_LAUNCH_CHECK("k_vp_init");
-  k_vp_init_finish<<<1, VP_NT, 0, s>>>(sc, partials, gi);
+  k_vp_init_finish<<<1, VP_NT, 0, s>>>(sc, partials, VP_INIT_BLOCKS);
   HM_LAUNCH_CHECK("k_vp_init_finish");
 
-  const dim3 b(VP_BX, VP_BY);
-  const dim3 g((nx + VP_BX - 1) / VP_BX, (ny + VP_BY - 1) / VP_BY);
-  const bool maintain = p.maintain_water_volume != 0;
-  const bool diff = p.flux_diffusion != 0;
-  const bool pl1 = p.pipe_length == 1.f;
-  const bool k1 = p.k_discharge_exp == 1.f;
-  int        parity = 0;
+  const FusedCfg cfg = vpipes_pick_config(nx, ny);
+  VpStep         st;
+  st.rain = rain;
+  st.H = cfg.h;
+  st.maintain = p.maintain_water_volume != 0;
+  st.diffusion = p.flux_diffusion != 0;
+  st.pl_one = p.pipe_length == 1.f;
+  st.kexp_one = p.k_discharge_exp == 1.f;
+  VpFields *cur = &A, *nxt = &B;
+  int       parity = 0;
   for (int it = 0; it < p.iterations; it++)
   {
-    if (maintain) launch_flow<true>(f, c, sc, parity, diff, pl1, g, b, s);
-    else launch_flow<false>(f, c, sc, parity, diff, pl1, g, b, s);
-    HM_LAUNCH_CHECK("k_vp_flow");
-    if (maintain) launch_we<true>(f, c, sc, parity, partials, pl1, k1, g, b, s);
-    else launch_we<false>(f, c, sc, parity, partials, pl1, k1, g, b, s);
-    HM_LAUNCH_CHECK("k_vp_water_erosion");
-    k_vp_transport<<<g, b, 0, s>>>(f, c);
-    HM_LAUNCH_CHECK("k_vp_transport");
-    float *t = f.z;
-    f.z = f.zn;
-    f.zn = t;
+    const bool last = it == p.iterations - 1;
+    st.in = VpState{cur->z, cur->d, cur->s, cur->fl, cur->fr, cur->ft, cur->fb};
+    st.out = VpStateOut{nxt->z, nxt->d, nxt->s, nxt->fl, nxt->fr, nxt->ft, nxt->fb, nullptr, nullptr};
+    if (last && (vel_u || vel_v))
+    {
+      st.out.u = vel_u ? vel_u : u_buf;
+      st.out.v = vel_v ? vel_v : v_buf;
+    }
+    st.parity = parity;
+    int rc = launch_step(cfg, st, c, sc, partials, df, s);
+    if (rc) return rc;
+    VpFields *t = cur;
+    cur = nxt;
+    nxt = t;
     parity ^= 1;
   }
-  if (f.z != z) HM_CUDA_TRY(cudaMemcpyAsync(z, f.z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  if (cur->z != z) HM_CUDA_TRY(cudaMemcpyAsync(z, cur->z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
 
   if (water_depth)
   {
-    if (maintain) k_vp_final_depth<true><<<592, 256, 0, s>>>(f.d, rain, sc, parity, water_depth, n);
-    else k_vp_final_depth<false><<<592, 256, 0, s>>>(f.d, rain, sc, parity, water_depth, n);
+    if (p.maintain_water_volume) k_vp_final_depth<true><<<592, 256, 0, s>>>(cur->d, rain, sc, parity, water_depth, n);
+    else k_vp_final_depth<false><<<592, 256, 0, s>>>(cur->d, rain, sc, parity, water_depth, n);
     HM_LAUNCH_CHECK("k_vp_final_depth");
   }
-  if (sediment) HM_CUDA_TRY(cudaMemcpyAsync(sediment, f.s, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-  if (vel_u) HM_CUDA_TRY(cudaMemcpyAsync(vel_u, f.u, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-  if (vel_v) HM_CUDA_TRY(cudaMemcpyAsync(vel_v, f.v, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  if (sediment) HM_CUDA_TRY(cudaMemcpyAsync(sediment, cur->s, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  if (p.iterations == 0)
+  {
+    if (vel_u) HM_CUDA_TRY(cudaMemsetAsync(vel_u, 0, n * sizeof(float), s));
+    if (vel_v) HM_CUDA_TRY(cudaMemsetAsync(vel_v, 0, n * sizeof(float), s));
+  }
   return HM_OK;
 }
 
 } // namespace hm
+
+extern "C" int hm_vpipes_set_launch(int tpb, int radius, int rows)
+{
+  hm::clear_error();
+  if (tpb == 0)
+  {
+    hm::g_cfg_override = hm::FusedCfg{0, 0, 0};
+    return HM_OK;
+  }
+  /* rows >= 32 keeps the grid within the partial-sum buffer (partials_bytes) */
+  if (!((tpb == 128 || tpb == 256) && (radius == 2 || radius == 3) && rows >= 32 && rows <= 4096))
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes_set_launch: unsupported launch shape");
+  hm::g_cfg_override = hm::FusedCfg{tpb, radius, rows};
+  return HM_OK;
+}
 
 extern "C" void hm_vpipes_default_params(hm_vpipes_params *p)
 {

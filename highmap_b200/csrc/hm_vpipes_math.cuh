@@ -163,9 +163,14 @@ __device__ __forceinline__ void erosion_cell(const VpConst &c,
   }
 }
 
-/* Mirror an unnormalised coordinate with period 2 * n (texel units). */
+/* Mirror an unnormalised coordinate with period 2 * n (texel units):
+ * |x - 2n * rint(x / 2n)|.  For |x| <= n the quotient rounds to at most
+ * 1/2 in magnitude and rint gives +-0, so the result is |x| exactly; the
+ * division is skipped there. */
 __device__ __forceinline__ float mirror_coord(float x, int n)
 {
+  const float ax = fabsf(x);
+  if (ax <= (float)n) return ax;
   float period = (float)(2 * n);
   float r = rintf(fdiv(x, period));
   return fabsf(fsub(x, fmul(period, r)));
@@ -187,8 +192,10 @@ __device__ __forceinline__ Tap linear_tap(float x, float y, int nx, int ny)
   Tap   t;
   t.a = fsub(xm, fx);
   t.b = fsub(ym, fy);
-  t.i0 = (int)fx;
-  t.j0 = (int)fy;
+  /* after mirroring fx lies in [-1, nx - 1]; the clamp only matters for
+   * coordinates too large to mirror exactly and keeps the taps in the grid */
+  t.i0 = (int)fminf(fmaxf(fx, -1.f), (float)(nx - 1));
+  t.j0 = (int)fminf(fmaxf(fy, -1.f), (float)(ny - 1));
   t.i1 = t.i0 + 1;
   t.j1 = t.j0 + 1;
   t.i0 = t.i0 < 0 ? 0 : t.i0;

@@ -225,6 +225,11 @@ def hydraulic_vpipes_device(z, params: VpipesParams | None = None, rain_map=None
                                      _tptr(vel_v, "vel_v", z.shape), _stream(stream)))
 
 
+def vpipes_set_launch(tpb: int = 0, radius: int = 2, rows: int = 128) -> None:
+    """Launch shape of the fused vpipes step (tpb=0: built-in choice)."""
+    L.check(L.lib().hm_vpipes_set_launch(int(tpb), int(radius), int(rows)))
+
+
 def launch_count() -> int:
     return int(L.lib().hm_launch_count())
 

@@ -230,6 +230,13 @@ int hm_vpipes_device(hm_context             *ctx,
                      float                  *vel_v,
                      void                   *stream);
 
+/* Launch shape of the fused vpipes step kernel, process-wide: threads per
+ * CTA (128 or 256, the strip width including its halo), advection radius
+ * staged in shared memory (2 or 3 cells; samples beyond it are recomputed
+ * exactly from global memory), output rows per CTA (32..4096).  tpb = 0
+ * restores the built-in choice.  Results do not depend on the shape. */
+int hm_vpipes_set_launch(int tpb, int radius, int rows);
+
 /* ---- instrumentation --------------------------------------------------- */
 
 /* Number of kernel launches issued by this library on the calling thread

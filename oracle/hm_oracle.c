@@ -25,6 +25,8 @@
 #define RINT rintf
 #define FABS fabsf
 #define FLOOR floorf
+#define FMIN fminf
+#define FMAX fmaxf
 #include "hm_oracle_body.inc"
 #undef REAL
 #undef K
@@ -34,6 +36,8 @@
 #undef RINT
 #undef FABS
 #undef FLOOR
+#undef FMIN
+#undef FMAX
 
 /* double instance: the same scheme in FP64 (the "FP64 CPU run") */
 #define REAL double
@@ -44,6 +48,8 @@
 #define RINT rint
 #define FABS fabs
 #define FLOOR floor
+#define FMIN fmin
+#define FMAX fmax
 #include "hm_oracle_body.inc"
 #undef REAL
 #undef K
@@ -53,6 +59,8 @@
 #undef RINT
 #undef FABS
 #undef FLOOR
+#undef FMIN
+#undef FMAX
 
 float hmo_sample_linear_mirror_f32(const float *s, int nx, int ny, float x, float y)
 {

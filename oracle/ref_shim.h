@@ -106,7 +106,9 @@ inline float4 read_imagef(image2d_t img, sampler_t, float2 c)
   float     ym = hm_mirror(c.y, ny) - 0.5f;
   float     fx = std::floor(xm), fy = std::floor(ym);
   float     a = xm - fx, b = ym - fy;
-  int       i0 = (int)fx, j0 = (int)fy;
+  float     fxc = std::fmin(std::fmax(fx, -1.f), (float)(nx - 1));
+  float     fyc = std::fmin(std::fmax(fy, -1.f), (float)(ny - 1));
+  int       i0 = (int)fxc, j0 = (int)fyc;
   int       i1 = i0 + 1, j1 = j0 + 1;
   i0 = i0 < 0 ? 0 : i0;
   j0 = j0 < 0 ? 0 : j0;

@@ -176,3 +176,14 @@ def test_float_vs_double_vpipes_error_small():
     a = po.vpipes(z, p)
     b = po.vpipes(z.astype(np.float64), p, dtype=np.float64)
     assert np.abs(a[0] - b[0]).max() <= 1e-3 * float(z.max() - z.min())
+
+
+def test_fast_water_case_exceeds_staged_radius():
+    """The fast-water case of the GPU launch-shape tests moves sediment
+    further than the largest staged advection radius (3 cells), so those
+    tests exercise the kernel's exact slow path."""
+    fast = dict(maintain_water_volume=0, flux_diffusion=1, dt=0.5, gravity=40.0, initial_water=0.05, iterations=12)
+    z0 = fbm(333, 300, seed=5)
+    out = po.vpipes(z0, po.VpipesParams.make(**fast))
+    reach = fast["dt"] * np.maximum(np.abs(out[3]), np.abs(out[4]))
+    assert float(reach.max()) > 3.5

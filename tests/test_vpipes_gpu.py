@@ -135,3 +135,24 @@ def test_full_size_config_properties(gpu):
     want = po.vpipes(z0[:band], po.VpipesParams.make(**dict(CONFIG2, iterations=iters)))[0]
     got = c.cpu().numpy()[:rows]
     assert np.array_equal(got, want[:rows])
+
+
+FAST = dict(maintain_water_volume=0, flux_diffusion=1, dt=0.5, gravity=40.0, initial_water=0.05, iterations=12)
+
+
+@pytest.mark.parametrize("launch", [(128, 2, 32), (128, 2, 128), (256, 2, 64), (128, 3, 48), (256, 3, 256)])
+@pytest.mark.parametrize("case", ["config2", "fast_water", "defaults"])
+def test_launch_shapes(gpu, launch, case):
+    """Every launch shape of the fused step gives the oracle's bits; the
+    fast-water case moves sediment further than the staged advection radius,
+    so its samples go through the exact recomputation from global memory."""
+    ny, nx = 300, 333
+    z0 = fbm(nx, ny, seed=5)
+    pkw = {"config2": dict(CONFIG2, iterations=40), "fast_water": FAST, "defaults": dict(iterations=20)}[case]
+    want = po.vpipes(z0, po.VpipesParams.make(**pkw))
+    gpu.vpipes_set_launch(*launch)
+    try:
+        got = _run_gpu(gpu, z0, pkw)
+    finally:
+        gpu.vpipes_set_launch(0)
+    _check(got, want, z0, exact=not pkw.get("maintain_water_volume", 1))
