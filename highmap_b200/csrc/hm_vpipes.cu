@@ -136,7 +136,7 @@ FusedCfg vpipes_pick_config(int nx, int ny)
   if (g_cfg_override.tpb) return g_cfg_override;
   (void)nx;
   (void)ny;
-  return FusedCfg{128, 3, 128};
+  return FusedCfg{128, 2, 64};
 }
 
 static int fused_w(const FusedCfg &c) { return c.tpb - 2 * (c.r + 2); }

@@ -29,12 +29,19 @@ __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b)
 /* the reference's max / min as the oracle spells them: a > b ? a : b */
 __device__ __forceinline__ float rmax(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float rmin(float a, float b) { return a < b ? a : b; }
+/* a > b ? x : y */
+__device__ __forceinline__ float sel_gt(float a, float b, float x, float y) { return a > b ? x : y; }
 
 __device__ __forceinline__ float hyp(float x, float y)
 {
   double dx = (double)x, dy = (double)y;
   return __double2float_rn(__dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy))));
 }
+
+template <class T> __device__ __forceinline__ T bc(float v);
+template <> __device__ __forceinline__ float bc<float>(float v) { return v; }
+
+__device__ __forceinline__ float powr(float b, float e) { return __double2float_rn(pow((double)b, (double)e)); }
 
 /* Scalars of one vpipes call, prepared on the host with the same float
  * operations the reference performs. */
@@ -58,54 +65,61 @@ struct VpConst
 /* Depth at the start of a step: the stored evaporated depth, plus the
  * volume top-up of the previous step ((add * rain) / R, :167-168), plus the
  * optional per-step rain. */
-template <bool MAINTAIN, bool RAIN>
-__device__ __forceinline__ float depth_d1(float d, float rain, float add, float rvol, float rps)
+template <bool MAINTAIN, bool RAIN, class T>
+__device__ __forceinline__ T depth_d1(T d, T rain, float add, float rvol, float rps)
 {
-  float dc = MAINTAIN ? fadd(d, fdiv(fmul(add, rain), rvol)) : d;
-  if (RAIN) dc = fadd(dc, fmul(rps, rain));
+  T dc = d;
+  if (MAINTAIN) dc = fadd(d, fdiv(fmul(bc<T>(add), rain), bc<T>(rvol)));
+  if (RAIN) dc = fadd(dc, fmul(bc<T>(rps), rain));
   return dc;
 }
 
-/* Flow pass for one cell; h* are z + d1 neighbours' terms split as the
- * reference subtracts them ((h0 - z_n) - d1_n). */
-template <bool DIFFUSION, bool PL_ONE>
+/* Flow pass for one cell; the height differences are formed
+ * as the reference subtracts them: (h0 - z_n) - d1_n.  "s" is j + 1 (the
+ * reference's "top"), "n" is j - 1. */
+template <bool DIFFUSION, bool PL_ONE, class T>
 __device__ __forceinline__ void flow_cell(const VpConst &c,
-                                          float zc, float d1c,
-                                          float zw, float d1w,
-                                          float ze, float d1e,
-                                          float zs, float d1s,
-                                          float zn, float d1n,
-                                          float &fl, float &fr, float &ft, float &fb)
+                                          T zc, T d1c,
+                                          T zw, T d1w,
+                                          T ze, T d1e,
+                                          T zs, T d1s,
+                                          T zn, T d1n,
+                                          T &fl, T &fr, T &ft, T &fb)
 {
-  float h0 = fadd(zc, d1c);
-  float dhl = fsub(fsub(h0, zw), d1w);
-  float dhr = fsub(fsub(h0, ze), d1e);
-  float dht = fsub(fsub(h0, zs), d1s); /* "top" is j + 1 */
-  float dhb = fsub(fsub(h0, zn), d1n);
-  float ql = fmul(c.dtga, dhl), qr = fmul(c.dtga, dhr), qt = fmul(c.dtga, dht), qb = fmul(c.dtga, dhb);
+  const T zero = bc<T>(0.f);
+  T       h0 = fadd(zc, d1c);
+  T       dhl = fsub(fsub(h0, zw), d1w);
+  T       dhr = fsub(fsub(h0, ze), d1e);
+  T       dht = fsub(fsub(h0, zs), d1s);
+  T       dhb = fsub(fsub(h0, zn), d1n);
+  const T dtga = bc<T>(c.dtga);
+  T       ql = fmul(dtga, dhl), qr = fmul(dtga, dhr), qt = fmul(dtga, dht), qb = fmul(dtga, dhb);
   if (!PL_ONE)
   {
-    ql = fdiv(ql, c.pl);
-    qr = fdiv(qr, c.pl);
-    qt = fdiv(qt, c.pl);
-    qb = fdiv(qb, c.pl);
+    const T pl = bc<T>(c.pl);
+    ql = fdiv(ql, pl);
+    qr = fdiv(qr, pl);
+    qt = fdiv(qt, pl);
+    qb = fdiv(qb, pl);
   }
-  float nl = rmax(0.f, fadd(fl, ql));
-  float nr = rmax(0.f, fadd(fr, qr));
-  float nt = rmax(0.f, fadd(ft, qt));
-  float nb = rmax(0.f, fadd(fb, qb));
+  T nl = rmax(zero, fadd(fl, ql));
+  T nr = rmax(zero, fadd(fr, qr));
+  T nt = rmax(zero, fadd(ft, qt));
+  T nb = rmax(zero, fadd(fb, qb));
   if (DIFFUSION)
   {
-    float f_diff = fmul(c.c0, fadd(fadd(fadd(nl, nr), nt), nb));
-    nl = fadd(fmul(c.c1, nl), f_diff);
-    nr = fadd(fmul(c.c1, nr), f_diff);
-    nt = fadd(fmul(c.c1, nt), f_diff);
-    nb = fadd(fmul(c.c1, nb), f_diff);
+    const T c1 = bc<T>(c.c1);
+    T       f_diff = fmul(bc<T>(c.c0), fadd(fadd(fadd(nl, nr), nt), nb));
+    nl = fadd(fmul(c1, nl), f_diff);
+    nr = fadd(fmul(c1, nr), f_diff);
+    nt = fadd(fmul(c1, nt), f_diff);
+    nb = fadd(fmul(c1, nb), f_diff);
   }
-  float sum = fadd(fadd(fadd(nl, nr), nt), nb);
-  float k = 0.f;
-  if (sum > 1e-5f) k = fdiv(fmul(fmul(d1c, c.pl), c.pl), fmul(sum, c.dt));
-  k = rmin(rmax(k, 0.f), 1.f);
+  T sum = fadd(fadd(fadd(nl, nr), nt), nb);
+  /* k = sum > 1e-5 ? d1 * l * l / (sum * dt) : 0, clamped to [0, 1] */
+  T kq = fdiv(fmul(fmul(d1c, bc<T>(c.pl)), bc<T>(c.pl)), fmul(sum, bc<T>(c.dt)));
+  T k = sel_gt(sum, bc<T>(1e-5f), kq, zero);
+  k = rmin(rmax(k, zero), bc<T>(1.f));
   fl = fmul(nl, k);
   fr = fmul(nr, k);
   ft = fmul(nt, k);
@@ -114,53 +128,47 @@ __device__ __forceinline__ void flow_cell(const VpConst &c,
 
 /* Water pass for one cell: new depth d2 and velocity (u, v).
  * frw = fr(i-1, j), fle = fl(i+1, j), ftn = ft(i, j-1), fbs = fb(i, j+1). */
-template <bool PL_ONE>
+template <bool PL_ONE, class T>
 __device__ __forceinline__ void water_cell(const VpConst &c,
-                                           float d1c,
-                                           float flc, float frc, float ftc, float fbc,
-                                           float frw, float fle, float ftn, float fbs,
-                                           float &d2, float &u, float &v)
+                                           T d1c,
+                                           T flc, T frc, T ftc, T fbc,
+                                           T frw, T fle, T ftn, T fbs,
+                                           T &d2, T &u, T &v)
 {
-  float dv = fmul(c.dt, fsub(fsub(fsub(fsub(fadd(fadd(fadd(frw, ftn), fle), fbs), flc), frc), ftc), fbc));
-  d2 = rmax(0.f, fadd(d1c, PL_ONE ? dv : fdiv(dv, c.pl2)));
-  float un = fmul(0.5f, fsub(fadd(fsub(frw, flc), frc), fle));
-  float vn = fmul(0.5f, fsub(fadd(fsub(ftn, fbc), ftc), fbs));
-  float dmean = rmax(c.vel_floor, d2);
+  T dv = fmul(bc<T>(c.dt), fsub(fsub(fsub(fsub(fadd(fadd(fadd(frw, ftn), fle), fbs), flc), frc), ftc), fbc));
+  d2 = rmax(bc<T>(0.f), fadd(d1c, PL_ONE ? dv : fdiv(dv, bc<T>(c.pl2))));
+  T un = fmul(bc<T>(0.5f), fsub(fadd(fsub(frw, flc), frc), fle));
+  T vn = fmul(bc<T>(0.5f), fsub(fadd(fsub(ftn, fbc), ftc), fbs));
+  T dmean = rmax(bc<T>(c.vel_floor), d2);
   u = fdiv(un, dmean);
   v = fdiv(vn, dmean);
 }
 
-/* Erosion / deposition for one cell from the old z and s around it. */
-template <bool KEXP_ONE>
+/* Erosion / deposition for one cell from the old z and s around it; both
+ * branches of :170-183 are formed and one is selected. */
+template <bool KEXP_ONE, class T>
 __device__ __forceinline__ void erosion_cell(const VpConst &c,
-                                             float zc, float sc,
-                                             float zw, float ze, float zn, float zs,
-                                             float sw, float se, float sn, float ss,
-                                             float d2, float u, float v,
-                                             float &z_out, float &s_out)
+                                             T zc, T sc,
+                                             T zw, T ze, T zn, T zs,
+                                             T sw, T se, T sn, T ss,
+                                             T d2, T u, T v,
+                                             T &z_out, T &s_out)
 {
-  float dzx = fmul(0.5f, fsub(fadd(fsub(ze, zw), se), sw));
-  float dzy = fmul(0.5f, fsub(fadd(fsub(zs, zn), ss), sn));
-  float talus = hyp(dzx, dzy);
-  float dzn = rmax(1e-3f, fmul(c.fnx, talus));
-  float salpha = rmax(0.01f, fdiv(dzn, hyp(1.f, dzn)));
-  float speed = hyp(u, v);
-  float depth = rmin(fdiv(d2, c.water_height), c.ratio);
-  float discharge = fmul(depth, speed);
-  float pw = KEXP_ONE ? discharge : __double2float_rn(pow((double)discharge, (double)c.k_exp));
-  float capa = fmul(fmul(c.k_capacity, pw), salpha);
-  if (capa > sc)
-  {
-    float amount = fmul(c.k_erode, fsub(capa, sc));
-    z_out = fsub(zc, amount);
-    s_out = fadd(sc, amount);
-  }
-  else
-  {
-    float amount = fmul(c.k_depose, fsub(sc, capa));
-    z_out = fadd(zc, amount);
-    s_out = fsub(sc, amount);
-  }
+  const T half = bc<T>(0.5f);
+  T       dzx = fmul(half, fsub(fadd(fsub(ze, zw), se), sw));
+  T       dzy = fmul(half, fsub(fadd(fsub(zs, zn), ss), sn));
+  T       talus = hyp(dzx, dzy);
+  T       dzn = rmax(bc<T>(1e-3f), fmul(bc<T>(c.fnx), talus));
+  T       salpha = rmax(bc<T>(0.01f), fdiv(dzn, hyp(bc<T>(1.f), dzn)));
+  T       speed = hyp(u, v);
+  T       depth = rmin(fdiv(d2, bc<T>(c.water_height)), bc<T>(c.ratio));
+  T       discharge = fmul(depth, speed);
+  T       pw = KEXP_ONE ? discharge : powr(discharge, c.k_exp);
+  T       capa = fmul(fmul(bc<T>(c.k_capacity), pw), salpha);
+  T       ero = fmul(bc<T>(c.k_erode), fsub(capa, sc));
+  T       dep = fmul(bc<T>(c.k_depose), fsub(sc, capa));
+  z_out = sel_gt(capa, sc, fsub(zc, ero), fadd(zc, dep));
+  s_out = sel_gt(capa, sc, fadd(sc, ero), fsub(sc, dep));
 }
 
 /* Mirror an unnormalised coordinate with period 2 * n (texel units):

@@ -142,11 +142,13 @@ FAST = dict(maintain_water_volume=0, flux_diffusion=1, dt=0.5, gravity=40.0, ini
 
 @pytest.mark.parametrize("launch", [(128, 2, 32), (128, 2, 128), (256, 2, 64), (128, 3, 48), (256, 3, 256)])
 @pytest.mark.parametrize("case", ["config2", "fast_water", "defaults"])
-def test_launch_shapes(gpu, launch, case):
-    """Every launch shape of the fused step gives the oracle's bits; the
-    fast-water case moves sediment further than the staged advection radius,
-    so its samples go through the exact recomputation from global memory."""
-    ny, nx = 300, 333
+@pytest.mark.parametrize("nx", [333, 334])
+def test_launch_shapes(gpu, launch, case, nx):
+    """Every launch shape of the fused step gives the oracle's bits, for an
+    odd and an even row length.  The fast-water case moves sediment further than the staged advection
+    radius, so its samples go through the exact recomputation from global
+    memory."""
+    ny = 300
     z0 = fbm(nx, ny, seed=5)
     pkw = {"config2": dict(CONFIG2, iterations=40), "fast_water": FAST, "defaults": dict(iterations=20)}[case]
     want = po.vpipes(z0, po.VpipesParams.make(**pkw))
@@ -156,3 +158,20 @@ def test_launch_shapes(gpu, launch, case):
     finally:
         gpu.vpipes_set_launch(0)
     _check(got, want, z0, exact=not pkw.get("maintain_water_volume", 1))
+
+
+def test_unaligned_device_buffer(gpu):
+    """A z that is not 8-byte aligned (a view one element into a buffer)
+    still matches the oracle."""
+    import torch
+    ny, nx = 120, 256
+    z0 = fbm(nx, ny, seed=8)
+    pkw = dict(CONFIG2, iterations=30)
+    want = po.vpipes(z0, po.VpipesParams.make(**pkw))
+    buf = torch.zeros(ny * nx + 1, device="cuda")
+    z = buf[1:].view(ny, nx)
+    z.copy_(torch.from_numpy(z0))
+    assert z.data_ptr() % 8 != 0
+    gpu.hydraulic_vpipes_device(z, gpu.vpipes_params(**pkw))
+    torch.cuda.synchronize()
+    assert np.array_equal(z.cpu().numpy(), want[0])
