@@ -30,7 +30,7 @@ EXPORTED = (
     "hm_thermal", "hm_thermal_scalar", "hm_thermal_masked", "hm_thermal_device",
     "hm_vpipes_default_params", "hm_vpipes", "hm_vpipes_device",
     "hm_launch_count", "hm_launch_count_reset",
-    "hm_thermal_device_noalloc", "hm_vpipes_set_launch",
+    "hm_thermal_device_noalloc", "hm_vpipes_set_launch", "hm_thermal_set_launch",
 )
 
 
@@ -95,6 +95,7 @@ def _declare(lib):
     lib.hm_launch_count.restype = C.c_ulonglong
     lib.hm_thermal_device_noalloc.argtypes = [vp, i, i, vp, f, i, vp, i, vp]
     lib.hm_vpipes_set_launch.argtypes = [i, i, i]
+    lib.hm_thermal_set_launch.argtypes = [i]
     for name in EXPORTED:
         getattr(lib, name)  # raises AttributeError if a symbol is missing
     return lib

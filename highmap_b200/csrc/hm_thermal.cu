@@ -16,9 +16,10 @@
  *   k_thermal_step    one step per launch, one cell per thread; HBM bound:
  *                     reads z (9-point, reuse through L1/L2), talus and
  *                     bedrock, writes z: 12 B/cell (16 B with bedrock).
- *   k_thermal_tb      several steps per launch (temporal blocking): a
+ *   k_thermal_tb      up to 8 steps per launch (temporal blocking): a
  *                     strip of columns streams down the grid; each time
- *                     level keeps a 4-row ring in shared memory.
+ *                     level keeps a 4-row ring in shared memory, so HBM
+ *                     sees the 12/16 B of one step per T steps.
  *   k_extrapolate     the outer ring, one block.
  *   k_thermal_final   deposition map and mask blend, elementwise.
  */
@@ -37,6 +38,8 @@ namespace hm
 /* ------------------------------------------------------------------ */
 /* one step per launch                                                */
 /* ------------------------------------------------------------------ */
+
+__device__ __forceinline__ int clamp_col(int g, int n) { return g < 0 ? 0 : (g > n - 1 ? n - 1 : g); }
 
 constexpr int STEP_BX = 64;
 constexpr int STEP_BY = 4;
@@ -68,6 +71,113 @@ __global__ void __launch_bounds__(STEP_BX *STEP_BY)
   const float  zb = BED != BED_NONE ? __ldg(bedrock + idx) : 0.f;
   b[idx] = thermal_cell<BED>(__ldg(mid), __ldg(mid - 1), __ldg(dn), __ldg(up), __ldg(mid + 1),
                              __ldg(up - 1), __ldg(dn - 1), __ldg(up + 1), __ldg(dn + 1), t, zb);
+}
+
+/* ------------------------------------------------------------------ */
+/* several steps per launch (temporal blocking)                       */
+/* ------------------------------------------------------------------ */
+
+constexpr int TB_TPB = 256; /* strip width in columns, one thread each      */
+constexpr int TB_TMAX = 8;  /* most steps one launch advances                */
+
+__device__ __forceinline__ void tb_cp_async4(float *smem, const float *gmem)
+{
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+/* T Jacobi steps of a column strip in one pass down the rows.
+ *
+ * Thread t owns global column gi = x0 - T + t of a strip of TPB columns
+ * (W = TPB - 2T output columns), and the CTA owns output rows [y0, y1).
+ * Level 0 is the input z, staged row by row into an 8-row ring with
+ * cp.async; level k (1 <= k < T) keeps a 4-row ring.  Iteration r loads
+ * row r and computes, for every level k, row r - 1 - 2k from rows
+ * r - 2 - 2k .. r - 2k of level k - 1, all finished in earlier iterations;
+ * one __syncthreads per iteration publishes them.  Level T goes straight
+ * to the output grid.  Level k is needed on rows [y0 - (T-k), y1 + T-k)
+ * and is correct on columns [k, TPB - k) of the strip, so the T halo
+ * columns each side cover the shrinking valid region.
+ *
+ * Each cell follows the rule of the one-step kernel (border copy, then
+ * the talus exchange with bedrock), so T steps here are bit-identical to
+ * T launches of k_thermal_step. */
+template <bool TMAP, int BED>
+__global__ void __launch_bounds__(TB_TPB)
+    k_thermal_tb(const float *__restrict__ a,
+                 float *__restrict__ b,
+                 int nx,
+                 int ny,
+                 const float *__restrict__ talus,
+                 float talus_value,
+                 const float *__restrict__ bedrock,
+                 int T,
+                 int H)
+{
+  __shared__ float lv0[8][TB_TPB];
+  __shared__ float lvk[TB_TMAX - 1][4][TB_TPB];
+
+  const int  tid = threadIdx.x;
+  const int  W = TB_TPB - 2 * T;
+  const int  x0 = blockIdx.x * W;
+  const int  gi = x0 - T + tid;
+  const bool in_grid = gi >= 0 && gi < nx;
+  const int  gic = clamp_col(gi, nx);
+  const int  y0 = blockIdx.y * H;
+  const int  y1 = min(ny, y0 + H);
+  const int  lw = max(tid - 1, 0), le = min(tid + 1, TB_TPB - 1);
+  const bool out_col = tid >= T && tid < T + W && gi < nx;
+  const int  load_lo = max(0, y0 - T), load_hi = min(ny - 1, y1 - 1 + T);
+
+  for (int r = y0 - T; r <= y1 + 2 * T; ++r)
+  {
+    if (r >= load_lo && r <= load_hi && in_grid) tb_cp_async4(&lv0[r & 7][tid], a + (size_t)r * nx + gi);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+
+#pragma unroll
+    for (int k = 1; k <= TB_TMAX; k++)
+    {
+      if (k > T) break;
+      const int j = r - 1 - 2 * k;
+      if (j < max(0, y0 - (T - k)) || j > min(ny - 1, y1 - 1 + (T - k))) continue;
+      /* rows j-1, j, j+1 of level k-1 */
+      const float *pn, *pc, *ps;
+      if (k == 1)
+      {
+        pn = lv0[(j - 1) & 7];
+        pc = lv0[j & 7];
+        ps = lv0[(j + 1) & 7];
+      }
+      else
+      {
+        pn = lvk[k - 2][(j - 1) & 3];
+        pc = lvk[k - 2][j & 3];
+        ps = lvk[k - 2][(j + 1) & 3];
+      }
+      float out;
+      /* apply_boundaries, _common_index.cl:106-132 */
+      if (gi == 0) out = pc[le];
+      else if (gi == nx - 1) out = pc[lw];
+      else if (j == 0) out = ps[tid];
+      else if (j == ny - 1) out = pn[tid];
+      else
+      {
+        const size_t q = (size_t)j * nx + gic;
+        const float  t = TMAP ? __ldg(talus + q) : talus_value;
+        const float  zb = BED != BED_NONE ? __ldg(bedrock + q) : 0.f;
+        out = thermal_cell<BED>(pc[tid], pc[lw], ps[tid], pn[tid], pc[le], pn[lw], ps[lw], pn[le], ps[le], t, zb);
+      }
+      if (k == T)
+      {
+        if (out_col && j >= y0 && j < y1) b[(size_t)j * nx + gi] = out;
+      }
+      else
+        lvk[k - 1][j & 3][tid] = out;
+    }
+    __syncthreads();
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 /* ------------------------------------------------------------------ */
@@ -159,6 +269,44 @@ static void step_dispatch(const float *a, float *b, int nx, int ny, const float 
   }
 }
 
+template <bool TMAP, int BED>
+static void launch_tb(const float *a, float *b, int nx, int ny, const float *talus, float tv, const float *bed,
+                      int T, int H, cudaStream_t s)
+{
+  const int W = TB_TPB - 2 * T;
+  dim3      grid((nx + W - 1) / W, (ny + H - 1) / H);
+  k_thermal_tb<TMAP, BED><<<grid, TB_TPB, 0, s>>>(a, b, nx, ny, talus, tv, bed, T, H);
+}
+
+static void tb_dispatch(const float *a, float *b, int nx, int ny, const float *talus, float tv, const float *bed,
+                        int bed_mode, int T, int H, cudaStream_t s)
+{
+  const int mode = bed ? (bed_mode == HM_BEDROCK_LITERAL ? BED_LITERAL : BED_INTENDED) : BED_NONE;
+  if (talus)
+  {
+    if (mode == BED_NONE) launch_tb<true, BED_NONE>(a, b, nx, ny, talus, tv, bed, T, H, s);
+    else if (mode == BED_INTENDED) launch_tb<true, BED_INTENDED>(a, b, nx, ny, talus, tv, bed, T, H, s);
+    else launch_tb<true, BED_LITERAL>(a, b, nx, ny, talus, tv, bed, T, H, s);
+  }
+  else
+  {
+    if (mode == BED_NONE) launch_tb<false, BED_NONE>(a, b, nx, ny, talus, tv, bed, T, H, s);
+    else if (mode == BED_INTENDED) launch_tb<false, BED_INTENDED>(a, b, nx, ny, talus, tv, bed, T, H, s);
+    else launch_tb<false, BED_LITERAL>(a, b, nx, ny, talus, tv, bed, T, H, s);
+  }
+}
+
+static int g_tb_rows = 0; /* output rows per CTA of the blocked kernel; 0 = built-in */
+
+/* steps per launch when the caller leaves the choice to the library */
+static int g_tb_default = 1;
+int        thermal_pick_block(int nx, int ny)
+{
+  (void)nx;
+  (void)ny;
+  return g_tb_default;
+}
+
 int thermal_check_args(const float *z, int nx, int ny, int iterations, const hm_thermal_options *o)
 {
   if (!z) return fail(HM_ERR_INVALID_ARGUMENT, "thermal: z is NULL");
@@ -203,12 +351,31 @@ int thermal_core(int device,
 
   if (need_z0) HM_CUDA_TRY(cudaMemcpyAsync(z0, z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
 
+  /* steps per launch: 1 runs the one-step kernel, 2..8 the blocked kernel.
+   * 0 takes the tuned choice for this grid (thermal_pick_block), else one
+   * step per launch, the faster of the two on B200 at 4096^2 when untuned
+   * (both are bound by the issue rate of the exact arithmetic, not by
+   * HBM). */
+  int tb = o.time_block;
+  if (tb == 0) tb = thermal_pick_block(nx, ny);
+  if (tb > TB_TMAX) tb = TB_TMAX;
+  const int rows = g_tb_rows > 0 ? g_tb_rows : 128;
   const float *src = z;
   float       *dst = tmp;
-  for (int it = 0; it < iterations; it++)
+  for (int done = 0; done < iterations;)
   {
-    step_dispatch(src, dst, nx, ny, talus, talus_value, bedrock, o.bedrock_mode, s);
-    HM_LAUNCH_CHECK("k_thermal_step");
+    const int T = (iterations - done < tb) ? iterations - done : tb;
+    if (tb == 1)
+    {
+      step_dispatch(src, dst, nx, ny, talus, talus_value, bedrock, o.bedrock_mode, s);
+      HM_LAUNCH_CHECK("k_thermal_step");
+    }
+    else
+    {
+      tb_dispatch(src, dst, nx, ny, talus, talus_value, bedrock, o.bedrock_mode, T, rows, s);
+      HM_LAUNCH_CHECK("k_thermal_tb");
+    }
+    done += T;
     const float *t = src;
     src = dst;
     dst = const_cast<float *>(t);
@@ -228,6 +395,15 @@ int thermal_core(int device,
 }
 
 } // namespace hm
+
+extern "C" int hm_thermal_set_launch(int rows)
+{
+  hm::clear_error();
+  if (rows != 0 && (rows < 8 || rows > 4096))
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_set_launch: rows must be 0 or in [8, 4096]");
+  hm::g_tb_rows = rows;
+  return HM_OK;
+}
 
 extern "C" void hm_thermal_default_options(hm_thermal_options *opts)
 {

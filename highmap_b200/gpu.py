@@ -230,6 +230,11 @@ def vpipes_set_launch(tpb: int = 0, radius: int = 2, rows: int = 128) -> None:
     L.check(L.lib().hm_vpipes_set_launch(int(tpb), int(radius), int(rows)))
 
 
+def thermal_set_launch(rows: int = 0) -> None:
+    """Output rows per CTA of the blocked thermal kernel (0: built-in)."""
+    L.check(L.lib().hm_thermal_set_launch(int(rows)))
+
+
 def launch_count() -> int:
     return int(L.lib().hm_launch_count())
 

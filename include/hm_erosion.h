@@ -237,6 +237,11 @@ int hm_vpipes_device(hm_context             *ctx,
  * restores the built-in choice.  Results do not depend on the shape. */
 int hm_vpipes_set_launch(int tpb, int radius, int rows);
 
+/* Output rows per CTA of the temporally blocked thermal kernel,
+ * process-wide (8..4096; 0 restores the built-in choice).  Results do not
+ * depend on it. */
+int hm_thermal_set_launch(int rows);
+
 /* ---- instrumentation --------------------------------------------------- */
 
 /* Number of kernel launches issued by this library on the calling thread
