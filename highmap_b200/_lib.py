@@ -31,7 +31,13 @@ EXPORTED = (
     "hm_vpipes_default_params", "hm_vpipes", "hm_vpipes_device",
     "hm_launch_count", "hm_launch_count_reset",
     "hm_thermal_device_noalloc", "hm_vpipes_set_launch", "hm_thermal_set_launch",
+    "hm_batch_create", "hm_batch_destroy", "hm_batch_job_bytes", "hm_batch_add", "hm_batch_step",
+    "hm_batch_synchronize", "hm_batch_job_status", "hm_batch_release", "hm_batch_bytes_in_use",
+    "hm_batch_round", "hm_batch_run",
 )
+
+HM_JOB_THERMAL = 1
+HM_JOB_VPIPES = 2
 
 
 class HMError(RuntimeError):
@@ -69,6 +75,20 @@ class VpipesParams(C.Structure):
     ]
 
 
+class Job(C.Structure):
+    """hm_job: one solve of a batch (device pointers)."""
+
+    _fields_ = [
+        ("kind", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("iterations", C.c_int),
+        ("z", C.c_void_p),
+        ("talus", C.c_void_p), ("talus_value", C.c_float), ("bedrock", C.c_void_p), ("bedrock_mode", C.c_int),
+        ("deposition_map", C.c_void_p),
+        ("vpipes", VpipesParams),
+        ("rain_map", C.c_void_p), ("water_depth", C.c_void_p), ("sediment", C.c_void_p),
+        ("vel_u", C.c_void_p), ("vel_v", C.c_void_p),
+    ]
+
+
 _lock = threading.Lock()
 _lib = None
 
@@ -96,6 +116,20 @@ def _declare(lib):
     lib.hm_thermal_device_noalloc.argtypes = [vp, i, i, vp, f, i, vp, i, vp]
     lib.hm_vpipes_set_launch.argtypes = [i, i, i]
     lib.hm_thermal_set_launch.argtypes = [i]
+    lib.hm_batch_create.argtypes = [vp, C.POINTER(vp)]
+    lib.hm_batch_destroy.argtypes = [vp]
+    lib.hm_batch_job_bytes.argtypes = [vp]
+    lib.hm_batch_job_bytes.restype = C.c_size_t
+    lib.hm_batch_add.argtypes = [vp, vp, C.POINTER(i)]
+    lib.hm_batch_step.argtypes = [vp, i]
+    lib.hm_batch_synchronize.argtypes = [vp]
+    lib.hm_batch_job_status.argtypes = [vp, i, C.POINTER(i), C.POINTER(i)]
+    lib.hm_batch_release.argtypes = [vp, i]
+    lib.hm_batch_bytes_in_use.argtypes = [vp]
+    lib.hm_batch_bytes_in_use.restype = C.c_size_t
+    lib.hm_batch_round.argtypes = [vp]
+    lib.hm_batch_round.restype = C.c_longlong
+    lib.hm_batch_run.argtypes = [vp, vp, i, i]
     for name in EXPORTED:
         getattr(lib, name)  # raises AttributeError if a symbol is missing
     return lib

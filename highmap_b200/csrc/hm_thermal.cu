@@ -269,6 +269,22 @@ static void step_dispatch(const float *a, float *b, int nx, int ny, const float 
   }
 }
 
+/* post-processing of a finished thermal solve (z holds the last step):
+ * border extrapolation, then the deposition map and the mask blend when
+ * asked (z0 = the input heights) */
+int thermal_finish(int device, float *z, int nx, int ny, const float *z0, float *depo, const float *mask,
+                   cudaStream_t s)
+{
+  k_extrapolate<<<1, 1024, 0, s>>>(z, nx, ny);
+  HM_LAUNCH_CHECK("k_extrapolate");
+  if (depo || mask)
+  {
+    k_thermal_final<<<num_sms(device) * 8, 256, 0, s>>>(z, z0, depo, mask, (size_t)nx * ny);
+    HM_LAUNCH_CHECK("k_thermal_final");
+  }
+  return HM_OK;
+}
+
 template <bool TMAP, int BED>
 static void launch_tb(const float *a, float *b, int nx, int ny, const float *talus, float tv, const float *bed,
                       int T, int H, cudaStream_t s)
@@ -381,17 +397,7 @@ int thermal_core(int device,
     dst = const_cast<float *>(t);
   }
   if (src != z) HM_CUDA_TRY(cudaMemcpyAsync(z, src, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-
-  k_extrapolate<<<1, 1024, 0, s>>>(z, nx, ny);
-  HM_LAUNCH_CHECK("k_extrapolate");
-
-  if (need_z0)
-  {
-    int blocks = num_sms(device) * 8;
-    k_thermal_final<<<blocks, 256, 0, s>>>(z, z0, depo, mask, n);
-    HM_LAUNCH_CHECK("k_thermal_final");
-  }
-  return HM_OK;
+  return thermal_finish(device, z, nx, ny, z0, depo, mask, s);
 }
 
 } // namespace hm

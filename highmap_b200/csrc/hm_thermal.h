@@ -15,6 +15,9 @@ size_t thermal_scratch_floats(int nx, int ny, bool need_z0);
 int    thermal_core(int device, float *z, int nx, int ny, const float *talus, float talus_value, int iterations,
                     const float *bedrock, float *depo, const float *mask, const hm_thermal_options *opts,
                     float *scratch_buf, cudaStream_t s);
+/* border extrapolation, deposition map and mask blend after the steps */
+int    thermal_finish(int device, float *z, int nx, int ny, const float *z0, float *depo, const float *mask,
+                      cudaStream_t s);
 } // namespace hm
 
 #endif

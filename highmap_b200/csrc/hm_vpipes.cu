@@ -36,12 +36,6 @@ namespace hm
 constexpr int VP_NT = 256;
 constexpr unsigned VP_INIT_BLOCKS = 296;
 
-/* one copy of the solver state (SoA grids) */
-struct VpFields
-{
-  float *z, *d, *s, *fl, *fr, *ft, *fb;
-};
-
 /* ---- init --------------------------------------------------------- */
 
 /* d = initial depth * rain, s = f = 0; fp64 partial sums of d and rain
@@ -121,6 +115,27 @@ __global__ void k_vp_final_depth(const float *__restrict__ d,
 /* ------------------------------------------------------------------ */
 /* host side                                                          */
 /* ------------------------------------------------------------------ */
+
+int vpipes_init(const VpFields &A, const float *rain, size_t n, float init_depth, VpScalars *sc, double *partials,
+                cudaStream_t s)
+{
+  k_vp_init<<<VP_INIT_BLOCKS, VP_NT, 0, s>>>(A, rain, n, init_depth, partials);
+  HM_LAUNCH_CHECK("k_vp_init");
+  k_vp_init_finish<<<1, VP_NT, 0, s>>>(sc, partials, VP_INIT_BLOCKS);
+  HM_LAUNCH_CHECK("k_vp_init_finish");
+  return HM_OK;
+}
+
+int vpipes_final_depth(const float *d, const float *rain, const VpScalars *sc, int parity, bool maintain,
+                       float *out, size_t n, cudaStream_t s)
+{
+  if (maintain) k_vp_final_depth<true><<<592, 256, 0, s>>>(d, rain, sc, parity, out, n);
+  else k_vp_final_depth<false><<<592, 256, 0, s>>>(d, rain, sc, parity, out, n);
+  HM_LAUNCH_CHECK("k_vp_final_depth");
+  return HM_OK;
+}
+
+size_t vpipes_init_partials() { return 2 * VP_INIT_BLOCKS; }
 
 /* launch shapes of the fused step kernel (threads per CTA = strip width
  * including the halo, sampler radius R) */
@@ -285,10 +300,10 @@ int vpipes_core(float *z,
   const VpConst c = vpipes_consts(nx, ny, p);
   const float   init_depth = p.initial_water < 0.f ? p.water_height : p.initial_water;
 
-  k_vp_init<<<VP_INIT_BLOCKS, VP_NT, 0, s>>>(A, rain, n, init_depth, partials);
-  HM_LAUNCH_CHECK("k_vp_init");
-  k_vp_init_finish<<<1, VP_NT, 0, s>>>(sc, partials, VP_INIT_BLOCKS);
-  HM_LAUNCH_CHECK("k_vp_init_finish");
+  {
+    int rc = vpipes_init(A, rain, n, init_depth, sc, partials, s);
+    if (rc) return rc;
+  }
 
   const FusedCfg cfg = vpipes_pick_config(nx, ny);
   VpStep         st;
@@ -311,6 +326,7 @@ int vpipes_core(float *z,
       st.out.v = vel_v ? vel_v : v_buf;
     }
     st.parity = parity;
+    st.dparity = parity;
     int rc = launch_step(cfg, st, c, sc, partials, df, s);
     if (rc) return rc;
     VpFields *t = cur;
@@ -322,9 +338,8 @@ int vpipes_core(float *z,
 
   if (water_depth)
   {
-    if (p.maintain_water_volume) k_vp_final_depth<true><<<592, 256, 0, s>>>(cur->d, rain, sc, parity, water_depth, n);
-    else k_vp_final_depth<false><<<592, 256, 0, s>>>(cur->d, rain, sc, parity, water_depth, n);
-    HM_LAUNCH_CHECK("k_vp_final_depth");
+    int rc = vpipes_final_depth(cur->d, rain, sc, parity, p.maintain_water_volume != 0, water_depth, n, s);
+    if (rc) return rc;
   }
   if (sediment) HM_CUDA_TRY(cudaMemcpyAsync(sediment, cur->s, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
   if (p.iterations == 0)

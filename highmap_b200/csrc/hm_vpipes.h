@@ -13,6 +13,18 @@ size_t vpipes_scratch_bytes(int nx, int ny);
 /* Device pointers; ordered on s.  rain and the outputs are nullable. */
 int    vpipes_core(float *z, int nx, int ny, const hm_vpipes_params &p, const float *rain, float *water_depth,
                    float *sediment, float *vel_u, float *vel_v, void *scratch_buf, cudaStream_t s);
+struct VpFields;
+struct VpScalars;
+struct VpConst;
+VpConst vpipes_consts(int nx, int ny, const hm_vpipes_params &p);
+/* initial state of copy A (depth, zero sediment and fluxes) and V0, R */
+int     vpipes_init(const VpFields &A, const float *rain, size_t n, float init_depth, VpScalars *sc,
+                    double *partials, cudaStream_t s);
+/* fp64 partial-sum slots vpipes_init needs */
+size_t  vpipes_init_partials();
+/* water-depth output: stored depth plus the top-up of the last step */
+int     vpipes_final_depth(const float *d, const float *rain, const VpScalars *sc, int parity, bool maintain,
+                           float *out, size_t n, cudaStream_t s);
 } // namespace hm
 
 #endif

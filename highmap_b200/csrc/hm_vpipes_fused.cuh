@@ -38,6 +38,12 @@
 namespace hm
 {
 
+/* one copy of the solver state (SoA grids) */
+struct VpFields
+{
+  float *z, *d, *s, *fl, *fr, *ft, *fb;
+};
+
 struct VpState
 {
   const float *z, *d, *s, *fl, *fr, *ft, *fb;
@@ -64,7 +70,8 @@ struct VpStep
   VpState      in;
   VpStateOut   out;
   const float *rain; /* nullable */
-  int          parity;
+  int          parity;  /* step parity: which top-up slot is read         */
+  int          dparity; /* deferred-list slot this step appends to         */
   int          H;    /* output rows per CTA */
   int          maintain, diffusion, pl_one, kexp_one;
 };
@@ -181,6 +188,7 @@ struct FusedLayout
  * velocity, resolved after the step by k_vp_fixup. */
 struct Deferred
 {
+  unsigned job; /* index into the batch's job table (0 for a single solve) */
   unsigned k;
   float    u, v;
 };
@@ -201,11 +209,23 @@ __device__ __forceinline__ float advect_global(const Glob &g, int gi, int gj, fl
   return blend(t, g.s1_at(t.i0, t.j0), g.s1_at(t.i1, t.j0), g.s1_at(t.i0, t.j1), g.s1_at(t.i1, t.j1));
 }
 
+/* One tile (strip bx, chunk by of an nbx x nby decomposition) of one step;
+ * the body of k_vp_fused and of the batched round kernel.  `smem` holds
+ * FusedLayout<TPB, R>::SMEM bytes.  Every thread of the CTA calls it. */
 template <int TPB, int R, bool MAINTAIN>
-__global__ void __launch_bounds__(TPB) k_vp_fused(VpStep st, VpConst c, VpScalars *sc, double *partials, VpDefer df)
+__device__ __forceinline__ void vp_tile(const VpStep &st,
+                                        const VpConst &c,
+                                        VpScalars *sc,
+                                        double *partials,
+                                        const VpDefer &df,
+                                        unsigned job,
+                                        int bx,
+                                        int by,
+                                        int nbx,
+                                        int nby,
+                                        float *smem)
 {
   using L = FusedLayout<TPB, R>;
-  extern __shared__ float smem[];
   float(*sZ)[TPB] = (float(*)[TPB])smem;
   float(*sD)[TPB] = sZ + L::DZ;
   float(*sS)[TPB] = sD + L::DZ;
@@ -217,11 +237,11 @@ __global__ void __launch_bounds__(TPB) k_vp_fused(VpStep st, VpConst c, VpScalar
 
   const int  tid = threadIdx.x;
   const int  nx = c.nx, ny = c.ny;
-  const int  x0 = blockIdx.x * L::W;          /* first output column         */
+  const int  x0 = bx * L::W;                  /* first output column         */
   const int  xs = x0 - L::XH;                 /* global column of thread 0    */
   const int  gi = xs + tid;                   /* this thread's column         */
   const bool in_grid = gi >= 0 && gi < nx;
-  const int  y0 = blockIdx.y * st.H;          /* first output row             */
+  const int  y0 = by * st.H;                  /* first output row             */
   const int  y1 = min(ny, y0 + st.H);         /* one past the last output row  */
   const bool out_col = tid >= L::XH && tid < L::XH + L::W && gi < nx;
 
@@ -377,9 +397,9 @@ __global__ void __launch_bounds__(TPB) k_vp_fused(VpStep st, VpConst c, VpScalar
           st.out.s[k] = sn;
         else
         {
-          const unsigned slot = atomicAdd(&df.count[st.parity], 1u);
+          const unsigned slot = atomicAdd(&df.count[st.dparity], 1u);
           if (slot < df.cap)
-            df.list[slot] = Deferred{(unsigned)k, u, v};
+            df.list[slot] = Deferred{job, (unsigned)k, u, v};
           else
           {
             const Glob g{st, c, add, rvol};
@@ -395,13 +415,20 @@ __global__ void __launch_bounds__(TPB) k_vp_fused(VpStep st, VpConst c, VpScalar
 
   if (MAINTAIN)
   {
-    const unsigned nb = gridDim.x * gridDim.y;
-    const unsigned bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const unsigned nb = (unsigned)(nbx * nby);
+    const unsigned bid = (unsigned)(by * nbx + bx);
     const float    v0 = sc->v0;
     float         *outp = &sc->add[st.parity ^ 1];
     grid_sum_commit<TPB>(part, partials, &sc->ticket, nb, bid,
                          [&](double total) { *outp = fsub(v0, (float)total); });
   }
+}
+
+template <int TPB, int R, bool MAINTAIN>
+__global__ void __launch_bounds__(TPB) k_vp_fused(VpStep st, VpConst c, VpScalars *sc, double *partials, VpDefer df)
+{
+  extern __shared__ float smem[];
+  vp_tile<TPB, R, MAINTAIN>(st, c, sc, partials, df, 0u, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, smem);
 }
 
 /* Resolves the cells k_vp_fused deferred in the same step: their sediment
@@ -413,8 +440,8 @@ __global__ void __launch_bounds__(NT) k_vp_fixup(VpStep st, VpConst c, VpScalars
 {
   const float    add = st.maintain ? sc->add[st.parity] : 0.f;
   const float    rvol = st.maintain ? sc->rvol : 1.f;
-  const unsigned n = min(df.count[st.parity], df.cap);
-  if (blockIdx.x == 0 && threadIdx.x == 0) df.count[st.parity ^ 1] = 0u;
+  const unsigned n = min(df.count[st.dparity], df.cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) df.count[st.dparity ^ 1] = 0u;
   for (unsigned e = blockIdx.x * NT + threadIdx.x; e < n; e += gridDim.x * NT)
   {
     const Deferred d = df.list[e];

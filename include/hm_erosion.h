@@ -242,6 +242,61 @@ int hm_vpipes_set_launch(int tpb, int radius, int rows);
  * depend on it. */
 int hm_thermal_set_launch(int rows);
 
+/* ---- batched and served forms ------------------------------------------ */
+
+/* No counterpart in the reference, which solves one heightmap per call.
+ * A batch holds many device-resident solves of uneven sizes and iteration
+ * counts and advances them together: every job's grid is cut into tiles,
+ * the tiles of all jobs form one packed list, and each round (one step of
+ * every active job) is one persistent kernel over that list.  Results are
+ * bit-identical to solving each job alone with hm_thermal_device /
+ * hm_vpipes_device. */
+
+#define HM_JOB_THERMAL 1
+#define HM_JOB_VPIPES 2
+
+typedef struct hm_job
+{
+  int    kind; /* HM_JOB_THERMAL or HM_JOB_VPIPES */
+  int    nx, ny;
+  int    iterations;
+  float *z; /* device grid, in/out; must stay valid until the job is released */
+  /* thermal (hm_thermal_device's arguments; mask unsupported) */
+  const float *talus; /* NULL selects talus_value */
+  float        talus_value;
+  const float *bedrock;
+  int          bedrock_mode;
+  float       *deposition_map;
+  /* vpipes (hm_vpipes_device's arguments; vpipes.iterations is ignored) */
+  hm_vpipes_params vpipes;
+  const float     *rain_map;
+  float           *water_depth, *sediment, *vel_u, *vel_v;
+} hm_job;
+
+typedef struct hm_batch hm_batch;
+
+/* A batch on ctx's device with its own CUDA stream. */
+int       hm_batch_create(hm_context *ctx, hm_batch **batch);
+int       hm_batch_destroy(hm_batch *batch);
+/* Device bytes a job holds from hm_batch_add to hm_batch_release. */
+size_t    hm_batch_job_bytes(const hm_job *job);
+/* Admits a job: allocates its state (stream-ordered) and initialises it.
+ * The job's first step is the batch's next round. */
+int       hm_batch_add(hm_batch *batch, const hm_job *job, int *job_id);
+/* Advances every admitted, unfinished job by up to `rounds` steps (queued
+ * on the batch stream); jobs that reach their iteration count get their
+ * outputs written (borders, deposition map, water depth ...). */
+int       hm_batch_step(hm_batch *batch, int rounds);
+int       hm_batch_synchronize(hm_batch *batch);
+int       hm_batch_job_status(hm_batch *batch, int job_id, int *steps_done, int *finished);
+/* Frees a job's device state (after its outputs are read). */
+int       hm_batch_release(hm_batch *batch, int job_id);
+size_t    hm_batch_bytes_in_use(const hm_batch *batch);
+long long hm_batch_round(const hm_batch *batch);
+/* All jobs to completion in one call; use_graph != 0 captures every round
+ * into one CUDA graph.  Returns after the results are written. */
+int       hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph);
+
 /* ---- instrumentation --------------------------------------------------- */
 
 /* Number of kernel launches issued by this library on the calling thread

@@ -1,0 +1,142 @@
+"""Batched form: many heightmaps of uneven sizes and iteration counts in one
+batch give, job by job, the oracle's results (bit-exact where the single
+solves are; within the vpipes tolerance with the water-volume top-up)."""
+import numpy as np
+import pytest
+
+from highmap_b200.inputs import fbm
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+CONFIG2 = dict(maintain_water_volume=0, flux_diffusion=0, dt=0.1, k_capacity=0.05, k_erode=0.01, k_depose=0.01,
+               evap_rate=0.01, gravity=9.81, pipe_area=1.0, pipe_length=1.0, rain_per_step=1e-4,
+               initial_water=0.0, water_height=1e-2)
+FAST = dict(maintain_water_volume=0, flux_diffusion=1, dt=0.5, gravity=40.0, initial_water=0.05)
+
+
+def _specs():
+    """(kind, nx, ny, iterations, options) of a mixed batch."""
+    return [
+        ("thermal", 130, 257, 37, dict(talus="map", bedrock=True, depo=True)),
+        ("thermal", 64, 64, 5, dict(talus=0.02)),
+        ("thermal", 3, 3, 4, dict(talus=0.01)),
+        ("thermal", 300, 90, 0, dict(talus=0.01, depo=True)),
+        ("vpipes", 333, 300, 40, dict(params=CONFIG2)),
+        ("vpipes", 128, 200, 25, dict(params=dict(), outputs=True)),
+        ("vpipes", 131, 97, 33, dict(params=dict(maintain_water_volume=0), rain=True, outputs=True)),
+        ("vpipes", 250, 250, 12, dict(params=FAST, outputs=True)),
+        ("vpipes", 40, 40, 0, dict(params=dict(), outputs=True)),
+    ]
+
+
+def _make(specs, seed0=30):
+    import torch
+    from highmap_b200 import batch as B
+    jobs, cases = [], []
+    for k, (kind, nx, ny, it, o) in enumerate(specs):
+        z0 = fbm(nx, ny, seed=seed0 + k)
+        z = torch.from_numpy(z0.copy()).cuda()
+        case = dict(kind=kind, z0=z0, z=z, it=it, o=o)
+        if kind == "thermal":
+            if o["talus"] == "map":
+                t = ((0.5 + fbm(nx, ny, seed=seed0 + 100 + k)) / nx).astype(np.float32)
+                case["talus"] = t
+                talus = torch.from_numpy(t).cuda()
+            else:
+                case["talus"] = np.float32(o["talus"])
+                talus = float(o["talus"])
+            bed = None
+            if o.get("bedrock"):
+                case["bed"] = (0.3 * z0).astype(np.float32)
+                bed = torch.from_numpy(case["bed"]).cuda()
+            depo = torch.empty_like(z) if o.get("depo") else None
+            case["depo"] = depo
+            jobs.append(B.thermal_job(z, talus, it, bedrock=bed, deposition_map=depo))
+        else:
+            rain = None
+            if o.get("rain"):
+                case["rain"] = (0.25 + fbm(nx, ny, seed=seed0 + 200 + k)).astype(np.float32)
+                rain = torch.from_numpy(case["rain"]).cuda()
+            outs = [torch.empty_like(z) for _ in range(4)] if o.get("outputs") else [None] * 4
+            case["outs"] = outs
+            jobs.append(B.vpipes_job(z, it, rain, *outs, **o["params"]))
+        cases.append(case)
+    return jobs, cases
+
+
+def _verify(cases):
+    for c in cases:
+        z0, it, o = c["z0"], c["it"], c["o"]
+        got = c["z"].cpu().numpy()
+        rng = float(z0.max() - z0.min())
+        if c["kind"] == "thermal":
+            talus = c["talus"] if isinstance(c["talus"], np.ndarray) else np.full_like(z0, c["talus"])
+            want, depo = po.thermal(z0, talus, it, bedrock=c.get("bed"), deposition=True)
+            assert np.array_equal(got, want), (z0.shape, it)
+            if c["depo"] is not None:
+                assert np.array_equal(c["depo"].cpu().numpy(), depo)
+        else:
+            p = po.VpipesParams.make(**dict(o["params"], iterations=it))
+            want = po.vpipes(z0, p, rain_map=c.get("rain"))
+            exact = not p.maintain_water_volume
+            if exact:
+                assert np.array_equal(got, want[0]), (z0.shape, it)
+            else:
+                assert np.abs(got - want[0]).max() <= 1e-3 * rng
+            if o.get("outputs"):
+                for t, w in zip(c["outs"], want[1:]):
+                    g = t.cpu().numpy()
+                    if exact:
+                        assert np.array_equal(g, w), (z0.shape, it)
+                    else:
+                        assert np.abs(g - w).max() <= 1e-3 * max(rng, float(np.abs(w).max()))
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_run_matches_oracle(gpu, use_graph):
+    import torch
+    from highmap_b200 import batch as B
+    jobs, cases = _make(_specs())
+    B.run(jobs, use_graph=use_graph)
+    torch.cuda.synchronize()
+    _verify(cases)
+
+
+def test_staggered_admission(gpu):
+    """Jobs admitted at different rounds (as the served form admits them)
+    still each see their own step sequence."""
+    import torch
+    from highmap_b200 import batch as B
+    specs = _specs()
+    jobs, cases = _make(specs, seed0=60)
+    b = B.Batch()
+    ids = []
+    order = [4, 0, 5, 1, 6, 2, 7, 3, 8]
+    for n, k in enumerate(order):
+        ids.append(b.add(jobs[k]))
+        b.step(3 + n)
+    while any(not b.status(i)[1] for i in ids):
+        b.step(7)
+    b.synchronize()
+    torch.cuda.synchronize()
+    for i in ids:
+        steps, done = b.status(i)
+        assert done
+    _verify(cases)
+    before = b.bytes_in_use()
+    assert before > 0
+    for i in ids:
+        b.release(i)
+    assert b.bytes_in_use() == 0
+    b.close()
+
+
+def test_job_bytes_accounts_state(gpu):
+    import torch
+    from highmap_b200 import batch as B
+    z = torch.zeros((100, 120), device="cuda")
+    jt = B.thermal_job(z, 0.01, 10)
+    jv = B.vpipes_job(z, 10)
+    assert B.job_bytes(jt) >= 120 * 100 * 4
+    assert B.job_bytes(jv) >= 13 * 120 * 100 * 4
