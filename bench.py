@@ -61,6 +61,11 @@ def _args():
     ap.add_argument("--size", type=int, default=N_SIDE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", choices=["plain", "batch", "serve"], default="plain",
+                    help="plain: the drop-in headline; batch: 256 mixed jobs batched vs plain calls; "
+                         "serve: Poisson request stream, continuous batching vs plain FIFO")
+    ap.add_argument("--jobs", type=int, default=256, help="jobs of the batch form")
+    ap.add_argument("--requests", type=int, default=100, help="requests per rate of the serve form")
     ap.add_argument("--vpipes-launch", default=None,
                     help="fused vpipes launch shape 'tpb,radius,rows' (default: built-in choice)")
     a = ap.parse_args()
@@ -432,10 +437,47 @@ def run_ours(a):
     return 0
 
 
+def run_form(a):
+    """The batched or served form on one GPU (rank 0 of a torchrun launch
+    runs it; the others exit)."""
+    import torch
+
+    from highmap_b200 import forms
+    from highmap_b200 import gpu as G
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if not G.init_opencl():
+        raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
+    if a.form == "batch":
+        r = forms.run_batch_benchmark(n_jobs=a.jobs)
+        out = {"metric": "aggregate cell-updates/s, %d mixed thermal/vpipes jobs (128..2048, 50..1000 iterations), "
+                         "batched vs plain per-job calls" % a.jobs,
+               "value": r["batched_cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": 1,
+               "higher_is_better": True, "dtype": "f32", "data": "synthetic", "form": "batch",
+               "config": {"workload": "batched form", "jobs": a.jobs, "sizes": "log-uniform 128..2048, x8, aspect<=2",
+                          "iterations": "uniform 50..1000", "kinds": "half thermal, half vpipes"},
+               "detail": r}
+    else:
+        r = forms.run_serve_benchmark(n_requests=a.requests, rates=(10.0, 30.0, 100.0))
+        best = max(r["sweep"], key=lambda x: x["served"]["cell_updates_per_s"])
+        out = {"metric": "served cell-updates/s and p50/p99 latency, Poisson requests (256..4096, 20..2000 "
+                         "iterations), continuous batching vs plain FIFO",
+               "value": best["served"]["cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": 1,
+               "higher_is_better": True, "dtype": "f32", "data": "synthetic", "form": "serve",
+               "config": {"workload": "served form", "requests_per_rate": a.requests,
+                          "budget_bytes": 120 << 30, "rates_per_s": [10.0, 30.0, 100.0]},
+               "detail": r}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     a = _args()
     if a.impl == "reference":
         return run_reference(a)
+    if a.form != "plain":
+        return run_form(a)
     return run_ours(a)
 
 

@@ -77,8 +77,11 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
   const int    nx = J.nx, ny = J.ny;
   const int    i = bx * TH_W + threadIdx.x;
   const int    y0 = by * TH_H, y1 = min(ny, y0 + TH_H);
-  const float *a = J.tz[par];
-  float       *b = J.tz[par ^ 1];
+  const float *__restrict__ a = J.tz[par];
+  float *__restrict__ b = J.tz[par ^ 1];
+  const float *__restrict__ talus = J.talus;
+  const float *__restrict__ bed = J.bed;
+  const float  tv = J.tv;
   if (i >= nx) return;
   for (int j = y0; j < y1; j++)
   {
@@ -89,8 +92,8 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
     if (j == 0) { b[idx] = __ldg(a + idx + nx); continue; }
     if (j == ny - 1) { b[idx] = __ldg(a + idx - nx); continue; }
     const float *up = a + idx - nx, *mid = a + idx, *dn = a + idx + nx;
-    const float  t = TMAP ? __ldg(J.talus + idx) : J.tv;
-    const float  zb = BED != BED_NONE ? __ldg(J.bed + idx) : 0.f;
+    const float  t = TMAP ? __ldg(talus + idx) : tv;
+    const float  zb = BED != BED_NONE ? __ldg(bed + idx) : 0.f;
     b[idx] = thermal_cell<BED>(__ldg(mid), __ldg(mid - 1), __ldg(dn), __ldg(up), __ldg(mid + 1), __ldg(up - 1),
                                __ldg(dn - 1), __ldg(up + 1), __ldg(dn + 1), t, zb);
   }
@@ -128,23 +131,35 @@ __global__ void __launch_bounds__(BT)
                   VpDefer df)
 {
   extern __shared__ float smem[];
-  __shared__ int s_tile;
+  __shared__ int     s_tile;
+  /* the current vpipes tile's job descriptor, staged in shared memory once
+   * per tile (kept in a local struct, it lands on the stack and every use
+   * in the row loop becomes a local-memory load) */
+  __shared__ VpStep  s_st;
+  __shared__ VpConst s_c;
   for (;;)
   {
     if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
     __syncthreads();
     const int t = s_tile;
+    if (t < nv && threadIdx.x == 0)
+    {
+      const BJob &J = jobs[vt[t].x];
+      const int   step = (int)(round - J.start);
+      s_st = job_step(J, step & 1, step, round);
+      s_c = J.c;
+    }
     __syncthreads();
     if (t >= nv + nt) return;
     if (t < nv)
     {
       const int4  tl = vt[t];
       const BJob &J = jobs[tl.x];
-      const int   step = (int)(round - J.start);
-      const int   par = step & 1;
-      VpStep      st = job_step(J, par, step, round);
-      if (J.maintain) vp_tile<BT, BR, true>(st, J.c, J.sc, J.partials, df, (unsigned)tl.x, tl.y, tl.z, J.nbx, J.nby, smem);
-      else vp_tile<BT, BR, false>(st, J.c, J.sc, J.partials, df, (unsigned)tl.x, tl.y, tl.z, J.nbx, J.nby, smem);
+      VpScalars  *sc = J.sc;
+      double     *partials = J.partials;
+      const int   nbx = J.nbx, nby = J.nby;
+      if (s_st.maintain) vp_tile<BT, BR, true>(s_st, s_c, sc, partials, df, (unsigned)tl.x, tl.y, tl.z, nbx, nby, smem);
+      else vp_tile<BT, BR, false>(s_st, s_c, sc, partials, df, (unsigned)tl.x, tl.y, tl.z, nbx, nby, smem);
     }
     else
     {
@@ -556,6 +571,32 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
   h.live = true;
   b->jobs.push_back(h);
   b->dirty = true;
+  /* deferred-advection list: room for 1/32 of the admitted vpipes cells
+   * (the same share as a single solve); overflowing samples would be
+   * resolved inline, stalling their CTA */
+  if (job->kind == HM_JOB_VPIPES)
+  {
+    size_t cells = 0;
+    for (const HJob &x : b->jobs)
+      if (x.live && x.desc.kind == HM_JOB_VPIPES) cells += (size_t)x.desc.nx * x.desc.ny;
+    const size_t want = std::max<size_t>(1u << 16, cells / 32);
+    if (want > b->defer_cap)
+    {
+      /* the list is empty between rounds: reallocation only has to be
+       * ordered after the work already queued */
+      HM_CUDA_TRY(cudaFreeAsync(b->d_defer, b->stream));
+      b->d_defer = nullptr;
+      const size_t cap = want + want / 2;
+      e = cudaMallocAsync((void **)&b->d_defer, cap * sizeof(hm::Deferred), b->stream);
+      if (e != cudaSuccess)
+      {
+        cudaGetLastError();
+        b->defer_cap = 0;
+        return hm::cuda_fail(e, "hm_batch_add: deferred list allocation");
+      }
+      b->defer_cap = (unsigned)cap;
+    }
+  }
   *job_id = (int)b->jobs.size() - 1;
   if (job->iterations == 0) return finalize_job(b, b->jobs.back());
   return HM_OK;

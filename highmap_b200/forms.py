@@ -1,0 +1,265 @@
+"""Workloads and measurement of the batched and served forms.
+
+Batched form: many heightmaps of uneven sizes and iteration counts run as
+one batch (hm_batch_run, one CUDA graph) against the same jobs solved one
+call at a time with the plain device path (hm_thermal_device /
+hm_vpipes_device), both on device-resident inputs.
+
+Served form: a request loop, as an interactive node-graph editor would
+drive it: requests arrive as a Poisson stream, are admitted into an open
+batch while their device state fits an HBM budget, advance together a few
+rounds per tick (continuous batching), and are retired when done; latency
+is completion minus arrival.  The same stream served first-come
+first-served by the plain path is the comparison point.
+
+Inputs are seeded synthetic fBm fields (highmap_b200.inputs).
+"""
+from __future__ import annotations
+
+import heapq
+import math
+import time
+
+import numpy as np
+
+from . import batch as B
+from . import gpu as G
+from .inputs import fbm
+
+VPIPES_BASE = dict(maintain_water_volume=0, flux_diffusion=0, dt=0.1, k_capacity=0.05, k_erode=0.01,
+                   k_depose=0.01, evap_rate=0.01, gravity=9.81, pipe_area=1.0, pipe_length=1.0,
+                   initial_water=0.0, water_height=1e-2)
+
+
+# ---------------------------------------------------------------- batched
+
+def batch_specs(n_jobs=256, seed=0, lo=128, hi=2048):
+    """Job list of the batched configuration: sides log-uniform in [lo, hi]
+    rounded to multiples of 8, aspect ratio up to 2:1, half thermal (talus
+    uniform in [0.5, 2] / nx) and half vpipes (rain uniform in [5e-5, 5e-4]
+    per step), iterations uniform in [50, 1000], fBm seeds 100 + k."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for k in range(n_jobs):
+        a = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        ratio = rng.uniform(1.0, 2.0)
+        if rng.uniform() < 0.5:
+            nx, ny = a, a / ratio
+        else:
+            nx, ny = a / ratio, a
+        nx = int(min(hi, max(lo, round(nx / 8) * 8)))
+        ny = int(min(hi, max(lo, round(ny / 8) * 8)))
+        kind = "thermal" if k % 2 == 0 else "vpipes"
+        it = int(rng.integers(50, 1001))
+        talus = float(rng.uniform(0.5, 2.0)) / nx
+        rain = float(rng.uniform(5e-5, 5e-4))
+        specs.append(dict(kind=kind, nx=nx, ny=ny, iterations=it, talus=talus, rain=rain, seed=100 + k))
+    return specs
+
+
+def _inputs(specs):
+    return [fbm(s["nx"], s["ny"], seed=s["seed"]) for s in specs]
+
+
+def _job(s, z):
+    if s["kind"] == "thermal":
+        return B.thermal_job(z, s["talus"], s["iterations"])
+    return B.vpipes_job(z, s["iterations"], **dict(VPIPES_BASE, rain_per_step=s["rain"]))
+
+
+def _plain(s, z, ctx, stream):
+    if s["kind"] == "thermal":
+        G.thermal_device(z, s["talus"], s["iterations"], ctx=ctx, stream=stream)
+    else:
+        p = G.vpipes_params(**dict(VPIPES_BASE, rain_per_step=s["rain"], iterations=s["iterations"]))
+        G.hydraulic_vpipes_device(z, p, ctx=ctx, stream=stream)
+
+
+def run_batch_benchmark(n_jobs=256, seed=0, check=4):
+    """Aggregate cell-updates/s of the batched run and of plain per-job
+    calls on the same jobs; `check` jobs are compared bit for bit."""
+    import torch
+    specs = batch_specs(n_jobs, seed)
+    fields = _inputs(specs)
+    host = [torch.from_numpy(f) for f in fields]
+    cells = sum(s["nx"] * s["ny"] * s["iterations"] for s in specs)
+    ctx = G.Context(torch.cuda.current_device())
+    stream = torch.cuda.current_stream().cuda_stream
+
+    # plain: one call per job, device-resident inputs
+    zs = [h.cuda() for h in host]
+    _plain(specs[0], zs[0].clone(), ctx, stream)  # warm the workspace
+    torch.cuda.synchronize()
+    zs = [h.cuda() for h in host]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s, z in zip(specs, zs):
+        _plain(s, z, ctx, stream)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_s = e0.elapsed_time(e1) * 1e-3
+    plain_out = [z[:4].cpu() for z in zs[:check]]
+    del zs
+
+    # batched: every job in one graph-captured batch
+    zb = [h.cuda() for h in host]
+    jobs = [_job(s, z) for s, z in zip(specs, zb)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    B.run(jobs, use_graph=True, ctx=ctx)
+    torch.cuda.synchronize()
+    batch_s = time.perf_counter() - t0
+    same = all(torch.equal(z[:4].cpu(), p) for z, p in zip(zb[:check], plain_out))
+    ctx.close()
+    return {
+        "jobs": n_jobs, "cell_updates": cells,
+        "batched_cell_updates_per_s": cells / batch_s, "plain_cell_updates_per_s": cells / plain_s,
+        "speedup": plain_s / batch_s, "batched_s": batch_s, "plain_s": plain_s,
+        "batched_includes": "admission, state init, graph capture and instantiation, all rounds",
+        "bit_identical_to_plain_sample": same,
+    }
+
+
+# ---------------------------------------------------------------- served
+
+def serve_requests(n, rate, seed=0, lo=256, hi=4096, it_lo=20, it_hi=2000):
+    """Request stream of the served configuration: Poisson arrivals at
+    `rate` per second, sides log-uniform in [lo, hi] (multiples of 8),
+    50/50 thermal / vpipes, iterations log-uniform in [it_lo, it_hi]."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs = []
+    for rid in range(n):
+        t += rng.exponential(1.0 / rate)
+        side = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        side = int(max(lo, min(hi, round(side / 8) * 8)))
+        it = int(round(math.exp(rng.uniform(math.log(it_lo), math.log(it_hi)))))
+        kind = "thermal" if rng.uniform() < 0.5 else "vpipes"
+        reqs.append(dict(id=rid, arrival=t, kind=kind, nx=side, ny=side, iterations=it, talus=1.0 / side,
+                         rain=1e-4, seed=rid))
+    return reqs
+
+
+class FieldPool:
+    """Device-resident source heightmaps: a few large fBm fields; request k
+    takes a window of field k % count at an offset drawn from its id."""
+
+    def __init__(self, count=4, side=4096, seed=7):
+        import torch
+        self.fields = [torch.from_numpy(fbm(side, side, seed=seed + k)).cuda() for k in range(count)]
+        self.side = side
+
+    def take(self, rid, nx, ny):
+        f = self.fields[rid % len(self.fields)]
+        rng = np.random.default_rng(rid)
+        ox = int(rng.integers(0, self.side - nx + 1))
+        oy = int(rng.integers(0, self.side - ny + 1))
+        return f[oy:oy + ny, ox:ox + nx].contiguous()
+
+
+def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=8):
+    """Continuous batching: returns per-request latencies (s) and totals."""
+    import torch
+    b = B.Batch(G.Context(torch.cuda.current_device()))
+    pending = list(reqs)
+    waiting = []  # arrived, not admitted (FIFO)
+    active = {}   # job id -> (request, tensor, job)
+    lat = {}
+    t0 = time.perf_counter()
+    cells = 0
+    while pending or waiting or active:
+        now = time.perf_counter() - t0
+        while pending and pending[0]["arrival"] <= now:
+            waiting.append(pending.pop(0))
+        while waiting:
+            r = waiting[0]
+            z = pool.take(r["id"], r["nx"], r["ny"])
+            job = _job(r, z)
+            if active and b.bytes_in_use() + B.job_bytes(job) > budget_bytes:
+                break
+            waiting.pop(0)
+            jid = b.add(job)
+            active[jid] = (r, z, job)
+        if not active:
+            if pending:
+                time.sleep(max(0.0, min(0.01, pending[0]["arrival"] - now)))
+            continue
+        b.step(rounds_per_tick)
+        b.synchronize()
+        done_t = time.perf_counter() - t0
+        for jid in list(active):
+            if b.status(jid)[1]:
+                r, z, job = active.pop(jid)
+                lat[r["id"]] = done_t - r["arrival"]
+                cells += r["nx"] * r["ny"] * r["iterations"]
+                b.release(jid)
+    total = time.perf_counter() - t0
+    b.close()
+    return lat, cells, total
+
+
+def serve_plain(reqs, pool):
+    """First-come first-served, one plain call per request."""
+    import torch
+    ctx = G.Context(torch.cuda.current_device())
+    stream = torch.cuda.current_stream().cuda_stream
+    lat = {}
+    t0 = time.perf_counter()
+    cells = 0
+    for r in reqs:
+        now = time.perf_counter() - t0
+        if r["arrival"] > now:
+            time.sleep(r["arrival"] - now)
+        z = pool.take(r["id"], r["nx"], r["ny"])
+        _plain(r, z, ctx, stream)
+        torch.cuda.synchronize()
+        lat[r["id"]] = time.perf_counter() - t0 - r["arrival"]
+        cells += r["nx"] * r["ny"] * r["iterations"]
+    total = time.perf_counter() - t0
+    ctx.close()
+    return lat, cells, total
+
+
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v), q)) if v else None
+
+
+def run_serve_benchmark(n_requests=200, rates=(2.0, 8.0, 32.0), seed=0, check=3):
+    """Throughput and p50/p99 latency of the served form and of the plain
+    path for each arrival rate; `check` requests are re-solved alone and
+    compared bit for bit with their served result."""
+    import torch
+    pool = FieldPool()
+    out = []
+    for rate in rates:
+        reqs = serve_requests(n_requests, rate, seed)
+        lat_b, cells_b, tot_b = serve(reqs, pool)
+        lat_p, cells_p, tot_p = serve_plain(reqs, pool)
+        out.append({
+            "rate_per_s": rate, "requests": n_requests,
+            "served": {"cell_updates_per_s": cells_b / tot_b, "p50_s": _pct(list(lat_b.values()), 50),
+                       "p99_s": _pct(list(lat_b.values()), 99), "wall_s": tot_b},
+            "plain": {"cell_updates_per_s": cells_p / tot_p, "p50_s": _pct(list(lat_p.values()), 50),
+                      "p99_s": _pct(list(lat_p.values()), 99), "wall_s": tot_p},
+        })
+    # results of the served path equal the plain path's
+    reqs = serve_requests(check, 100.0, seed + 1, hi=512, it_hi=200)
+    b = B.Batch(G.Context(torch.cuda.current_device()))
+    zs, ids = [], []
+    for r in reqs:
+        z = pool.take(r["id"], r["nx"], r["ny"])
+        zs.append(z)
+        ids.append(b.add(_job(r, z)))
+    while not all(b.status(i)[1] for i in ids):
+        b.step(16)
+    b.synchronize()
+    ctx = G.Context(torch.cuda.current_device())
+    same = True
+    for r, z in zip(reqs, zs):
+        w = pool.take(r["id"], r["nx"], r["ny"])
+        _plain(r, w, ctx, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        same = same and bool(torch.equal(w, z))
+    b.close()
+    ctx.close()
+    return {"sweep": out, "bit_identical_to_plain_sample": same}
