@@ -303,6 +303,10 @@ def run_ours(a):
     bed_d = torch.from_numpy(bed).to(dev)
     z_th = torch.empty_like(z0_d)
     z_vp = torch.empty_like(z0_d)
+    # launch shapes picked by the autotuner for this grid size (part of warm-up)
+    from highmap_b200 import tune
+    tuned = {"vpipes": tune.autotune(tune.VPIPES, n, n, steps=20, ctx=ctx),
+             "thermal": tune.autotune(tune.THERMAL, n, n, steps=40, ctx=ctx)}
     pv = G.vpipes_params(**dict(CONFIG2_VPIPES, iterations=VPIPES_ITERS))
     stream = torch.cuda.Stream(device=dev)
 
@@ -429,6 +433,7 @@ def run_ours(a):
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "bytes_per_cell_update": VPIPES_BYTES},
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
+            "launch_shapes": tuned,
         }
         print(json.dumps(out), flush=True)
     ctx.close()

@@ -34,6 +34,7 @@ EXPORTED = (
     "hm_batch_create", "hm_batch_destroy", "hm_batch_job_bytes", "hm_batch_add", "hm_batch_step",
     "hm_batch_synchronize", "hm_batch_job_status", "hm_batch_release", "hm_batch_bytes_in_use",
     "hm_batch_round", "hm_batch_run",
+    "hm_autotune", "hm_autotune_save", "hm_autotune_load", "hm_autotune_clear",
 )
 
 HM_JOB_THERMAL = 1
@@ -73,6 +74,11 @@ class VpipesParams(C.Structure):
         ("rain_per_step", C.c_float),
         ("initial_water", C.c_float),
     ]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("tpb", C.c_int), ("radius", C.c_int), ("rows", C.c_int), ("time_block", C.c_int),
+                ("ms_per_step", C.c_float), ("candidates", C.c_int)]
 
 
 class Job(C.Structure):
@@ -130,6 +136,9 @@ def _declare(lib):
     lib.hm_batch_round.argtypes = [vp]
     lib.hm_batch_round.restype = C.c_longlong
     lib.hm_batch_run.argtypes = [vp, vp, i, i]
+    lib.hm_autotune.argtypes = [vp, i, i, i, i, vp]
+    lib.hm_autotune_save.argtypes = [C.c_char_p]
+    lib.hm_autotune_load.argtypes = [C.c_char_p, C.POINTER(i)]
     for name in EXPORTED:
         getattr(lib, name)  # raises AttributeError if a symbol is missing
     return lib

@@ -31,6 +31,7 @@
 #include "hm_internal.h"
 #include "hm_thermal.h"
 #include "hm_thermal_math.cuh"
+#include "hm_tune.h"
 
 namespace hm
 {
@@ -314,14 +315,9 @@ static void tb_dispatch(const float *a, float *b, int nx, int ny, const float *t
 
 static int g_tb_rows = 0; /* output rows per CTA of the blocked kernel; 0 = built-in */
 
-/* steps per launch when the caller leaves the choice to the library */
+/* steps per launch when the caller leaves the choice to the library and
+ * the grid's size class is not tuned */
 static int g_tb_default = 1;
-int        thermal_pick_block(int nx, int ny)
-{
-  (void)nx;
-  (void)ny;
-  return g_tb_default;
-}
 
 int thermal_check_args(const float *z, int nx, int ny, int iterations, const hm_thermal_options *o)
 {
@@ -373,9 +369,20 @@ int thermal_core(int device,
    * (both are bound by the issue rate of the exact arithmetic, not by
    * HBM). */
   int tb = o.time_block;
-  if (tb == 0) tb = thermal_pick_block(nx, ny);
+  int rows = g_tb_rows;
+  if (tb == 0)
+  {
+    TuneEntry e;
+    if (tuned_thermal(nx, ny, &e))
+    {
+      tb = e.block;
+      if (rows == 0) rows = e.rows;
+    }
+    else
+      tb = g_tb_default;
+  }
   if (tb > TB_TMAX) tb = TB_TMAX;
-  const int rows = g_tb_rows > 0 ? g_tb_rows : 128;
+  if (rows <= 0) rows = 128;
   const float *src = z;
   float       *dst = tmp;
   for (int done = 0; done < iterations;)

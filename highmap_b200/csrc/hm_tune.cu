@@ -1,0 +1,256 @@
+/*
+ * hm_tune.cu - the launch-shape autotuner.
+ *
+ * For one solver and grid size it times every candidate launch shape on a
+ * synthetic terrain of that size (generated on the device: a sum of
+ * sinusoids with the value range of a remapped fBm field) and keeps the
+ * fastest per size class (nx and ny rounded up to powers of two):
+ *   vpipes  : threads per CTA (strip width) x staged advection radius x
+ *             output rows per CTA (the occupancy / halo / warm-up trade);
+ *   thermal : steps per launch (temporal-block depth 1, 2, 4, 8) x rows
+ *             per CTA of the blocked kernel.
+ * The solvers consult the table whenever the caller leaves the choice to
+ * the library (time_block 0, no hm_vpipes_set_launch override).  Results
+ * never depend on the shape; only the speed does.
+ */
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "hm_internal.h"
+#include "hm_thermal.h"
+#include "hm_tune.h"
+#include "hm_vpipes.h"
+
+namespace hm
+{
+
+namespace
+{
+
+std::mutex                                   g_mu;
+std::map<std::pair<int, int>, TuneEntry>     g_vp, g_th; /* size class -> shape */
+
+int pow2_class(int v)
+{
+  int c = 0;
+  while ((1 << c) < v && c < 30) c++;
+  return c;
+}
+
+std::pair<int, int> size_class(int nx, int ny) { return {pow2_class(nx), pow2_class(ny)}; }
+
+__global__ void k_synthetic_terrain(float *z, int nx, int ny)
+{
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < (size_t)nx * ny;
+       k += (size_t)gridDim.x * blockDim.x)
+  {
+    const float x = (float)(k % nx) / nx, y = (float)(k / nx) / ny;
+    float       v = 0.f, a = 0.5f, f = 4.f;
+    for (int o = 0; o < 6; o++)
+    {
+      v += a * __sinf(6.2831853f * f * x + 1.7f * o) * __cosf(6.2831853f * f * y + 0.9f * o);
+      a *= 0.5f;
+      f *= 2.f;
+    }
+    z[k] = 0.5f + 0.5f * v;
+  }
+}
+
+} // namespace
+
+bool tuned_vpipes(int nx, int ny, TuneEntry *out)
+{
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto                        it = g_vp.find(size_class(nx, ny));
+  if (it == g_vp.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+bool tuned_thermal(int nx, int ny, TuneEntry *out)
+{
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto                        it = g_th.find(size_class(nx, ny));
+  if (it == g_th.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+} // namespace hm
+
+extern "C" {
+
+int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_result *result)
+{
+  hm::clear_error();
+  if (!ctx || (kind != HM_JOB_THERMAL && kind != HM_JOB_VPIPES) || nx < 3 || ny < 3 || steps < 1)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_autotune: bad argument");
+  int st = hm::use_device(ctx->device);
+  if (st) return st;
+  cudaStream_t s = ctx->stream;
+  const size_t n = (size_t)nx * ny;
+  float       *z = nullptr, *z0 = nullptr;
+  HM_CUDA_TRY(cudaMallocAsync((void **)&z, n * sizeof(float), s));
+  HM_CUDA_TRY(cudaMallocAsync((void **)&z0, n * sizeof(float), s));
+  hm::k_synthetic_terrain<<<592, 256, 0, s>>>(z0, nx, ny);
+  HM_LAUNCH_CHECK("k_synthetic_terrain");
+  cudaEvent_t e0, e1;
+  HM_CUDA_TRY(cudaEventCreate(&e0));
+  HM_CUDA_TRY(cudaEventCreate(&e1));
+
+  std::vector<hm::TuneEntry> cands;
+  if (kind == HM_JOB_VPIPES)
+  {
+    const int shapes[][3] = {{128, 2, 32}, {128, 2, 64}, {128, 2, 128}, {256, 2, 64},
+                             {128, 3, 32}, {128, 3, 64}, {256, 3, 64}};
+    for (auto &c : shapes) cands.push_back(hm::TuneEntry{c[0], c[1], c[2], 0, 0.f});
+  }
+  else
+  {
+    const int shapes[][2] = {{1, 0}, {2, 64}, {4, 64}, {4, 128}, {8, 64}, {8, 128}};
+    for (auto &c : shapes) cands.push_back(hm::TuneEntry{0, 0, c[1], c[0], 0.f});
+  }
+
+  /* the benchmark configuration's parameters: rain per step, gravity 9.81 */
+  hm_vpipes_params vp;
+  hm_vpipes_default_params(&vp);
+  vp.maintain_water_volume = 0;
+  vp.flux_diffusion = 0;
+  vp.dt = 0.1f;
+  vp.k_capacity = 0.05f;
+  vp.k_erode = vp.k_depose = 0.01f;
+  vp.evap_rate = 0.01f;
+  vp.gravity = 9.81f;
+  vp.rain_per_step = 1e-4f;
+  vp.initial_water = 0.f;
+  vp.iterations = steps;
+
+  int       best = -1;
+  float     best_ms = 0.f;
+  const int warm = 2;
+  for (size_t k = 0; k < cands.size() && !st; k++)
+  {
+    const hm::TuneEntry &c = cands[k];
+    float                ms = 0.f;
+    for (int rep = 0; rep < warm + 1 && !st; rep++)
+    {
+      HM_CUDA_TRY(cudaMemcpyAsync(z, z0, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+      HM_CUDA_TRY(cudaEventRecord(e0, s));
+      if (kind == HM_JOB_VPIPES)
+      {
+        if ((st = hm_vpipes_set_launch(c.tpb, c.radius, c.rows))) break;
+        st = hm_vpipes_device(ctx, z, nx, ny, &vp, nullptr, nullptr, nullptr, nullptr, nullptr, s);
+      }
+      else
+      {
+        hm_thermal_options o;
+        hm_thermal_default_options(&o);
+        o.time_block = c.block;
+        if ((st = hm_thermal_set_launch(c.rows))) break;
+        st = hm_thermal_device(ctx, z, nx, ny, nullptr, 1.f / nx, steps, nullptr, nullptr, nullptr, &o, s);
+      }
+      HM_CUDA_TRY(cudaEventRecord(e1, s));
+      HM_CUDA_TRY(cudaEventSynchronize(e1));
+      HM_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    }
+    cands[k].ms_per_step = ms / steps;
+    if (!st && (best < 0 || ms < best_ms))
+    {
+      best = (int)k;
+      best_ms = ms;
+    }
+  }
+  if (kind == HM_JOB_VPIPES) hm_vpipes_set_launch(0, 0, 0);
+  else hm_thermal_set_launch(0);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(z, s);
+  cudaFreeAsync(z0, s);
+  cudaStreamSynchronize(s);
+  if (st) return st;
+
+  {
+    std::lock_guard<std::mutex> lk(hm::g_mu);
+    (kind == HM_JOB_VPIPES ? hm::g_vp : hm::g_th)[hm::size_class(nx, ny)] = cands[best];
+  }
+  if (result)
+  {
+    result->tpb = cands[best].tpb;
+    result->radius = cands[best].radius;
+    result->rows = cands[best].rows;
+    result->time_block = cands[best].block;
+    result->ms_per_step = cands[best].ms_per_step;
+    result->candidates = (int)cands.size();
+  }
+  return HM_OK;
+}
+
+int hm_autotune_save(const char *path)
+{
+  if (!path) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_autotune_save: NULL path");
+  FILE *f = fopen(path, "w");
+  if (!f) return hm::fail(HM_ERR_INVALID_ARGUMENT, std::string("hm_autotune_save: cannot open ") + path);
+  std::lock_guard<std::mutex> lk(hm::g_mu);
+  fprintf(f, "# highmap_b200 launch shapes: kind log2nx log2ny tpb radius rows time_block ms_per_step\n");
+  for (auto &kv : hm::g_vp)
+    fprintf(f, "vpipes %d %d %d %d %d %d %.6f\n", kv.first.first, kv.first.second, kv.second.tpb, kv.second.radius,
+            kv.second.rows, kv.second.block, kv.second.ms_per_step);
+  for (auto &kv : hm::g_th)
+    fprintf(f, "thermal %d %d %d %d %d %d %.6f\n", kv.first.first, kv.first.second, kv.second.tpb,
+            kv.second.radius, kv.second.rows, kv.second.block, kv.second.ms_per_step);
+  fclose(f);
+  return HM_OK;
+}
+
+int hm_autotune_load(const char *path, int *loaded_out)
+{
+  if (loaded_out) *loaded_out = 0;
+  if (!path) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_autotune_load: NULL path");
+  FILE *f = fopen(path, "r");
+  if (!f) return hm::fail(HM_ERR_INVALID_ARGUMENT, std::string("hm_autotune_load: cannot open ") + path);
+  char line[256];
+  int  loaded = 0;
+  while (fgets(line, sizeof line, f))
+  {
+    char          kind[16];
+    int           cx, cy;
+    hm::TuneEntry e{};
+    if (line[0] == '#') continue;
+    if (sscanf(line, "%15s %d %d %d %d %d %d %f", kind, &cx, &cy, &e.tpb, &e.radius, &e.rows, &e.block,
+               &e.ms_per_step) != 8)
+      continue;
+    std::string k(kind);
+    /* keep only shapes the kernels accept */
+    if (k == "vpipes" && hm_vpipes_set_launch(e.tpb, e.radius, e.rows) == HM_OK)
+    {
+      std::lock_guard<std::mutex> lk(hm::g_mu);
+      hm::g_vp[{cx, cy}] = e;
+      loaded++;
+    }
+    else if (k == "thermal" && e.block >= 1 && e.block <= 8 && (e.rows == 0 || (e.rows >= 8 && e.rows <= 4096)))
+    {
+      std::lock_guard<std::mutex> lk(hm::g_mu);
+      hm::g_th[{cx, cy}] = e;
+      loaded++;
+    }
+  }
+  hm_vpipes_set_launch(0, 0, 0);
+  fclose(f);
+  if (loaded_out) *loaded_out = loaded;
+  return HM_OK;
+}
+
+void hm_autotune_clear(void)
+{
+  std::lock_guard<std::mutex> lk(hm::g_mu);
+  hm::g_vp.clear();
+  hm::g_th.clear();
+}
+
+} // extern "C"

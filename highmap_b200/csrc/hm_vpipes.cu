@@ -26,6 +26,7 @@
 
 #include "hm_internal.h"
 #include "hm_reduce.cuh"
+#include "hm_tune.h"
 #include "hm_vpipes.h"
 #include "hm_vpipes_fused.cuh"
 #include "hm_vpipes_math.cuh"
@@ -149,8 +150,8 @@ static FusedCfg g_cfg_override = {0, 0, 0};
 FusedCfg vpipes_pick_config(int nx, int ny)
 {
   if (g_cfg_override.tpb) return g_cfg_override;
-  (void)nx;
-  (void)ny;
+  TuneEntry e;
+  if (tuned_vpipes(nx, ny, &e)) return FusedCfg{e.tpb, e.radius, e.rows};
   return FusedCfg{128, 2, 64};
 }
 

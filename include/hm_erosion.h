@@ -297,6 +297,28 @@ long long hm_batch_round(const hm_batch *batch);
  * into one CUDA graph.  Returns after the results are written. */
 int       hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph);
 
+/* ---- autotuner ----------------------------------------------------------- */
+
+/* No counterpart in the reference.  Times every candidate launch shape of
+ * one solver on a synthetic terrain of nx x ny (steps steps each) and keeps
+ * the fastest for grids of that size class (nx, ny rounded up to powers of
+ * two); solves that leave the choice to the library (time_block 0, no
+ * hm_vpipes_set_launch override) then use it.  Process-wide; do not run
+ * while other threads solve.  kind: HM_JOB_THERMAL or HM_JOB_VPIPES. */
+typedef struct hm_tune_result
+{
+  int   tpb, radius, rows; /* vpipes launch shape (rows: also thermal's blocked kernel) */
+  int   time_block;        /* thermal steps per launch                               */
+  float ms_per_step;
+  int   candidates;
+} hm_tune_result;
+
+int  hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_result *result);
+/* the tuned table as text, and back (unknown or invalid lines skipped) */
+int  hm_autotune_save(const char *path);
+int  hm_autotune_load(const char *path, int *loaded);
+void hm_autotune_clear(void);
+
 /* ---- instrumentation --------------------------------------------------- */
 
 /* Number of kernel launches issued by this library on the calling thread

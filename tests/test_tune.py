@@ -1,0 +1,53 @@
+"""The launch-shape autotuner: tuned shapes are valid candidates, results
+do not depend on them, and the table survives a save / load round trip."""
+import numpy as np
+import pytest
+
+from highmap_b200.inputs import fbm
+from oracle import pyoracle as po
+
+
+def test_load_skips_invalid_lines(built_lib, tmp_path):
+    from highmap_b200 import tune
+    p = tmp_path / "shapes.txt"
+    p.write_text("# header\n"
+                 "vpipes 9 9 128 2 64 0 0.100\n"
+                 "vpipes 10 10 999 2 64 0 0.100\n"      # unsupported threads per CTA
+                 "thermal 9 9 0 0 128 8 0.050\n"
+                 "thermal 9 8 0 0 128 99 0.050\n"       # unsupported block depth
+                 "garbage line\n")
+    tune.clear()
+    assert tune.load(str(p)) == 2
+    out = tmp_path / "out.txt"
+    tune.save(str(out))
+    lines = [l for l in out.read_text().splitlines() if not l.startswith("#")]
+    assert sorted(l.split()[0] for l in lines) == ["thermal", "vpipes"]
+    tune.clear()
+
+
+@pytest.mark.gpu
+def test_autotune_then_parity(gpu, tmp_path):
+    from highmap_b200 import tune
+    tune.clear()
+    rv = tune.autotune(tune.VPIPES, 300, 260, steps=6)
+    rt = tune.autotune(tune.THERMAL, 300, 260, steps=6)
+    assert rv["tpb"] in (128, 256) and rv["radius"] in (2, 3) and rv["rows"] >= 32
+    assert rt["time_block"] in (1, 2, 4, 8)
+    assert rv["ms_per_step"] > 0 and rt["ms_per_step"] > 0
+    # the tuned shapes are used for this size class; results stay the oracle's
+    z0 = fbm(300, 260, seed=3)
+    z = z0.copy()
+    gpu.thermal(z, 1 / 300, 21)
+    want, _ = po.thermal(z0, np.full_like(z0, 1 / 300, dtype=np.float32), 21)
+    assert np.array_equal(z, want)
+    cfg = dict(maintain_water_volume=0, flux_diffusion=0, dt=0.1, gravity=9.81, rain_per_step=1e-4,
+               initial_water=0.0, iterations=30)
+    z = z0.copy()
+    gpu.hydraulic_vpipes(z, **cfg)
+    want = po.vpipes(z0, po.VpipesParams.make(**cfg))[0]
+    assert np.array_equal(z, want)
+    p = tmp_path / "t.txt"
+    tune.save(str(p))
+    tune.clear()
+    assert tune.load(str(p)) == 2
+    tune.clear()
