@@ -107,8 +107,9 @@ int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_re
   std::vector<hm::TuneEntry> cands;
   if (kind == HM_JOB_VPIPES)
   {
-    const int shapes[][3] = {{128, 2, 32}, {128, 2, 64}, {128, 2, 128}, {256, 2, 64},
-                             {128, 3, 32}, {128, 3, 64}, {256, 3, 64}};
+    /* {0, 0, 0}: the tiled step kernels; the others: the streaming kernel */
+    const int shapes[][3] = {{0, 0, 0},     {128, 2, 32}, {128, 2, 64}, {128, 2, 128},
+                             {256, 2, 64},  {128, 3, 32}, {128, 3, 64}, {256, 3, 64}};
     for (auto &c : shapes) cands.push_back(hm::TuneEntry{c[0], c[1], c[2], 0, 0.f});
   }
   else
@@ -144,7 +145,9 @@ int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_re
       HM_CUDA_TRY(cudaEventRecord(e0, s));
       if (kind == HM_JOB_VPIPES)
       {
-        if ((st = hm_vpipes_set_launch(c.tpb, c.radius, c.rows))) break;
+        if (c.tpb == 0) st = hm_vpipes_set_algorithm(HM_VPIPES_TILED);
+        else if (!(st = hm_vpipes_set_algorithm(HM_VPIPES_STREAMING))) st = hm_vpipes_set_launch(c.tpb, c.radius, c.rows);
+        if (st) break;
         st = hm_vpipes_device(ctx, z, nx, ny, &vp, nullptr, nullptr, nullptr, nullptr, nullptr, s);
       }
       else
@@ -166,8 +169,13 @@ int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_re
       best_ms = ms;
     }
   }
-  if (kind == HM_JOB_VPIPES) hm_vpipes_set_launch(0, 0, 0);
-  else hm_thermal_set_launch(0);
+  if (kind == HM_JOB_VPIPES)
+  {
+    hm_vpipes_set_launch(0, 0, 0);
+    hm_vpipes_set_algorithm(HM_VPIPES_AUTO);
+  }
+  else
+    hm_thermal_set_launch(0);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFreeAsync(z, s);
@@ -227,7 +235,7 @@ int hm_autotune_load(const char *path, int *loaded_out)
       continue;
     std::string k(kind);
     /* keep only shapes the kernels accept */
-    if (k == "vpipes" && hm_vpipes_set_launch(e.tpb, e.radius, e.rows) == HM_OK)
+    if (k == "vpipes" && (e.tpb == 0 || hm_vpipes_set_launch(e.tpb, e.radius, e.rows) == HM_OK))
     {
       std::lock_guard<std::mutex> lk(hm::g_mu);
       hm::g_vp[{cx, cy}] = e;

@@ -29,6 +29,7 @@
 #include "hm_tune.h"
 #include "hm_vpipes.h"
 #include "hm_vpipes_fused.cuh"
+#include "hm_vpipes_tiled.cuh"
 #include "hm_vpipes_math.cuh"
 
 namespace hm
@@ -146,13 +147,24 @@ struct FusedCfg
 };
 
 static FusedCfg g_cfg_override = {0, 0, 0};
+/* step kernels: 0 = tiled (k_vp_fwe + k_vp_advect), 1 = streaming (k_vp_fused) */
+static int g_algo_override = -1;
 
 FusedCfg vpipes_pick_config(int nx, int ny)
 {
   if (g_cfg_override.tpb) return g_cfg_override;
   TuneEntry e;
-  if (tuned_vpipes(nx, ny, &e)) return FusedCfg{e.tpb, e.radius, e.rows};
+  if (tuned_vpipes(nx, ny, &e) && e.tpb) return FusedCfg{e.tpb, e.radius, e.rows};
   return FusedCfg{128, 2, 64};
+}
+
+int vpipes_pick_algo(int nx, int ny)
+{
+  if (g_algo_override >= 0) return g_algo_override;
+  if (g_cfg_override.tpb) return 1;
+  TuneEntry e;
+  if (tuned_vpipes(nx, ny, &e)) return e.tpb ? 1 : 0;
+  return 0;
 }
 
 static int fused_w(const FusedCfg &c) { return c.tpb - 2 * (c.r + 2); }
@@ -165,8 +177,11 @@ static dim3 fused_grid(const FusedCfg &c, int nx, int ny)
 
 static size_t partials_bytes(int nx, int ny)
 {
-  /* the smallest strip and chunk any configuration uses bound the grid */
-  size_t blocks = (size_t)((nx + 63) / 64 + 1) * ((ny + 31) / 32 + 1);
+  /* one slot per block of the step grid: the tiled kernel's 32 x 16 tiles
+   * outnumber the streaming kernel's strips and chunks */
+  size_t blocks = (size_t)((nx + FT_TX - 1) / FT_TX) * ((ny + FT_TY - 1) / FT_TY);
+  const size_t streaming = (size_t)((nx + 63) / 64 + 1) * ((ny + 31) / 32 + 1);
+  if (blocks < streaming) blocks = streaming;
   if (blocks < 2 * VP_INIT_BLOCKS) blocks = 2 * VP_INIT_BLOCKS;
   return align_up(blocks * sizeof(double), 256);
 }
@@ -194,9 +209,9 @@ static size_t defer_cap(int nx, int ny)
 size_t vpipes_scratch_bytes(int nx, int ny)
 {
   const size_t n = align_up((size_t)nx * ny, 64);
-  /* state copy B (7 grids), state A's d, s and fluxes (6 grids), u and v,
-   * fp64 partials, the scalar block, the deferred list */
-  return n * sizeof(float) * 15 + partials_bytes(nx, ny) + align_up(sizeof(VpScalars), 256) +
+  /* state copy B (7 grids), state A's d, s and fluxes (6 grids), u, v and
+   * s1, fp64 partials, the scalar block, the deferred list */
+  return n * sizeof(float) * 16 + partials_bytes(nx, ny) + align_up(sizeof(VpScalars), 256) +
          align_up(defer_cap(nx, ny) * sizeof(Deferred), 256);
 }
 
@@ -260,6 +275,61 @@ static int launch_step(const FusedCfg &cfg, const VpStep &st, const VpConst &c, 
   return fail(HM_ERR_INVALID_ARGUMENT, "vpipes: unsupported fused configuration");
 }
 
+/* the steps of vpipes_core with the tiled kernels (k_vp_fwe, k_vp_advect) */
+static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &p, const VpConst &c, VpFields &A,
+                              VpFields &B, float *u_buf, float *v_buf, float *s1, const float *rain,
+                              float *water_depth, float *sediment, float *vel_u, float *vel_v, VpScalars *sc,
+                              double *partials, cudaStream_t s)
+{
+  const size_t n = (size_t)nx * ny;
+  FweIo        io;
+  io.rain = rain;
+  io.maintain = p.maintain_water_volume != 0;
+  io.diffusion = p.flux_diffusion != 0;
+  io.pl_one = p.pipe_length == 1.f;
+  io.kexp_one = p.k_discharge_exp == 1.f;
+  io.s1 = s1;
+  io.u = u_buf;
+  io.v = v_buf;
+  const dim3 g1((nx + FT_TX - 1) / FT_TX, (ny + FT_TY - 1) / FT_TY);
+  const dim3 g2((nx + 255) / 256, ny < 4096 ? ny : 4096);
+  VpFields  *cur = &A, *nxt = &B;
+  int        parity = 0;
+  for (int it = 0; it < p.iterations; it++)
+  {
+    const bool last = it == p.iterations - 1;
+    io.in = VpState{cur->z, cur->d, cur->s, cur->fl, cur->fr, cur->ft, cur->fb};
+    io.out = VpStateOut{nxt->z, nxt->d, nxt->s, nxt->fl, nxt->fr, nxt->ft, nxt->fb, nullptr, nullptr};
+    io.u_out = last ? vel_u : nullptr;
+    io.v_out = last ? vel_v : nullptr;
+    if (io.u_out && !io.v_out) io.v_out = v_buf;
+    if (io.v_out && !io.u_out) io.u_out = u_buf;
+    io.parity = parity;
+    if (io.maintain) k_vp_fwe<true><<<g1, FT_NT, 0, s>>>(io, c, sc, partials);
+    else k_vp_fwe<false><<<g1, FT_NT, 0, s>>>(io, c, sc, partials);
+    HM_LAUNCH_CHECK("k_vp_fwe");
+    k_vp_advect<<<g2, 256, 0, s>>>(s1, u_buf, v_buf, nxt->s, c);
+    HM_LAUNCH_CHECK("k_vp_advect");
+    VpFields *t = cur;
+    cur = nxt;
+    nxt = t;
+    parity ^= 1;
+  }
+  if (cur->z != z) HM_CUDA_TRY(cudaMemcpyAsync(z, cur->z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  if (water_depth)
+  {
+    int rc = vpipes_final_depth(cur->d, rain, sc, parity, p.maintain_water_volume != 0, water_depth, n, s);
+    if (rc) return rc;
+  }
+  if (sediment) HM_CUDA_TRY(cudaMemcpyAsync(sediment, cur->s, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  if (p.iterations == 0)
+  {
+    if (vel_u) HM_CUDA_TRY(cudaMemsetAsync(vel_u, 0, n * sizeof(float), s));
+    if (vel_v) HM_CUDA_TRY(cudaMemsetAsync(vel_v, 0, n * sizeof(float), s));
+  }
+  return HM_OK;
+}
+
 int vpipes_core(float *z,
                 int nx,
                 int ny,
@@ -290,8 +360,8 @@ int vpipes_core(float *z,
   B.fr = base + 10 * na;
   B.ft = base + 11 * na;
   B.fb = base + 12 * na;
-  float     *u_buf = base + 13 * na, *v_buf = base + 14 * na;
-  double    *partials = (double *)(base + 15 * na);
+  float     *u_buf = base + 13 * na, *v_buf = base + 14 * na, *s1_buf = base + 15 * na;
+  double    *partials = (double *)(base + 16 * na);
   VpScalars *sc = (VpScalars *)((char *)partials + partials_bytes(nx, ny));
   VpDefer    df;
   df.list = (Deferred *)((char *)sc + align_up(sizeof(VpScalars), 256));
@@ -307,6 +377,9 @@ int vpipes_core(float *z,
   }
 
   const FusedCfg cfg = vpipes_pick_config(nx, ny);
+  const int      algo = vpipes_pick_algo(nx, ny);
+  if (algo == 0) return vpipes_tiled_steps(z, nx, ny, p, c, A, B, u_buf, v_buf, s1_buf, rain, water_depth, sediment,
+                                           vel_u, vel_v, sc, partials, s);
   VpStep         st;
   st.rain = rain;
   st.H = cfg.h;
@@ -352,6 +425,14 @@ int vpipes_core(float *z,
 }
 
 } // namespace hm
+
+extern "C" int hm_vpipes_set_algorithm(int algo)
+{
+  hm::clear_error();
+  if (algo < -1 || algo > 1) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes_set_algorithm: unknown algorithm");
+  hm::g_algo_override = algo;
+  return HM_OK;
+}
 
 extern "C" int hm_vpipes_set_launch(int tpb, int radius, int rows)
 {

@@ -230,6 +230,14 @@ def vpipes_set_launch(tpb: int = 0, radius: int = 2, rows: int = 128) -> None:
     L.check(L.lib().hm_vpipes_set_launch(int(tpb), int(radius), int(rows)))
 
 
+VPIPES_AUTO, VPIPES_TILED, VPIPES_STREAMING = -1, 0, 1
+
+
+def vpipes_set_algorithm(algo: int = VPIPES_AUTO) -> None:
+    """Step kernels of the vpipes solver (tiled, streaming, or auto)."""
+    L.check(L.lib().hm_vpipes_set_algorithm(int(algo)))
+
+
 def thermal_set_launch(rows: int = 0) -> None:
     """Output rows per CTA of the blocked thermal kernel (0: built-in)."""
     L.check(L.lib().hm_thermal_set_launch(int(rows)))

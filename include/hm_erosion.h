@@ -237,6 +237,17 @@ int hm_vpipes_device(hm_context             *ctx,
  * restores the built-in choice.  Results do not depend on the shape. */
 int hm_vpipes_set_launch(int tpb, int radius, int rows);
 
+/* Step kernels of the vpipes solver, process-wide: HM_VPIPES_TILED (flow,
+ * water and erosion in one kernel over 32 x 16 tiles, then an advection
+ * gather), HM_VPIPES_STREAMING (all four passes in one kernel streaming
+ * down column strips, shaped by hm_vpipes_set_launch), or
+ * HM_VPIPES_AUTO (-1: the tuned or built-in choice).  Results do not
+ * depend on it. */
+#define HM_VPIPES_AUTO (-1)
+#define HM_VPIPES_TILED 0
+#define HM_VPIPES_STREAMING 1
+int hm_vpipes_set_algorithm(int algo);
+
 /* Output rows per CTA of the temporally blocked thermal kernel,
  * process-wide (8..4096; 0 restores the built-in choice).  Results do not
  * depend on it. */
