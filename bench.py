@@ -61,9 +61,11 @@ def _args():
     ap.add_argument("--size", type=int, default=N_SIDE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=["plain", "batch", "serve"], default="plain",
+    ap.add_argument("--form", choices=["plain", "batch", "serve", "sweep"], default="plain",
                     help="plain: the drop-in headline; batch: 256 mixed jobs batched vs plain calls; "
-                         "serve: Poisson request stream, continuous batching vs plain FIFO")
+                         "serve: Poisson request stream, continuous batching vs plain FIFO; "
+                         "sweep: thermal and vpipes at 1024^2..16384^2, 200 iterations, rates and errors")
+    ap.add_argument("--sizes", default="1024,2048,4096,8192,16384", help="grid sides of the sweep form")
     ap.add_argument("--jobs", type=int, default=256, help="jobs of the batch form")
     ap.add_argument("--requests", type=int, default=100, help="requests per rate of the serve form")
     ap.add_argument("--vpipes-launch", default=None,
@@ -167,6 +169,13 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _vp_kernels(shape):
+    """Kernels of one vpipes step for the launch shape in use."""
+    if shape and shape.get("tpb"):
+        return "k_vp_fused + k_vp_fixup"
+    return "k_vp_fwe + k_vp_advect"
+
+
 def _traffic():
     """dram bytes per vpipes launch from the committed ncu summary, if any."""
     try:
@@ -181,7 +190,10 @@ def _traffic():
 
 def _cpu_rates(n, budget_s=12.0, use_ref=True):
     """Cell-update rates of the CPU implementation on a bounded sample:
-    a few thermal and vpipes iterations on the full n x n inputs."""
+    a few thermal and vpipes iterations on the full n x n inputs, about
+    budget_s seconds of work in all.  The per-iteration cost is sized from
+    runs of 1 and 3 iterations, so fixed per-call costs (copies, thread
+    start-up) do not shrink the sample."""
     import numpy as np
 
     from oracle import pyoracle as po
@@ -202,9 +214,9 @@ def _cpu_rates(n, budget_s=12.0, use_ref=True):
         vp(z, p)
         return time.perf_counter() - t
 
-    # one iteration each to size the sample, then the sample itself
-    t1 = max(t_thermal(1), 1e-3)
-    v1 = max(t_vpipes(1), 1e-3)
+    # per-iteration cost from 1 and 3 iterations, then the sample itself
+    t1 = max((t_thermal(3) - t_thermal(1)) / 2, 1e-4)
+    v1 = max((t_vpipes(3) - t_vpipes(1)) / 2, 1e-4)
     kt = max(1, int(0.35 * budget_s / t1))
     kv = max(1, int(0.65 * budget_s / v1))
     tt = t_thermal(kt)
@@ -292,8 +304,6 @@ def run_ours(a):
     if not G.init_opencl():
         raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
     ctx = G.Context(local)
-    if a.vpipes_launch:
-        G.vpipes_set_launch(*[int(x) for x in a.vpipes_launch.split(",")])
     n = a.size
     cells = float(n) * n
     z, talus, bed = _inputs(n)
@@ -307,6 +317,10 @@ def run_ours(a):
     from highmap_b200 import tune
     tuned = {"vpipes": tune.autotune(tune.VPIPES, n, n, steps=20, ctx=ctx),
              "thermal": tune.autotune(tune.THERMAL, n, n, steps=40, ctx=ctx)}
+    if a.vpipes_launch:  # an explicit shape overrides the tuned one (the tuner clears overrides)
+        shape = [int(x) for x in a.vpipes_launch.split(",")]
+        G.vpipes_set_launch(*shape)
+        tuned["vpipes"] = {"tpb": shape[0], "radius": shape[1], "rows": shape[2], "override": True}
     pv = G.vpipes_params(**dict(CONFIG2_VPIPES, iterations=VPIPES_ITERS))
     stream = torch.cuda.Stream(device=dev)
 
@@ -346,12 +360,15 @@ def run_ours(a):
     G.launch_count_reset()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    # NVTX range "timed": lets a profiler's launch list select exactly these steps
+    torch.cuda.nvtx.range_push("timed")
     with torch.cuda.stream(stream):
         t_start.record(stream)
         for k in range(a.steps):
             step(ev[k])
         t_end.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     launches = G.launch_count()
     if world > 1:
         dist.barrier()
@@ -429,7 +446,7 @@ def run_ours(a):
                 "thermal_roofline": {"bound": "hbm", "achieved": th_achieved, "peak": peak, "unit": "GB/s",
                                      "frac": th_achieved / peak, "bytes_per_cell_update": THERMAL_BYTES},
             },
-            "roofline": {"bound": "hbm", "kernel": "vpipes step", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": "vpipes step (%s)" % _vp_kernels(tuned["vpipes"]), "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "bytes_per_cell_update": VPIPES_BYTES},
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
@@ -439,6 +456,134 @@ def run_ours(a):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------- sweep
+
+SWEEP_ITERS = 200
+SWEEP_FULL_CHECK = 2048  # sides up to this are checked against the oracle on the whole grid
+SWEEP_BAND = 256         # larger sides: the top SWEEP_BAND rows, run by the oracle with a halo
+
+
+def _errors(got, want, z0):
+    """max / mean absolute error (as a fraction of the input height range),
+    the relative L1 distance of HighMap's array comparison
+    (HighMap/src/dbg/assert.cpp:47-70: sum|a-b| / min(sum|a|, sum|b|)) and
+    whether the two fields are bit-identical."""
+    import numpy as np
+    g = got.astype(np.float64)
+    w = want.astype(np.float64)
+    d = np.abs(g - w)
+    rng = float(z0.max() - z0.min()) or 1.0
+    den = min(float(np.abs(g).sum()), float(np.abs(w).sum()))
+    return {"max_abs_of_range": float(d.max()) / rng, "mean_abs_of_range": float(d.mean()) / rng,
+            "rel_l1": float(d.sum()) / den if den else float(d.sum()), "bit_exact": bool(np.array_equal(got, want))}
+
+
+def run_sweep(a):
+    """Thermal and vpipes (the plain drop-in configuration's parameters) on
+    square grids, 200 iterations each, seeds 10.. by size: device-timed
+    cell-updates/s and algorithmic GB/s against the measured copy bandwidth,
+    the autotuner's launch shapes, mass drift, and errors of the GPU result
+    against the fp32 oracle and the fp64 oracle (whole grid up to 2048^2;
+    above, the top 256 rows, which the oracle recomputes on a band with a
+    halo wider than the information reach)."""
+    import numpy as np
+    import torch
+
+    from highmap_b200 import gpu as G
+    from highmap_b200 import tune
+    from highmap_b200.inputs import fbm
+    from oracle import pyoracle as po
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if not G.init_opencl():
+        raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
+    ctx = G.Context(local)
+    dev = torch.device("cuda", local)
+    peak, peak_kind = _peaks()
+    sizes = [int(x) for x in a.sizes.split(",")]
+    it = SWEEP_ITERS
+    pv = dict(CONFIG2_VPIPES)
+    rows = []
+    for k, n in enumerate(sizes):
+        seed = 10 + k
+        z0 = fbm(n, n, seed=seed)
+        talus = ((0.5 + fbm(n, n, seed=seed + 100)) / n).astype(np.float32)
+        bed = (0.3 * z0).astype(np.float32)
+        shapes = {"vpipes": tune.autotune(tune.VPIPES, n, n, steps=20, ctx=ctx),
+                  "thermal": tune.autotune(tune.THERMAL, n, n, steps=40, ctx=ctx)}
+        zd = torch.from_numpy(z0).to(dev)
+        td = torch.from_numpy(talus).to(dev)
+        bd = torch.from_numpy(bed).to(dev)
+        zt = torch.empty_like(zd)
+        zv = torch.empty_like(zd)
+        wd = torch.empty_like(zd)
+        sd = torch.empty_like(zd)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        for rep in range(2):  # the first pass warms up
+            zt.copy_(zd)
+            zv.copy_(zd)
+            torch.cuda.synchronize()
+            e[0].record()
+            G.thermal_device(zt, td, it, bedrock=bd, ctx=ctx)
+            e[1].record()
+            e[2].record()
+            G.hydraulic_vpipes_device(zv, G.vpipes_params(**dict(pv, iterations=it)), None, wd, sd, ctx=ctx)
+            e[3].record()
+            torch.cuda.synchronize()
+        cells = float(n) * n
+        t_th = e[0].elapsed_time(e[1]) * 1e-3
+        t_vp = e[2].elapsed_time(e[3]) * 1e-3
+        got_t = zt.cpu().numpy()
+        got_v, got_w, got_s = zv.cpu().numpy(), wd.cpu().numpy(), sd.cpu().numpy()
+        row = {"n": n, "seed": seed, "launch_shapes": shapes,
+               "thermal": {"cell_updates_per_s": cells * it / t_th,
+                           "gb_per_s": THERMAL_BYTES * cells * it / t_th / 1e9,
+                           "frac": THERMAL_BYTES * cells * it / t_th / 1e9 / peak,
+                           "mass_drift": abs(float(got_t.astype(np.float64).sum() - z0.astype(np.float64).sum())) /
+                           float(np.abs(z0.astype(np.float64)).sum())},
+               "vpipes": {"cell_updates_per_s": cells * it / t_vp,
+                          "gb_per_s": VPIPES_BYTES * cells * it / t_vp / 1e9,
+                          "frac": VPIPES_BYTES * cells * it / t_vp / 1e9 / peak,
+                          # terrain + suspended sediment (the water itself is not conserved: rain and
+                          # evaporation); erosion moves material between the two, advection resamples s
+                          "material_drift": abs(float((got_v.astype(np.float64) + got_s).sum()) -
+                                                float(z0.astype(np.float64).sum())) /
+                          float(np.abs(z0.astype(np.float64)).sum()),
+                          "water_depth_max": float(got_w.max())}}
+        # errors against the oracle: whole grid, or the top band with a halo
+        if n <= SWEEP_FULL_CHECK:
+            r1, sl = n, slice(None)
+        else:
+            r1, sl = SWEEP_BAND + it + 16, slice(0, SWEEP_BAND)
+        scope = "whole grid" if n <= SWEEP_FULL_CHECK else "rows 0..%d (oracle on %d rows)" % (SWEEP_BAND - 1, r1)
+        ref_t32, _ = po.thermal(z0[:r1], talus[:r1], it, bedrock=bed[:r1])
+        ref_t64, _ = po.thermal(z0[:r1], talus[:r1], it, bedrock=bed[:r1], dtype=np.float64)
+        pp = po.VpipesParams.make(**dict(pv, iterations=it))
+        ref_v32 = po.vpipes(z0[:r1], pp)[0]
+        ref_v64 = po.vpipes(z0[:r1], pp, dtype=np.float64)[0]
+        row["thermal"]["vs_oracle_fp32"] = _errors(got_t[sl], ref_t32[sl], z0)
+        row["thermal"]["vs_oracle_fp64"] = _errors(got_t[sl], ref_t64[sl], z0)
+        row["vpipes"]["vs_oracle_fp32"] = _errors(got_v[sl], ref_v32[sl], z0)
+        row["vpipes"]["vs_oracle_fp64"] = _errors(got_v[sl], ref_v64[sl], z0)
+        row["checked"] = scope
+        rows.append(row)
+        print(json.dumps({"sweep_row": row}), flush=True)
+        del zd, td, bd, zt, zv, wd, sd
+        torch.cuda.empty_cache()
+    out = {"metric": "cell-updates/s and GB/s vs the HBM roofline, thermal and vpipes, 200 iterations per size",
+           "value": max(r["vpipes"]["cell_updates_per_s"] for r in rows), "unit": "cell-updates/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic", "form": "sweep",
+           "config": {"workload": "size sweep", "sizes": sizes, "iterations": it, "peak_gbs": peak,
+                      "peak_kind": peak_kind, "bytes_per_cell_update": {"thermal": THERMAL_BYTES,
+                                                                          "vpipes": VPIPES_BYTES}},
+           "rows": rows}
+    print(json.dumps(out), flush=True)
+    ctx.close()
     return 0
 
 
@@ -481,6 +626,8 @@ def main():
     a = _args()
     if a.impl == "reference":
         return run_reference(a)
+    if a.form == "sweep":
+        return run_sweep(a)
     if a.form != "plain":
         return run_form(a)
     return run_ours(a)

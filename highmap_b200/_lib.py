@@ -28,6 +28,8 @@ EXPORTED = (
     "hm_init", "hm_context_create", "hm_context_destroy", "hm_context_trim",
     "hm_status_string", "hm_last_error", "hm_thermal_default_options",
     "hm_thermal", "hm_thermal_scalar", "hm_thermal_masked", "hm_thermal_device",
+    "hm_thermal_auto_bedrock", "hm_thermal_auto_bedrock_scalar", "hm_thermal_auto_bedrock_masked",
+    "hm_thermal_auto_bedrock_device",
     "hm_vpipes_default_params", "hm_vpipes", "hm_vpipes_device",
     "hm_launch_count", "hm_launch_count_reset",
     "hm_thermal_device_noalloc", "hm_vpipes_set_launch", "hm_thermal_set_launch",
@@ -115,6 +117,10 @@ def _declare(lib):
     lib.hm_thermal_scalar.argtypes = [vp, vp, i, i, f, i, vp, vp, vp]
     lib.hm_thermal_masked.argtypes = [vp, vp, i, i, vp, vp, i, vp, vp, vp]
     lib.hm_thermal_device.argtypes = [vp, vp, i, i, vp, f, i, vp, vp, vp, vp, vp]
+    lib.hm_thermal_auto_bedrock.argtypes = [vp, vp, i, i, vp, i, vp, vp]
+    lib.hm_thermal_auto_bedrock_scalar.argtypes = [vp, vp, i, i, f, i, vp, vp]
+    lib.hm_thermal_auto_bedrock_masked.argtypes = [vp, vp, i, i, vp, vp, i, vp, vp]
+    lib.hm_thermal_auto_bedrock_device.argtypes = [vp, vp, i, i, vp, f, i, vp, vp, vp, vp]
     lib.hm_vpipes_default_params.argtypes = [vp]
     lib.hm_vpipes.argtypes = [vp, vp, i, i, vp, vp, vp, vp, vp, vp]
     lib.hm_vpipes_device.argtypes = [vp, vp, i, i, vp, vp, vp, vp, vp, vp, vp]

@@ -33,7 +33,7 @@ struct Slab
 
 int thermal_host(hm_context *ctx, float *z, int nx, int ny, const float *talus, float talus_value,
                  int iterations, const float *bedrock, float *depo, const float *mask,
-                 const hm_thermal_options *opts)
+                 const hm_thermal_options *opts, bool auto_bed = false)
 {
   hm::clear_error();
   if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "thermal: ctx is NULL");
@@ -42,7 +42,7 @@ int thermal_host(hm_context *ctx, float *z, int nx, int ny, const float *talus, 
   if ((st = hm::use_device(ctx->device))) return st;
   const size_t n = (size_t)nx * ny;
   const size_t nbytes = n * sizeof(float);
-  const bool   need_z0 = depo || mask;
+  const bool   need_z0 = depo || mask || auto_bed;
   size_t       fields = 1 + (talus ? 1 : 0) + (bedrock ? 1 : 0) + (depo ? 1 : 0) + (mask ? 1 : 0);
   size_t total = fields * align_up(nbytes, 256) + align_up(hm::thermal_scratch_floats(nx, ny, need_z0) * 4, 256);
   void  *ws = nullptr;
@@ -59,7 +59,7 @@ int thermal_host(hm_context *ctx, float *z, int nx, int ny, const float *talus, 
   if (dt) HM_CUDA_TRY(cudaMemcpyAsync(dt, talus, nbytes, cudaMemcpyHostToDevice, s));
   if (db) HM_CUDA_TRY(cudaMemcpyAsync(db, bedrock, nbytes, cudaMemcpyHostToDevice, s));
   if (dm) HM_CUDA_TRY(cudaMemcpyAsync(dm, mask, nbytes, cudaMemcpyHostToDevice, s));
-  st = hm::thermal_core(ctx->device, dz, nx, ny, dt, talus_value, iterations, db, dd, dm, opts, scr, s);
+  st = hm::thermal_core(ctx->device, dz, nx, ny, dt, talus_value, iterations, db, dd, dm, opts, scr, s, auto_bed);
   if (st)
   {
     cudaStreamSynchronize(s);
@@ -112,6 +112,42 @@ int hm_thermal_device(hm_context *ctx, float *z, int nx, int ny, const float *ta
                           opts, (float *)ws, (cudaStream_t)stream);
 }
 
+int hm_thermal_auto_bedrock(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
+                            float *deposition_map, const hm_thermal_options *opts)
+{
+  if (!talus) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_auto_bedrock: talus is NULL");
+  return thermal_host(ctx, z, nx, ny, talus, 0.f, iterations, nullptr, deposition_map, nullptr, opts, true);
+}
+
+int hm_thermal_auto_bedrock_scalar(hm_context *ctx, float *z, int nx, int ny, float talus, int iterations,
+                                   float *deposition_map, const hm_thermal_options *opts)
+{
+  return thermal_host(ctx, z, nx, ny, nullptr, talus, iterations, nullptr, deposition_map, nullptr, opts, true);
+}
+
+int hm_thermal_auto_bedrock_masked(hm_context *ctx, float *z, int nx, int ny, const float *mask,
+                                   const float *talus, int iterations, float *deposition_map,
+                                   const hm_thermal_options *opts)
+{
+  if (!talus) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_auto_bedrock_masked: talus is NULL");
+  return thermal_host(ctx, z, nx, ny, talus, 0.f, iterations, nullptr, deposition_map, mask, opts, true);
+}
+
+int hm_thermal_auto_bedrock_device(hm_context *ctx, float *z, int nx, int ny, const float *talus,
+                                   float talus_value, int iterations, float *deposition_map, const float *mask,
+                                   const hm_thermal_options *opts, void *stream)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_auto_bedrock_device: ctx is NULL");
+  int st = hm::thermal_check_args(z, nx, ny, iterations, opts);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::thermal_scratch_floats(nx, ny, true) * sizeof(float), &ws))) return st;
+  return hm::thermal_core(ctx->device, z, nx, ny, talus, talus_value, iterations, nullptr, deposition_map, mask,
+                          opts, (float *)ws, (cudaStream_t)stream, true);
+}
+
 int hm_vpipes(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_params *params, const float *rain_map,
               float *water_depth, float *sediment, float *vel_u, float *vel_v)
 {
@@ -152,7 +188,11 @@ int hm_vpipes(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_params 
   if (ds) HM_CUDA_TRY(cudaMemcpyAsync(sediment, ds, nbytes, cudaMemcpyDeviceToHost, s));
   if (du) HM_CUDA_TRY(cudaMemcpyAsync(vel_u, du, nbytes, cudaMemcpyDeviceToHost, s));
   if (dv) HM_CUDA_TRY(cudaMemcpyAsync(vel_v, dv, nbytes, cudaMemcpyDeviceToHost, s));
+  unsigned dev_error = 0;
+  HM_CUDA_TRY(cudaMemcpyAsync(&dev_error, hm::vpipes_error_word(scr, nx, ny), sizeof dev_error,
+                              cudaMemcpyDeviceToHost, s));
   HM_CUDA_TRY(cudaStreamSynchronize(s));
+  if (dev_error) return hm::fail(HM_ERR_TIMEOUT, "hm_vpipes: tile loads timed out on the device");
   return HM_OK;
 }
 

@@ -4,6 +4,7 @@
  *
  * Mirrors the reference drivers' interface and error behaviour:
  *   thermal          HighMap/src/erosion/thermal_gpu.cpp:17-96
+ *   thermal_auto_bedrock  HighMap/src/erosion/thermal_gpu.cpp:98-152
  *   hydraulic_vpipes HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
  *   init_opencl      HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134
  * The reference functions return void and report problems only through
@@ -74,9 +75,9 @@ bool same_shape(const Array *a, const Array &z)
 }
 
 void thermal_impl(Array &z, const Array *p_mask, const Array *talus, float talus_value, int iterations,
-                  Array *p_bedrock, Array *p_deposition_map)
+                  Array *p_bedrock, Array *p_deposition_map, bool auto_bed = false)
 {
-  const char *fn = "hmap::gpu::thermal";
+  const char *fn = auto_bed ? "hmap::gpu::thermal_auto_bedrock" : "hmap::gpu::thermal";
   if (!same_shape(talus, z) || !same_shape(p_mask, z) || !same_shape(p_bedrock, z) ||
       z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
   {
@@ -96,7 +97,19 @@ void thermal_impl(Array &z, const Array *p_mask, const Array *talus, float talus
   float             *dp = p_deposition_map ? depo.data() : nullptr;
   const float       *bp = p_bedrock ? p_bedrock->vector.data() : nullptr;
   int                st;
-  if (p_mask)
+  if (auto_bed)
+  {
+    if (p_mask)
+      st = hm_thermal_auto_bedrock_masked(ctx, zw.data(), z.shape.x, z.shape.y, p_mask->vector.data(),
+                                          talus->vector.data(), iterations, dp, nullptr);
+    else if (talus)
+      st = hm_thermal_auto_bedrock(ctx, zw.data(), z.shape.x, z.shape.y, talus->vector.data(), iterations, dp,
+                                   nullptr);
+    else
+      st = hm_thermal_auto_bedrock_scalar(ctx, zw.data(), z.shape.x, z.shape.y, talus_value, iterations, dp,
+                                          nullptr);
+  }
+  else if (p_mask)
     st = hm_thermal_masked(ctx, zw.data(), z.shape.x, z.shape.y, p_mask->vector.data(), talus->vector.data(),
                            iterations, bp, dp, nullptr);
   else if (talus)
@@ -132,6 +145,22 @@ void thermal(Array &z, const Array *p_mask, const Array &talus, int iterations, 
 void thermal(Array &z, float talus, int iterations, Array *p_bedrock, Array *p_deposition_map)
 {
   thermal_impl(z, nullptr, nullptr, talus, iterations, p_bedrock, p_deposition_map);
+}
+
+void thermal_auto_bedrock(Array &z, const Array &talus, int iterations, Array *p_deposition_map)
+{
+  thermal_impl(z, nullptr, &talus, 0.f, iterations, nullptr, p_deposition_map, true);
+}
+
+void thermal_auto_bedrock(Array &z, const Array *p_mask, const Array &talus, int iterations,
+                          Array *p_deposition_map)
+{
+  thermal_impl(z, p_mask, &talus, 0.f, iterations, nullptr, p_deposition_map, true);
+}
+
+void thermal_auto_bedrock(Array &z, float talus, int iterations, Array *p_deposition_map)
+{
+  thermal_impl(z, nullptr, nullptr, talus, iterations, nullptr, p_deposition_map, true);
 }
 
 void hydraulic_vpipes(Array &z, float water_height, bool maintain_water_volume, float evap_rate, int iterations,

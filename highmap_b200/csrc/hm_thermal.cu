@@ -53,7 +53,8 @@ __global__ void __launch_bounds__(STEP_BX *STEP_BY)
                    int ny,
                    const float *__restrict__ talus,
                    float talus_value,
-                   const float *__restrict__ bedrock)
+                   const float *__restrict__ bedrock,
+                   int first)
 {
   const int i = blockIdx.x * STEP_BX + threadIdx.x;
   const int j = blockIdx.y * STEP_BY + threadIdx.y;
@@ -71,7 +72,105 @@ __global__ void __launch_bounds__(STEP_BX *STEP_BY)
   const float  t = TMAP ? __ldg(talus + idx) : talus_value;
   const float  zb = BED != BED_NONE ? __ldg(bedrock + idx) : 0.f;
   b[idx] = thermal_cell<BED>(__ldg(mid), __ldg(mid - 1), __ldg(dn), __ldg(up), __ldg(mid + 1),
-                             __ldg(up - 1), __ldg(dn - 1), __ldg(up + 1), __ldg(dn + 1), t, zb);
+                             __ldg(up - 1), __ldg(dn - 1), __ldg(up + 1), __ldg(dn + 1), t, zb, first != 0);
+}
+
+/* ------------------------------------------------------------------ */
+/* one step per launch, column sweep                                  */
+/* ------------------------------------------------------------------ */
+
+constexpr int SW_NT = 128; /* 4 warps; a warp owns 32 columns              */
+constexpr int SW_P = 8;    /* rows whose loads are issued together          */
+constexpr int SW_H = 64;   /* output rows per CTA (a multiple of SW_P)      */
+
+/* One Jacobi step.  A warp walks down SW_H rows of its 32 columns; every
+ * row of z is loaded once per warp (lanes 0 and 31 also load the column
+ * just outside the warp) and the west / east neighbours come from warp
+ * shuffles, so a cell costs two coalesced loads per 32 cells instead of
+ * nine loads.  The loads of SW_P rows (z, talus, bedrock) are issued
+ * before any of them is used, which keeps enough bytes in flight to cover
+ * the HBM latency.  Cell rule and border copies as k_thermal_step, so the
+ * two kernels give identical bits. */
+template <bool TMAP, int BED>
+__global__ void __launch_bounds__(SW_NT)
+    k_thermal_sweep(const float *__restrict__ a,
+                    float *__restrict__ b,
+                    int nx,
+                    int ny,
+                    const float *__restrict__ talus,
+                    float talus_value,
+                    const float *__restrict__ bedrock,
+                    int first)
+{
+  const int lane = threadIdx.x & 31;
+  const int wx = (blockIdx.x * (SW_NT / 32) + (threadIdx.x >> 5)) * 32;
+  if (wx >= nx) return; /* the whole warp: no CTA barrier in this kernel */
+  const int  gx = wx + lane;
+  const bool live = gx < nx;
+  const int  gxc = live ? gx : nx - 1;
+  /* lanes 0 and 31 also load the column west / east of the warp */
+  const int  hx = lane == 0 ? max(wx - 1, 0) : (lane == 31 ? min(wx + 32, nx - 1) : gxc);
+  const int  y0 = blockIdx.y * SW_H;
+  const int  y1 = min(ny, y0 + SW_H);
+
+  float vc[SW_P + 2], vl[SW_P + 2], vr[SW_P + 2];
+  {
+    const float *r0 = a + (size_t)max(y0 - 1, 0) * nx, *r1 = a + (size_t)y0 * nx;
+    vc[0] = __ldg(r0 + gxc);
+    vl[0] = __ldg(r0 + hx);
+    vc[1] = __ldg(r1 + gxc);
+    vl[1] = __ldg(r1 + hx);
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+    {
+      const float up = __shfl_up_sync(0xffffffffu, vc[q], 1), dn = __shfl_down_sync(0xffffffffu, vc[q], 1);
+      vr[q] = lane == 31 ? vl[q] : dn;
+      vl[q] = lane == 0 ? vl[q] : up;
+    }
+  }
+  for (int j0 = y0; j0 < y1; j0 += SW_P)
+  {
+    float tl[SW_P], bd[SW_P];
+#pragma unroll
+    for (int q = 0; q < SW_P; q++)
+    {
+      const float *r = a + (size_t)min(j0 + 1 + q, ny - 1) * nx;
+      vc[q + 2] = __ldg(r + gxc);
+      vl[q + 2] = __ldg(r + hx); /* the halo value until the shuffles below */
+      const size_t o = (size_t)min(j0 + q, ny - 1) * nx + gxc;
+      tl[q] = TMAP ? __ldg(talus + o) : talus_value;
+      bd[q] = BED != BED_NONE ? __ldg(bedrock + o) : 0.f;
+    }
+#pragma unroll
+    for (int q = 2; q < SW_P + 2; q++)
+    {
+      const float up = __shfl_up_sync(0xffffffffu, vc[q], 1), dn = __shfl_down_sync(0xffffffffu, vc[q], 1);
+      vr[q] = lane == 31 ? vl[q] : dn;
+      vl[q] = lane == 0 ? vl[q] : up;
+    }
+#pragma unroll
+    for (int q = 0; q < SW_P; q++)
+    {
+      const int j = j0 + q;
+      if (!live || j >= y1) continue;
+      float out;
+      /* apply_boundaries, _common_index.cl:106-132 */
+      if (gx == 0) out = vr[q + 1];
+      else if (gx == nx - 1) out = vl[q + 1];
+      else if (j == 0) out = vc[q + 2];
+      else if (j == ny - 1) out = vc[q];
+      else
+        out = thermal_cell<BED>(vc[q + 1], vl[q + 1], vc[q + 2], vc[q], vr[q + 1], vl[q], vl[q + 2], vr[q], vr[q + 2],
+                                tl[q], bd[q], first != 0);
+      b[(size_t)j * nx + gx] = out;
+    }
+    vc[0] = vc[SW_P];
+    vl[0] = vl[SW_P];
+    vr[0] = vr[SW_P];
+    vc[1] = vc[SW_P + 1];
+    vl[1] = vl[SW_P + 1];
+    vr[1] = vr[SW_P + 1];
+  }
 }
 
 /* ------------------------------------------------------------------ */
@@ -113,7 +212,8 @@ __global__ void __launch_bounds__(TB_TPB)
                  float talus_value,
                  const float *__restrict__ bedrock,
                  int T,
-                 int H)
+                 int H,
+                 int it0)
 {
   __shared__ float lv0[8][TB_TPB];
   __shared__ float lvk[TB_TMAX - 1][4][TB_TPB];
@@ -167,7 +267,8 @@ __global__ void __launch_bounds__(TB_TPB)
         const size_t q = (size_t)j * nx + gic;
         const float  t = TMAP ? __ldg(talus + q) : talus_value;
         const float  zb = BED != BED_NONE ? __ldg(bedrock + q) : 0.f;
-        out = thermal_cell<BED>(pc[tid], pc[lw], ps[tid], pn[tid], pc[le], pn[lw], ps[lw], pn[le], ps[le], t, zb);
+        out = thermal_cell<BED>(pc[tid], pc[lw], ps[tid], pn[tid], pc[le], pn[lw], ps[lw], pn[le], ps[le], t, zb,
+                                it0 + k == 1);
       }
       if (k == T)
       {
@@ -243,31 +344,50 @@ static int num_sms(int device)
   return n;
 }
 
+/* kernel bedrock mode: auto (bed = z0) or the caller's bedrock grid */
+static int kernel_bed_mode(const float *bed, int bed_mode, bool auto_bed)
+{
+  if (auto_bed) return BED_AUTO;
+  return bed ? (bed_mode == HM_BEDROCK_LITERAL ? BED_LITERAL : BED_INTENDED) : BED_NONE;
+}
+
+/* one-step kernel: 0 = column sweep (k_thermal_sweep), 1 = one cell per
+ * thread (k_thermal_step) */
+static int g_step_kernel = 0;
+
 template <bool TMAP, int BED>
 static void launch_step(const float *a, float *b, int nx, int ny, const float *talus, float tv,
-                        const float *bed, cudaStream_t s)
+                        const float *bed, int first, cudaStream_t s)
 {
+  if (g_step_kernel == 0)
+  {
+    dim3 grid((nx + SW_NT - 1) / SW_NT, (ny + SW_H - 1) / SW_H);
+    k_thermal_sweep<TMAP, BED><<<grid, SW_NT, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
+    return;
+  }
   dim3 block(STEP_BX, STEP_BY);
   dim3 grid((nx + STEP_BX - 1) / STEP_BX, (ny + STEP_BY - 1) / STEP_BY);
-  k_thermal_step<TMAP, BED><<<grid, block, 0, s>>>(a, b, nx, ny, talus, tv, bed);
+  k_thermal_step<TMAP, BED><<<grid, block, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
+}
+
+template <bool TMAP>
+static void step_dispatch_t(const float *a, float *b, int nx, int ny, const float *talus, float tv,
+                            const float *bed, int mode, int first, cudaStream_t s)
+{
+  switch (mode)
+  {
+  case BED_NONE: launch_step<TMAP, BED_NONE>(a, b, nx, ny, talus, tv, bed, first, s); break;
+  case BED_INTENDED: launch_step<TMAP, BED_INTENDED>(a, b, nx, ny, talus, tv, bed, first, s); break;
+  case BED_LITERAL: launch_step<TMAP, BED_LITERAL>(a, b, nx, ny, talus, tv, bed, first, s); break;
+  default: launch_step<TMAP, BED_AUTO>(a, b, nx, ny, talus, tv, bed, first, s); break;
+  }
 }
 
 static void step_dispatch(const float *a, float *b, int nx, int ny, const float *talus, float tv,
-                          const float *bed, int bed_mode, cudaStream_t s)
+                          const float *bed, int mode, int first, cudaStream_t s)
 {
-  const int mode = bed ? (bed_mode == HM_BEDROCK_LITERAL ? BED_LITERAL : BED_INTENDED) : BED_NONE;
-  if (talus)
-  {
-    if (mode == BED_NONE) launch_step<true, BED_NONE>(a, b, nx, ny, talus, tv, bed, s);
-    else if (mode == BED_INTENDED) launch_step<true, BED_INTENDED>(a, b, nx, ny, talus, tv, bed, s);
-    else launch_step<true, BED_LITERAL>(a, b, nx, ny, talus, tv, bed, s);
-  }
-  else
-  {
-    if (mode == BED_NONE) launch_step<false, BED_NONE>(a, b, nx, ny, talus, tv, bed, s);
-    else if (mode == BED_INTENDED) launch_step<false, BED_INTENDED>(a, b, nx, ny, talus, tv, bed, s);
-    else launch_step<false, BED_LITERAL>(a, b, nx, ny, talus, tv, bed, s);
-  }
+  if (talus) step_dispatch_t<true>(a, b, nx, ny, talus, tv, bed, mode, first, s);
+  else step_dispatch_t<false>(a, b, nx, ny, talus, tv, bed, mode, first, s);
 }
 
 /* post-processing of a finished thermal solve (z holds the last step):
@@ -288,29 +408,31 @@ int thermal_finish(int device, float *z, int nx, int ny, const float *z0, float 
 
 template <bool TMAP, int BED>
 static void launch_tb(const float *a, float *b, int nx, int ny, const float *talus, float tv, const float *bed,
-                      int T, int H, cudaStream_t s)
+                      int T, int H, int it0, cudaStream_t s)
 {
   const int W = TB_TPB - 2 * T;
   dim3      grid((nx + W - 1) / W, (ny + H - 1) / H);
-  k_thermal_tb<TMAP, BED><<<grid, TB_TPB, 0, s>>>(a, b, nx, ny, talus, tv, bed, T, H);
+  k_thermal_tb<TMAP, BED><<<grid, TB_TPB, 0, s>>>(a, b, nx, ny, talus, tv, bed, T, H, it0);
+}
+
+template <bool TMAP>
+static void tb_dispatch_t(const float *a, float *b, int nx, int ny, const float *talus, float tv, const float *bed,
+                          int mode, int T, int H, int it0, cudaStream_t s)
+{
+  switch (mode)
+  {
+  case BED_NONE: launch_tb<TMAP, BED_NONE>(a, b, nx, ny, talus, tv, bed, T, H, it0, s); break;
+  case BED_INTENDED: launch_tb<TMAP, BED_INTENDED>(a, b, nx, ny, talus, tv, bed, T, H, it0, s); break;
+  case BED_LITERAL: launch_tb<TMAP, BED_LITERAL>(a, b, nx, ny, talus, tv, bed, T, H, it0, s); break;
+  default: launch_tb<TMAP, BED_AUTO>(a, b, nx, ny, talus, tv, bed, T, H, it0, s); break;
+  }
 }
 
 static void tb_dispatch(const float *a, float *b, int nx, int ny, const float *talus, float tv, const float *bed,
-                        int bed_mode, int T, int H, cudaStream_t s)
+                        int mode, int T, int H, int it0, cudaStream_t s)
 {
-  const int mode = bed ? (bed_mode == HM_BEDROCK_LITERAL ? BED_LITERAL : BED_INTENDED) : BED_NONE;
-  if (talus)
-  {
-    if (mode == BED_NONE) launch_tb<true, BED_NONE>(a, b, nx, ny, talus, tv, bed, T, H, s);
-    else if (mode == BED_INTENDED) launch_tb<true, BED_INTENDED>(a, b, nx, ny, talus, tv, bed, T, H, s);
-    else launch_tb<true, BED_LITERAL>(a, b, nx, ny, talus, tv, bed, T, H, s);
-  }
-  else
-  {
-    if (mode == BED_NONE) launch_tb<false, BED_NONE>(a, b, nx, ny, talus, tv, bed, T, H, s);
-    else if (mode == BED_INTENDED) launch_tb<false, BED_INTENDED>(a, b, nx, ny, talus, tv, bed, T, H, s);
-    else launch_tb<false, BED_LITERAL>(a, b, nx, ny, talus, tv, bed, T, H, s);
-  }
+  if (talus) tb_dispatch_t<true>(a, b, nx, ny, talus, tv, bed, mode, T, H, it0, s);
+  else tb_dispatch_t<false>(a, b, nx, ny, talus, tv, bed, mode, T, H, it0, s);
 }
 
 static int g_tb_rows = 0; /* output rows per CTA of the blocked kernel; 0 = built-in */
@@ -350,13 +472,14 @@ int thermal_core(int device,
                  const float *mask,
                  const hm_thermal_options *opts,
                  float *scratch_buf,
-                 cudaStream_t s)
+                 cudaStream_t s,
+                 bool auto_bed)
 {
   hm_thermal_options o;
   hm_thermal_default_options(&o);
   if (opts) o = *opts;
   const size_t n = (size_t)nx * ny;
-  const bool   need_z0 = depo || mask;
+  const bool   need_z0 = depo || mask || auto_bed;
   float       *tmp = scratch_buf;
   float       *z0 = need_z0 ? scratch_buf + align_up(n, 64) : nullptr;
   (void)device;
@@ -383,6 +506,9 @@ int thermal_core(int device,
   }
   if (tb > TB_TMAX) tb = TB_TMAX;
   if (rows <= 0) rows = 128;
+  /* auto-bedrock reads the input heights as its bedrock */
+  const int    mode = kernel_bed_mode(bedrock, o.bedrock_mode, auto_bed);
+  const float *bed = auto_bed ? z0 : bedrock;
   const float *src = z;
   float       *dst = tmp;
   for (int done = 0; done < iterations;)
@@ -390,12 +516,12 @@ int thermal_core(int device,
     const int T = (iterations - done < tb) ? iterations - done : tb;
     if (tb == 1)
     {
-      step_dispatch(src, dst, nx, ny, talus, talus_value, bedrock, o.bedrock_mode, s);
+      step_dispatch(src, dst, nx, ny, talus, talus_value, bed, mode, done == 0, s);
       HM_LAUNCH_CHECK("k_thermal_step");
     }
     else
     {
-      tb_dispatch(src, dst, nx, ny, talus, talus_value, bedrock, o.bedrock_mode, T, rows, s);
+      tb_dispatch(src, dst, nx, ny, talus, talus_value, bed, mode, T, rows, done, s);
       HM_LAUNCH_CHECK("k_thermal_tb");
     }
     done += T;

@@ -11,10 +11,11 @@ namespace hm
 int    thermal_check_args(const float *z, int nx, int ny, int iterations, const hm_thermal_options *o);
 /* floats of workspace thermal_core needs (one grid, two with a z0 copy) */
 size_t thermal_scratch_floats(int nx, int ny, bool need_z0);
-/* Device pointers; ordered on s.  talus NULL selects talus_value. */
+/* Device pointers; ordered on s.  talus NULL selects talus_value.
+ * auto_bed: thermal_auto_bedrock (bedrock must be NULL; needs the z0 copy). */
 int    thermal_core(int device, float *z, int nx, int ny, const float *talus, float talus_value, int iterations,
                     const float *bedrock, float *depo, const float *mask, const hm_thermal_options *opts,
-                    float *scratch_buf, cudaStream_t s);
+                    float *scratch_buf, cudaStream_t s, bool auto_bed = false);
 /* border extrapolation, deposition map and mask blend after the steps */
 int    thermal_finish(int device, float *z, int nx, int ny, const float *z0, float *depo, const float *mask,
                       cudaStream_t s);

@@ -27,6 +27,8 @@
 #ifndef HM_THERMAL_MATH_CUH
 #define HM_THERMAL_MATH_CUH
 
+#include <cfloat>
+
 namespace hm
 {
 
@@ -85,12 +87,25 @@ enum BedMode
 {
   BED_NONE = 0,
   BED_INTENDED = 1,
-  BED_LITERAL = 2
+  BED_LITERAL = 2,
+  BED_AUTO = 3
 };
 
 /* New value of an interior cell.  BED_INTENDED: max(val + amount, bedrock)
  * when val >= bedrock, else bedrock.  BED_LITERAL: max(val, bedrock), the
- * value thermal.cl:99 leaves. */
+ * value thermal.cl:99 leaves.
+ *
+ * BED_AUTO is thermal_auto_bedrock (thermal.cl:102-145) with `bedrock` =
+ * z0, the heights the solve started from, and `first` set on the first
+ * step.  The reference keeps a bedrock grid: -FLT_MAX before the first
+ * step, then max(z0, z_new) after every update, where
+ * z_new = max(max(val + amount, z0), bedrock) is never below z0 (the
+ * selects return z0 when val + amount is NaN).  So after a step the grid
+ * holds exactly the new value, every later step finds bedrock == val and
+ * passes the gate val >= bedrock, and the grid need not exist: the gate
+ * becomes z0 >= -FLT_MAX (false only for cells that start NaN or -inf,
+ * which then never change) and the last max takes -FLT_MAX on the first
+ * step and val afterwards. */
 template <int BED>
 __device__ __forceinline__ float thermal_cell(float c,
                                               float w,
@@ -102,9 +117,18 @@ __device__ __forceinline__ float thermal_cell(float c,
                                               float ne,
                                               float se,
                                               float talus,
-                                              float bedrock)
+                                              float bedrock,
+                                              bool  first = false)
 {
   if (BED == BED_LITERAL) return c > bedrock ? c : bedrock;
+  if (BED == BED_AUTO)
+  {
+    if (!(bedrock >= -FLT_MAX)) return c;
+    const float x = __fadd_rn(c, thermal_amount(c, w, s, n, e, nw, sw, ne, se, talus));
+    const float zn = x > bedrock ? x : bedrock;
+    const float fl = first ? -FLT_MAX : c;
+    return zn > fl ? zn : fl;
+  }
   float out = c;
   if (BED == BED_NONE || c >= bedrock)
     out = __fadd_rn(c, thermal_amount(c, w, s, n, e, nw, sw, ne, se, talus));

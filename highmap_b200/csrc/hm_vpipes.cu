@@ -17,9 +17,14 @@
  *
  * Kernels
  *   k_vp_init          initial depth, zero sediment and fluxes, V0 and R.
- *   k_vp_fused         one whole step (hm_vpipes_fused.cuh).
+ *   k_vp_fwe(_tma), k_vp_advect   one step as two kernels over 2-D tiles
+ *                      (hm_vpipes_tiled.cuh), the default.
+ *   k_vp_fused         one whole step streaming down column strips
+ *                      (hm_vpipes_fused.cuh).
  *   k_vp_final_depth   water-depth output with the last top-up applied.
  */
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -91,6 +96,7 @@ __global__ void __launch_bounds__(VP_NT) k_vp_init_finish(VpScalars *sc, const d
     sc->slow = 0u;
     sc->defer_count[0] = 0u;
     sc->defer_count[1] = 0u;
+    sc->error = 0u;
   }
 }
 
@@ -276,12 +282,63 @@ static int launch_step(const FusedCfg &cfg, const VpStep &st, const VpConst &c, 
 }
 
 /* the steps of vpipes_core with the tiled kernels (k_vp_fwe, k_vp_advect) */
+/* ---- TMA tensor maps ---------------------------------------------- */
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void                           *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+    {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }();
+  return fn;
+}
+
+/* map of an nx x ny fp32 grid read in boxes of 40 x box_rows, zeros outside */
+static bool encode_grid_map(CUtensorMap *m, const float *base, int nx, int ny, int box_rows)
+{
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
+  cuuint64_t strides[1] = {(cuuint64_t)nx * sizeof(float)};
+  cuuint32_t box[2] = {40u, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1u, 1u};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+/* tensor maps of one state copy; false if the grid or buffers do not meet
+ * the TMA rules (row pitch and bases 16-byte aligned, boxes no larger than
+ * the grid) */
+static bool fwe_maps(const VpFields &f, int nx, int ny, FweMaps *m)
+{
+  if (nx % 4 != 0 || nx < 40 || ny < FT_H2) return false;
+  const float *all[7] = {f.z, f.d, f.s, f.fl, f.fr, f.ft, f.fb};
+  for (const float *q : all)
+    if (!aligned16(q)) return false;
+  return encode_grid_map(&m->z, f.z, nx, ny, FT_H2) && encode_grid_map(&m->d, f.d, nx, ny, FT_H2) &&
+         encode_grid_map(&m->s, f.s, nx, ny, FT_H1) && encode_grid_map(&m->fl, f.fl, nx, ny, FT_H1) &&
+         encode_grid_map(&m->fr, f.fr, nx, ny, FT_H1) && encode_grid_map(&m->ft, f.ft, nx, ny, FT_H1) &&
+         encode_grid_map(&m->fb, f.fb, nx, ny, FT_H1);
+}
+
 static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &p, const VpConst &c, VpFields &A,
                               VpFields &B, float *u_buf, float *v_buf, float *s1, const float *rain,
                               float *water_depth, float *sediment, float *vel_u, float *vel_v, VpScalars *sc,
-                              double *partials, cudaStream_t s)
+                              double *partials, bool allow_tma, cudaStream_t s)
 {
   const size_t n = (size_t)nx * ny;
+  FweMaps      maps[2];
+  const bool   tma = allow_tma && fwe_maps(A, nx, ny, &maps[0]) && fwe_maps(B, nx, ny, &maps[1]);
   FweIo        io;
   io.rain = rain;
   io.maintain = p.maintain_water_volume != 0;
@@ -292,7 +349,8 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
   io.u = u_buf;
   io.v = v_buf;
   const dim3 g1((nx + FT_TX - 1) / FT_TX, (ny + FT_TY - 1) / FT_TY);
-  const dim3 g2((nx + 255) / 256, ny < 4096 ? ny : 4096);
+  const int  row_groups = (ny + ADV_R - 1) / ADV_R;
+  const dim3 g2((nx + 255) / 256, row_groups < 65535 ? row_groups : 65535);
   VpFields  *cur = &A, *nxt = &B;
   int        parity = 0;
   for (int it = 0; it < p.iterations; it++)
@@ -305,9 +363,19 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
     if (io.u_out && !io.v_out) io.v_out = v_buf;
     if (io.v_out && !io.u_out) io.u_out = u_buf;
     io.parity = parity;
-    if (io.maintain) k_vp_fwe<true><<<g1, FT_NT, 0, s>>>(io, c, sc, partials);
-    else k_vp_fwe<false><<<g1, FT_NT, 0, s>>>(io, c, sc, partials);
-    HM_LAUNCH_CHECK("k_vp_fwe");
+    if (tma)
+    {
+      const FweMaps &m = maps[cur == &A ? 0 : 1];
+      if (io.maintain) k_vp_fwe_tma<true><<<g1, FT_NT, 0, s>>>(io, m, c, sc, partials);
+      else k_vp_fwe_tma<false><<<g1, FT_NT, 0, s>>>(io, m, c, sc, partials);
+      HM_LAUNCH_CHECK("k_vp_fwe_tma");
+    }
+    else
+    {
+      if (io.maintain) k_vp_fwe<true><<<g1, FT_NT, 0, s>>>(io, c, sc, partials);
+      else k_vp_fwe<false><<<g1, FT_NT, 0, s>>>(io, c, sc, partials);
+      HM_LAUNCH_CHECK("k_vp_fwe");
+    }
     k_vp_advect<<<g2, 256, 0, s>>>(s1, u_buf, v_buf, nxt->s, c);
     HM_LAUNCH_CHECK("k_vp_advect");
     VpFields *t = cur;
@@ -328,6 +396,13 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
     if (vel_v) HM_CUDA_TRY(cudaMemsetAsync(vel_v, 0, n * sizeof(float), s));
   }
   return HM_OK;
+}
+
+const unsigned *vpipes_error_word(const void *scratch_buf, int nx, int ny)
+{
+  const size_t na = align_up((size_t)nx * ny, 64);
+  const char  *partials = (const char *)scratch_buf + 16 * na * sizeof(float);
+  return &((const VpScalars *)(partials + partials_bytes(nx, ny)))->error;
 }
 
 int vpipes_core(float *z,
@@ -378,8 +453,9 @@ int vpipes_core(float *z,
 
   const FusedCfg cfg = vpipes_pick_config(nx, ny);
   const int      algo = vpipes_pick_algo(nx, ny);
-  if (algo == 0) return vpipes_tiled_steps(z, nx, ny, p, c, A, B, u_buf, v_buf, s1_buf, rain, water_depth, sediment,
-                                           vel_u, vel_v, sc, partials, s);
+  if (algo == 0 || algo == 2)
+    return vpipes_tiled_steps(z, nx, ny, p, c, A, B, u_buf, v_buf, s1_buf, rain, water_depth, sediment, vel_u, vel_v,
+                              sc, partials, algo == 0, s);
   VpStep         st;
   st.rain = rain;
   st.H = cfg.h;
@@ -429,7 +505,7 @@ int vpipes_core(float *z,
 extern "C" int hm_vpipes_set_algorithm(int algo)
 {
   hm::clear_error();
-  if (algo < -1 || algo > 1) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes_set_algorithm: unknown algorithm");
+  if (algo < -1 || algo > 2) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes_set_algorithm: unknown algorithm");
   hm::g_algo_override = algo;
   return HM_OK;
 }

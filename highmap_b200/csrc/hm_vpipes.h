@@ -20,6 +20,9 @@ VpConst vpipes_consts(int nx, int ny, const hm_vpipes_params &p);
 /* initial state of copy A (depth, zero sediment and fluxes) and V0, R */
 int     vpipes_init(const VpFields &A, const float *rain, size_t n, float init_depth, VpScalars *sc,
                     double *partials, cudaStream_t s);
+/* device address of the solve's error word (bit 0: a tile's TMA loads
+ * timed out and the tile was skipped) inside the scratch of vpipes_core */
+const unsigned *vpipes_error_word(const void *scratch_buf, int nx, int ny);
 /* fp64 partial-sum slots vpipes_init needs */
 size_t  vpipes_init_partials();
 /* water-depth output: stored depth plus the top-up of the last step */

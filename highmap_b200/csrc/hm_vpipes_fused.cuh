@@ -63,6 +63,7 @@ struct VpScalars
   unsigned ticket;
   unsigned slow;   /* advection samples taken by the global slow path      */
   unsigned defer_count[2]; /* deferred cells of the step, one per parity   */
+  unsigned error;  /* bit 0: a tile's TMA loads timed out (tile skipped)   */
 };
 
 struct VpStep

@@ -27,6 +27,7 @@
 #include "hm_reduce.cuh"
 #include "hm_vpipes_fused.cuh"
 #include "hm_vpipes_math.cuh"
+#include "hm_tma.cuh"
 
 namespace hm
 {
@@ -36,13 +37,35 @@ constexpr int FT_NT = 256;                     /* threads per CTA             */
 constexpr int FT_W2 = FT_TX + 4, FT_H2 = FT_TY + 4; /* z, depth region (halo 2) */
 constexpr int FT_W1 = FT_TX + 2, FT_H1 = FT_TY + 2; /* s, fluxes region (halo 1) */
 
+/* Shared-memory layout of the staged fields.
+ *   cp.async staging (TMA = false): region 2 (columns x0-2 .. x0+33, rows
+ *     y0-2 .. y0+17) as [20][36]; region 1 (x0-1 .. x0+32, y0-1 .. y0+16) as
+ *     [18][34]; element (0, 0) is the region's first cell.
+ *   TMA staging (TMA = true): every box starts at column x0-4 (a TMA box
+ *     must start on a 16-byte boundary) and is 40 columns wide; region 2
+ *     starts at row y0-2, region 1 at y0-1.  Region-2 column q sits at
+ *     q + 2, region-1 column l at l + 3.  Each array is padded to 20 rows
+ *     so every box starts 128-byte aligned. */
+template <bool TMA>
+struct FweLayout
+{
+  static constexpr int W2 = TMA ? 40 : FT_W2;
+  static constexpr int W1 = TMA ? 40 : FT_W1;
+  static constexpr int H1 = TMA ? FT_H2 : FT_H1; /* allocated rows of region-1 arrays */
+  static constexpr int C2 = TMA ? 2 : 0;         /* column of region-2 cell 0         */
+  static constexpr int C1 = TMA ? 3 : 0;         /* column of region-1 cell 0         */
+};
+
+template <bool TMA>
 struct FweSmem
 {
-  float z[FT_H2][FT_W2];
-  float d[FT_H2][FT_W2];
-  float s[FT_H1][FT_W1];
-  float fo[4][FT_H1][FT_W1];
-  float fn[4][FT_H1][FT_W1];
+  using L = FweLayout<TMA>;
+  alignas(128) float z[FT_H2][L::W2];
+  alignas(128) float d[FT_H2][L::W2];
+  alignas(128) float s[L::H1][L::W1];
+  alignas(128) float fo[4][L::H1][L::W1];
+  float    fn[4][FT_H1][FT_W1];
+  uint64_t bar;
 };
 
 /* the step's grids: old state in, new state out, plus this step's s1, u, v */
@@ -57,19 +80,23 @@ struct FweIo
   float       *u_out, *v_out; /* last step: velocity outputs, nullable */
 };
 
-template <bool MAINTAIN>
-__device__ __forceinline__ void fwe_tile(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials,
-                                         int bx, int by, int nbx, int nby, FweSmem &sm)
+/* tensor maps of the seven input fields of one step (TMA staging):
+ * z and d with a 40 x 20 box, s and the fluxes with a 40 x 18 box */
+struct FweMaps
 {
-  static_assert(FT_TX == 32, "a lane is a column of the tile");
-  const int   tid = threadIdx.x;
-  const int   nx = c.nx, ny = c.ny;
-  const int   x0 = bx * FT_TX, y0 = by * FT_TY;
-  const float add = MAINTAIN ? sc->add[io.parity] : 0.f;
-  const float rvol = MAINTAIN ? sc->rvol : 1.f;
-  const bool  rain_step = c.rps != 0.f;
+  CUtensorMap z, d, s, fl, fr, ft, fb;
+};
 
-  /* stage: z, d on the halo-2 region; s and old fluxes on the halo-1 region */
+/* bytes the seven TMA boxes deliver */
+constexpr unsigned FWE_TMA_BYTES = 4u * 40u * (2u * FT_H2 + 5u * FT_H1);
+
+/* cp.async staging: z, d on the halo-2 region; s and old fluxes on the
+ * halo-1 region; loads clamped to the grid, so every raw neighbour read is
+ * the reference's clamp-to-edge read */
+__device__ __forceinline__ void fwe_stage_cp_async(const FweIo &io, int nx, int ny, int x0, int y0,
+                                                   FweSmem<false> &sm)
+{
+  const int tid = threadIdx.x;
   for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
   {
     const int    ly = e / FT_W2, lx = e - ly * FT_W2;
@@ -89,11 +116,89 @@ __device__ __forceinline__ void fwe_tile(const FweIo &io, const VpConst &c, VpSc
   }
   cp_async_commit();
   cp_async_wait<0>();
+}
+
+/* TMA staging: thread 0 arms the barrier and issues the seven box loads;
+ * every thread waits (bounded).  Boxes read zeros outside the grid, so on
+ * tiles that touch the grid's edge the cells outside are then overwritten
+ * with their clamp-to-edge values (the clamped cell is always inside the
+ * box; the edge test depends only on the tile, so the barrier inside it is
+ * uniform).  Returns false, uniformly across the CTA, if the loads did not
+ * complete in time. */
+__device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int ny, int x0, int y0,
+                                              FweSmem<true> &sm)
+{
+  const int tid = threadIdx.x;
+  if (tid == 0)
+  {
+    mbar_init(&sm.bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0)
+  {
+    mbar_arrive_expect_tx(&sm.bar, FWE_TMA_BYTES);
+    tma_load_2d(&sm.z[0][0], &maps.z, x0 - 4, y0 - 2, &sm.bar);
+    tma_load_2d(&sm.d[0][0], &maps.d, x0 - 4, y0 - 2, &sm.bar);
+    tma_load_2d(&sm.s[0][0], &maps.s, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.fo[0][0][0], &maps.fl, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.fo[1][0][0], &maps.fr, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.fo[2][0][0], &maps.ft, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.fo[3][0][0], &maps.fb, x0 - 4, y0 - 1, &sm.bar);
+  }
+  bool ok = mbar_wait_bounded(&sm.bar, 0);
+  if (!ok) ok = mbar_wait_bounded(&sm.bar, 0); /* loads still in flight: give them a second window */
+  if (!__syncthreads_and(ok)) return false;
+  if (x0 - 2 < 0 || x0 + FT_TX + 2 > nx || y0 - 2 < 0 || y0 + FT_TY + 2 > ny)
+  {
+    /* region 2: columns x0-2 .. x0+33 at smem 2 .. 37, rows y0-2 .. y0+17 */
+    for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
+    {
+      const int ly = e / FT_W2, lx = e - ly * FT_W2;
+      const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
+      if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) continue;
+      const int cy = clampi(gy, 0, ny - 1) - (y0 - 2), cx = clampi(gx, 0, nx - 1) - (x0 - 4);
+      sm.z[ly][lx + 2] = sm.z[cy][cx];
+      sm.d[ly][lx + 2] = sm.d[cy][cx];
+    }
+    /* region 1: columns x0-1 .. x0+32 at smem 3 .. 36, rows y0-1 .. y0+16 */
+    for (int e = tid; e < FT_W1 * FT_H1; e += FT_NT)
+    {
+      const int ly = e / FT_W1, lx = e - ly * FT_W1;
+      const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
+      if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) continue;
+      const int cy = clampi(gy, 0, ny - 1) - (y0 - 1), cx = clampi(gx, 0, nx - 1) - (x0 - 4);
+      sm.s[ly][lx + 3] = sm.s[cy][cx];
+#pragma unroll
+      for (int f = 0; f < 4; f++) sm.fo[f][ly][lx + 3] = sm.fo[f][cy][cx];
+    }
+    /* the copies read in-grid cells that the depth pass rewrites in place */
+    __syncthreads();
+  }
+  return true;
+}
+
+/* One tile of the step on staged fields: depth at the start of the step,
+ * flow on the tile plus a 1-cell ring, then water and erosion on the tile. */
+template <bool MAINTAIN, bool TMA>
+__device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials,
+                                            int bx, int by, int nbx, int nby, FweSmem<TMA> &sm)
+{
+  static_assert(FT_TX == 32, "a lane is a column of the tile");
+  using L = FweLayout<TMA>;
+  constexpr int C1 = L::C1, C2 = L::C2;
+  const int     tid = threadIdx.x;
+  const int     nx = c.nx, ny = c.ny;
+  const int     x0 = bx * FT_TX, y0 = by * FT_TY;
+  const float   add = MAINTAIN ? sc->add[io.parity] : 0.f;
+  const float   rvol = MAINTAIN ? sc->rvol : 1.f;
+  const bool    rain_step = c.rps != 0.f;
+
   /* stored depth -> depth at the start of the step (own elements) */
   for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
   {
     const int   ly = e / FT_W2, lx = e - ly * FT_W2;
-    float      &d = sm.d[ly][lx];
+    float      &d = sm.d[ly][lx + C2];
     const float rn = io.rain ? __ldg(io.rain + (size_t)clampi(y0 - 2 + ly, 0, ny - 1) * nx +
                                     clampi(x0 - 2 + lx, 0, nx - 1))
                              : 1.f;
@@ -106,8 +211,9 @@ __device__ __forceinline__ void fwe_tile(const FweIo &io, const VpConst &c, VpSc
   for (int e = tid; e < FT_W1 * FT_H1; e += FT_NT)
   {
     const int ly = e / FT_W1, lx = e - ly * FT_W1;
-    const int qy = ly + 1, qx = lx + 1; /* region-2 coordinates of the cell */
-    float     fl = sm.fo[0][ly][lx], fr = sm.fo[1][ly][lx], ft = sm.fo[2][ly][lx], fb = sm.fo[3][ly][lx];
+    const int qy = ly + 1, qx = lx + 1 + C2; /* region-2 row and smem column of the cell */
+    const int l1 = lx + C1;
+    float     fl = sm.fo[0][ly][l1], fr = sm.fo[1][ly][l1], ft = sm.fo[2][ly][l1], fb = sm.fo[3][ly][l1];
     const float zc = sm.z[qy][qx], dc = sm.d[qy][qx];
     const float zw = sm.z[qy][qx - 1], dw = sm.d[qy][qx - 1], ze = sm.z[qy][qx + 1], de = sm.d[qy][qx + 1];
     const float zs = sm.z[qy + 1][qx], ds = sm.d[qy + 1][qx], zn = sm.z[qy - 1][qx], dn = sm.d[qy - 1][qx];
@@ -137,7 +243,7 @@ __device__ __forceinline__ void fwe_tile(const FweIo &io, const VpConst &c, VpSc
   }
   __syncthreads();
 
-  /* water and erosion on the tile: warp w takes rows w, w + 4, ...; a lane
+  /* water and erosion on the tile: warp w takes rows w, w + 8, ...; a lane
    * is a column */
   double    part = 0.0;
   const int lane = tid & 31, w = tid >> 5;
@@ -147,6 +253,7 @@ __device__ __forceinline__ void fwe_tile(const FweIo &io, const VpConst &c, VpSc
   const int lxc = lane + 1;
   const int lxw = clampi(gx - 1, 0, nx - 1) - (x0 - 1);
   const int lxe = clampi(gx + 1, 0, nx - 1) - (x0 - 1);
+  const int sc1 = lxc + C1; /* smem column of the cell in region-1 arrays */
   for (int ty = w; ty < FT_TY; ty += FT_NT / 32)
   {
     const int gy = y0 + ty;
@@ -154,7 +261,7 @@ __device__ __forceinline__ void fwe_tile(const FweIo &io, const VpConst &c, VpSc
     const int ly = ty + 1;
     const int lyn = clampi(gy - 1, 0, ny - 1) - (y0 - 1);
     const int lys = clampi(gy + 1, 0, ny - 1) - (y0 - 1);
-    const int qy = ty + 2, qx = lane + 2; /* region-2 coordinates */
+    const int qy = ty + 2, qx = lane + 2 + C2; /* region-2 row and smem column */
     float     d2, u, v;
     const float d1c = sm.d[qy][qx];
     if (io.pl_one)
@@ -165,13 +272,13 @@ __device__ __forceinline__ void fwe_tile(const FweIo &io, const VpConst &c, VpSc
                         sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc], sm.fn[3][lys][lxc], d2, u, v);
     float zo, so;
     if (io.kexp_one)
-      erosion_cell<true>(c, sm.z[qy][qx], sm.s[ly][lxc], sm.z[qy][qx - 1], sm.z[qy][qx + 1], sm.z[qy - 1][qx],
-                         sm.z[qy + 1][qx], sm.s[ly][lxc - 1], sm.s[ly][lxc + 1], sm.s[ly - 1][lxc],
-                         sm.s[ly + 1][lxc], d2, u, v, zo, so);
+      erosion_cell<true>(c, sm.z[qy][qx], sm.s[ly][sc1], sm.z[qy][qx - 1], sm.z[qy][qx + 1], sm.z[qy - 1][qx],
+                         sm.z[qy + 1][qx], sm.s[ly][sc1 - 1], sm.s[ly][sc1 + 1], sm.s[ly - 1][sc1],
+                         sm.s[ly + 1][sc1], d2, u, v, zo, so);
     else
-      erosion_cell<false>(c, sm.z[qy][qx], sm.s[ly][lxc], sm.z[qy][qx - 1], sm.z[qy][qx + 1], sm.z[qy - 1][qx],
-                          sm.z[qy + 1][qx], sm.s[ly][lxc - 1], sm.s[ly][lxc + 1], sm.s[ly - 1][lxc],
-                          sm.s[ly + 1][lxc], d2, u, v, zo, so);
+      erosion_cell<false>(c, sm.z[qy][qx], sm.s[ly][sc1], sm.z[qy][qx - 1], sm.z[qy][qx + 1], sm.z[qy - 1][qx],
+                          sm.z[qy + 1][qx], sm.s[ly][sc1 - 1], sm.s[ly][sc1 + 1], sm.s[ly - 1][sc1],
+                          sm.s[ly + 1][sc1], d2, u, v, zo, so);
     const size_t k = (size_t)gy * nx + gx;
     const float  de = fmul(d2, c.keep);
     io.out.z[k] = zo;
@@ -199,8 +306,35 @@ __device__ __forceinline__ void fwe_tile(const FweIo &io, const VpConst &c, VpSc
 template <bool MAINTAIN>
 __global__ void __launch_bounds__(FT_NT) k_vp_fwe(FweIo io, VpConst c, VpScalars *sc, double *partials)
 {
-  __shared__ FweSmem sm;
-  fwe_tile<MAINTAIN>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  __shared__ FweSmem<false> sm;
+  fwe_stage_cp_async(io, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm);
+  __syncthreads();
+  fwe_compute<MAINTAIN, false>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+}
+
+/* The same step with the input tiles fetched by TMA.  A tile whose loads
+ * time out sets bit 0 of sc->error and writes nothing; with the volume
+ * top-up it still takes part in the grid-wide sum (adding zero) so the
+ * last block's finish is not left waiting for it. */
+template <bool MAINTAIN>
+__global__ void __launch_bounds__(FT_NT)
+    k_vp_fwe_tma(FweIo io, const __grid_constant__ FweMaps maps, VpConst c, VpScalars *sc, double *partials)
+{
+  __shared__ FweSmem<true> sm;
+  if (!fwe_stage_tma(maps, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm))
+  {
+    if (threadIdx.x == 0) atomicOr(&sc->error, 1u);
+    if (MAINTAIN)
+    {
+      const float v0 = sc->v0;
+      float      *outp = &sc->add[io.parity ^ 1];
+      grid_sum_commit<FT_NT>(0.0, partials, &sc->ticket, gridDim.x * gridDim.y,
+                             blockIdx.y * gridDim.x + blockIdx.x,
+                             [&](double total) { *outp = fsub(v0, (float)total); });
+    }
+    return;
+  }
+  fwe_compute<MAINTAIN, true>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
 /* advection of one cell: s_new = bilinear(s1, (i - dt u, j - dt v)) */
@@ -214,7 +348,13 @@ __device__ __forceinline__ float advect_cell(const float *__restrict__ s1, int i
   return blend(t, __ldg(s1 + r0 + t.i0), __ldg(s1 + r0 + t.i1), __ldg(s1 + r1 + t.i0), __ldg(s1 + r1 + t.i1));
 }
 
-/* block x covers 256 columns of the rows blockIdx.y, blockIdx.y + gridDim.y, ... */
+/* Advection over the grid: block x covers 256 columns, and each thread
+ * takes ADV_R consecutive rows of its column at a time, so that the
+ * velocity loads of all ADV_R rows, then all their 4 ADV_R gathers, are in
+ * flight together (the pass is bound by the latency of these two dependent
+ * rounds of loads). */
+constexpr int ADV_R = 4;
+
 __global__ void __launch_bounds__(256) k_vp_advect(const float *__restrict__ s1,
                                                     const float *__restrict__ u,
                                                     const float *__restrict__ v,
@@ -223,10 +363,34 @@ __global__ void __launch_bounds__(256) k_vp_advect(const float *__restrict__ s1,
 {
   const int i = blockIdx.x * 256 + threadIdx.x;
   if (i >= c.nx) return;
-  for (int j = blockIdx.y; j < c.ny; j += gridDim.y)
+  for (int jb = blockIdx.y * ADV_R; jb < c.ny; jb += gridDim.y * ADV_R)
   {
-    const size_t k = (size_t)j * c.nx + i;
-    s_out[k] = advect_cell(s1, i, j, __ldg(u + k), __ldg(v + k), c);
+    float uu[ADV_R], vv[ADV_R];
+#pragma unroll
+    for (int q = 0; q < ADV_R; q++)
+    {
+      const size_t k = (size_t)min(jb + q, c.ny - 1) * c.nx + i;
+      uu[q] = __ldg(u + k);
+      vv[q] = __ldg(v + k);
+    }
+    Tap   t[ADV_R];
+    float g[ADV_R][4];
+#pragma unroll
+    for (int q = 0; q < ADV_R; q++)
+    {
+      const int    j = min(jb + q, c.ny - 1);
+      const float  x = fsub((float)i, fmul(c.dt, uu[q]));
+      const float  y = fsub((float)j, fmul(c.dt, vv[q]));
+      t[q] = linear_tap(x, y, c.nx, c.ny);
+      const size_t r0 = (size_t)t[q].j0 * c.nx, r1 = (size_t)t[q].j1 * c.nx;
+      g[q][0] = __ldg(s1 + r0 + t[q].i0);
+      g[q][1] = __ldg(s1 + r0 + t[q].i1);
+      g[q][2] = __ldg(s1 + r1 + t[q].i0);
+      g[q][3] = __ldg(s1 + r1 + t[q].i1);
+    }
+#pragma unroll
+    for (int q = 0; q < ADV_R; q++)
+      if (jb + q < c.ny) s_out[(size_t)(jb + q) * c.nx + i] = blend(t[q], g[q][0], g[q][1], g[q][2], g[q][3]);
   }
 }
 

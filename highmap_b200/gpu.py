@@ -130,6 +130,37 @@ def thermal(z: np.ndarray, talus, iterations: int = 10, bedrock: np.ndarray | No
                                _ptr(deposition_map), C.byref(opts)))
 
 
+def thermal_auto_bedrock(z: np.ndarray, talus, iterations: int = 10, deposition_map: np.ndarray | None = None,
+                         mask: np.ndarray | None = None, time_block: int = 0,
+                         ctx: Context | None = None) -> None:
+    """Thermal erosion with the reference's self-built bedrock, in place
+    (hmap::gpu::thermal_auto_bedrock, thermal_gpu.cpp:98-152).  ``talus``
+    is a grid or a float; ``mask`` selects the masked overload."""
+    _grid(z, "z", writable=True)
+    shape = z.shape
+    ny, nx = shape
+    ctx = ctx or default_context()
+    opts = thermal_options(BEDROCK_INTENDED, time_block)
+    if deposition_map is not None:
+        _grid(deposition_map, "deposition_map", shape, writable=True)
+    lib = L.lib()
+    if np.isscalar(talus) or (isinstance(talus, np.ndarray) and talus.ndim == 0):
+        if mask is not None:
+            talus = np.full(shape, float(talus), dtype=np.float32)
+        else:
+            L.check(lib.hm_thermal_auto_bedrock_scalar(ctx.handle, _ptr(z), nx, ny, C.c_float(float(talus)),
+                                                       int(iterations), _ptr(deposition_map), C.byref(opts)))
+            return
+    _grid(talus, "talus", shape)
+    if mask is not None:
+        _grid(mask, "mask", shape)
+        L.check(lib.hm_thermal_auto_bedrock_masked(ctx.handle, _ptr(z), nx, ny, _ptr(mask), _ptr(talus),
+                                                   int(iterations), _ptr(deposition_map), C.byref(opts)))
+    else:
+        L.check(lib.hm_thermal_auto_bedrock(ctx.handle, _ptr(z), nx, ny, _ptr(talus), int(iterations),
+                                            _ptr(deposition_map), C.byref(opts)))
+
+
 def vpipes_params(**kw) -> VpipesParams:
     p = VpipesParams()
     L.lib().hm_vpipes_default_params(C.byref(p))
@@ -212,6 +243,22 @@ def thermal_device(z, talus, iterations: int = 10, bedrock=None, deposition_map=
                                       _tptr(mask, "mask", z.shape), C.byref(opts), _stream(stream)))
 
 
+def thermal_auto_bedrock_device(z, talus, iterations: int = 10, deposition_map=None, mask=None,
+                                time_block: int = 0, ctx: Context | None = None, stream=None) -> None:
+    ny, nx = z.shape
+    zp = _tptr(z, "z")
+    ctx = ctx or default_context()
+    opts = thermal_options(BEDROCK_INTENDED, time_block)
+    if isinstance(talus, (int, float)):
+        tp, tv = None, float(talus)
+    else:
+        tp, tv = _tptr(talus, "talus", z.shape), 0.0
+    L.check(L.lib().hm_thermal_auto_bedrock_device(ctx.handle, zp, nx, ny, tp, C.c_float(tv), int(iterations),
+                                                   _tptr(deposition_map, "deposition_map", z.shape),
+                                                   _tptr(mask, "mask", z.shape), C.byref(opts),
+                                                   _stream(stream)))
+
+
 def hydraulic_vpipes_device(z, params: VpipesParams | None = None, rain_map=None, water_depth=None,
                             sediment=None, vel_u=None, vel_v=None, ctx: Context | None = None,
                             stream=None) -> None:
@@ -230,11 +277,12 @@ def vpipes_set_launch(tpb: int = 0, radius: int = 2, rows: int = 128) -> None:
     L.check(L.lib().hm_vpipes_set_launch(int(tpb), int(radius), int(rows)))
 
 
-VPIPES_AUTO, VPIPES_TILED, VPIPES_STREAMING = -1, 0, 1
+VPIPES_AUTO, VPIPES_TILED, VPIPES_STREAMING, VPIPES_TILED_CP_ASYNC = -1, 0, 1, 2
 
 
 def vpipes_set_algorithm(algo: int = VPIPES_AUTO) -> None:
-    """Step kernels of the vpipes solver (tiled, streaming, or auto)."""
+    """Step kernels of the vpipes solver (tiled with TMA staging where the
+    grid allows it, tiled with cp.async staging, streaming, or auto)."""
     L.check(L.lib().hm_vpipes_set_algorithm(int(algo)))
 
 

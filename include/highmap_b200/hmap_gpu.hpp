@@ -3,7 +3,8 @@
  *
  * Source-compatible with the declarations of
  * HighMap/include/highmap/erosion.hpp:1206-1223 (hydraulic_vpipes),
- * :1784-1801 (thermal, three overloads), :1822-1833 (thermal_auto_bedrock)
+ * :1784-1801 (thermal, three overloads), :1824-1838 (thermal_auto_bedrock, three
+ * overloads)
  * and HighMap/include/highmap/opencl/gpu_opencl.hpp:30 (init_opencl).
  * To use HighMap's own hmap::Array, include "highmap/array.hpp" first and
  * define HMAP_B200_EXTERNAL_ARRAY; otherwise this header brings in the
@@ -47,6 +48,22 @@ void thermal(Array &z,
              int    iterations = 10,
              Array *p_bedrock = nullptr,
              Array *p_deposition_map = nullptr);
+
+void thermal_auto_bedrock(Array       &z,
+                          const Array &talus,
+                          int          iterations = 10,
+                          Array       *p_deposition_map = nullptr);
+
+void thermal_auto_bedrock(Array       &z,
+                          const Array *p_mask,
+                          const Array &talus,
+                          int          iterations = 10,
+                          Array       *p_deposition_map = nullptr);
+
+void thermal_auto_bedrock(Array &z,
+                          float  talus,
+                          int    iterations = 10,
+                          Array *p_deposition_map = nullptr);
 
 void hydraulic_vpipes(Array &z,
                       float  water_height = 1e-2f,

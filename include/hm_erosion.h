@@ -145,6 +145,66 @@ int hm_thermal_device(hm_context               *ctx,
                       const hm_thermal_options *opts,
                       void                     *stream);
 
+/* ---- thermal with an automatic bedrock -------------------------------- */
+
+/* Replaces hmap::gpu::thermal_auto_bedrock(Array &z, const Array &talus,
+ * int iterations, Array *p_deposition_map)
+ * (HighMap/include/highmap/erosion.hpp:1824-1827,
+ *  HighMap/src/erosion/thermal_gpu.cpp:98-130, kernel thermal_auto_bedrock
+ *  in HighMap/src/gpu_opencl/kernels/thermal.cl:102-145).  The talus
+ * exchange of hm_thermal with the reference's self-built bedrock: a cell
+ * never drops below its input height nor below its previous value, so the
+ * solve only deposits.  Then the border extrapolation and the deposition
+ * map, as hm_thermal.  opts: only time_block is used (NULL = defaults). */
+int hm_thermal_auto_bedrock(hm_context               *ctx,
+                            float                    *z,
+                            int                       nx,
+                            int                       ny,
+                            const float              *talus,
+                            int                       iterations,
+                            float                    *deposition_map,
+                            const hm_thermal_options *opts);
+
+/* Replaces hmap::gpu::thermal_auto_bedrock(Array &z, float talus,
+ * int iterations, Array *p_deposition_map) (erosion.hpp:1835-1838,
+ * thermal_gpu.cpp:132-139); the talus is a kernel scalar. */
+int hm_thermal_auto_bedrock_scalar(hm_context               *ctx,
+                                   float                    *z,
+                                   int                       nx,
+                                   int                       ny,
+                                   float                     talus,
+                                   int                       iterations,
+                                   float                    *deposition_map,
+                                   const hm_thermal_options *opts);
+
+/* Replaces hmap::gpu::thermal_auto_bedrock(Array &z, const Array *p_mask,
+ * const Array &talus, int iterations, Array *p_deposition_map)
+ * (erosion.hpp:1829-1833, thermal_gpu.cpp:141-152): z = lerp(z, solve(z),
+ * mask).  mask NULL means no mask. */
+int hm_thermal_auto_bedrock_masked(hm_context               *ctx,
+                                   float                    *z,
+                                   int                       nx,
+                                   int                       ny,
+                                   const float              *mask,
+                                   const float              *talus,
+                                   int                       iterations,
+                                   float                    *deposition_map,
+                                   const hm_thermal_options *opts);
+
+/* Device-pointer form of the three above, ordered on `stream`; talus NULL
+ * selects talus_value; deposition_map and mask are nullable. */
+int hm_thermal_auto_bedrock_device(hm_context               *ctx,
+                                   float                    *z,
+                                   int                       nx,
+                                   int                       ny,
+                                   const float              *talus,
+                                   float                     talus_value,
+                                   int                       iterations,
+                                   float                    *deposition_map,
+                                   const float              *mask,
+                                   const hm_thermal_options *opts,
+                                   void                     *stream);
+
 /* No counterpart in the reference (which allocates its OpenCL buffers on
  * every call).  Thermal erosion on device buffers for callers that cannot
  * allocate device memory when they run it (an application whose own pool
@@ -239,13 +299,16 @@ int hm_vpipes_set_launch(int tpb, int radius, int rows);
 
 /* Step kernels of the vpipes solver, process-wide: HM_VPIPES_TILED (flow,
  * water and erosion in one kernel over 32 x 16 tiles, then an advection
- * gather), HM_VPIPES_STREAMING (all four passes in one kernel streaming
- * down column strips, shaped by hm_vpipes_set_launch), or
- * HM_VPIPES_AUTO (-1: the tuned or built-in choice).  Results do not
- * depend on it. */
+ * gather; the tiles are fetched by TMA when nx is a multiple of 4, nx >= 40,
+ * ny >= 20 and the state buffers are 16-byte aligned, else by cp.async),
+ * HM_VPIPES_TILED_CP_ASYNC (the same, always cp.async),
+ * HM_VPIPES_STREAMING (all four passes in one kernel streaming down column
+ * strips, shaped by hm_vpipes_set_launch), or HM_VPIPES_AUTO (-1: the
+ * tuned or built-in choice).  Results do not depend on it. */
 #define HM_VPIPES_AUTO (-1)
 #define HM_VPIPES_TILED 0
 #define HM_VPIPES_STREAMING 1
+#define HM_VPIPES_TILED_CP_ASYNC 2
 int hm_vpipes_set_algorithm(int algo);
 
 /* Output rows per CTA of the temporally blocked thermal kernel,

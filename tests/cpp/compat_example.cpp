@@ -6,7 +6,8 @@
  * requested solver, writes the results as raw float32 for the test to
  * compare with the oracle.
  *
- * usage: compat_example <thermal|thermal_scalar|thermal_mask|vpipes> nx ny in.f32 out_prefix
+ * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes>
+ *        nx ny in.f32 out_prefix
  */
 #include <cstdio>
 #include <cstdlib>
@@ -61,6 +62,20 @@ int main(int argc, char **argv)
   {
     hmap::gpu::thermal(z, 0.1f / shape.x, 60);
     write_raw(out + "_z.f32", z);
+  }
+  else if (mode == "auto_bedrock" || mode == "auto_bedrock_mask")
+  {
+    hmap::Array depo;
+    if (mode == "auto_bedrock")
+      hmap::gpu::thermal_auto_bedrock(z, 0.5f / shape.x, 40, &depo);
+    else
+    {
+      hmap::Array talus(shape, 0.5f / shape.x);
+      hmap::Array mask(shape, 0.75f);
+      hmap::gpu::thermal_auto_bedrock(z, &mask, talus, 40, &depo);
+    }
+    write_raw(out + "_z.f32", z);
+    write_raw(out + "_depo.f32", depo);
   }
   else if (mode == "vpipes")
   {

@@ -61,6 +61,25 @@ def test_thermal_scalar(gpu, example, tmp_path):
     assert np.array_equal(load("z"), want)
 
 
+def test_auto_bedrock(gpu, example, tmp_path):
+    z = fbm(120, 90, seed=5)
+    load = _run(example, "auto_bedrock", z, tmp_path)
+    want, depo = po.thermal_auto_bedrock(z, np.full_like(z, np.float32(0.5) / np.float32(120)), 40,
+                                         deposition=True)
+    assert np.array_equal(load("z"), want)
+    assert np.array_equal(load("depo"), depo)
+
+
+def test_auto_bedrock_mask(gpu, example, tmp_path):
+    z = fbm(88, 64, seed=6)
+    load = _run(example, "auto_bedrock_mask", z, tmp_path)
+    zf, depo = po.thermal_auto_bedrock(z, np.full_like(z, np.float32(0.5) / np.float32(88)), 40, deposition=True)
+    m = np.full_like(z, 0.75)
+    want = (z * (np.float32(1) - m)).astype(np.float32) + (zf * m).astype(np.float32)
+    assert np.array_equal(load("z"), want)
+    assert np.array_equal(load("depo"), depo)
+
+
 def test_vpipes(gpu, example, tmp_path):
     z = fbm(96, 64, seed=2)
     load = _run(example, "vpipes", z, tmp_path)
