@@ -79,9 +79,9 @@ __global__ void __launch_bounds__(STEP_BX *STEP_BY)
 /* one step per launch, column sweep                                  */
 /* ------------------------------------------------------------------ */
 
-constexpr int SW_NT = 128; /* 4 warps; a warp owns 32 columns              */
+constexpr int SW_NT = 256; /* 8 warps; a warp owns 32 columns              */
 constexpr int SW_P = 8;    /* rows whose loads are issued together          */
-constexpr int SW_H = 64;   /* output rows per CTA (a multiple of SW_P)      */
+constexpr int SW_H = 16;   /* output rows per CTA (a multiple of SW_P)      */
 
 /* One Jacobi step.  A warp walks down SW_H rows of its 32 columns; every
  * row of z is loaded once per warp (lanes 0 and 31 also load the column

@@ -179,7 +179,8 @@ __device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int n
 }
 
 /* One tile of the step on staged fields: depth at the start of the step,
- * flow on the tile plus a 1-cell ring, then water and erosion on the tile. */
+ * flow on the tile plus a 1-cell ring into shared memory, then water and
+ * erosion on the tile, which also store the tile's new fluxes. */
 template <bool MAINTAIN, bool TMA>
 __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials,
                                             int bx, int by, int nbx, int nby, FweSmem<TMA> &sm)
@@ -231,15 +232,6 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
     sm.fn[1][ly][lx] = fr;
     sm.fn[2][ly][lx] = ft;
     sm.fn[3][ly][lx] = fb;
-    const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-    if (lx >= 1 && lx <= FT_TX && ly >= 1 && ly <= FT_TY && gx < nx && gy < ny)
-    {
-      const size_t k = (size_t)gy * nx + gx;
-      io.out.fl[k] = fl;
-      io.out.fr[k] = fr;
-      io.out.ft[k] = ft;
-      io.out.fb[k] = fb;
-    }
   }
   __syncthreads();
 
@@ -264,12 +256,13 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
     const int qy = ty + 2, qx = lane + 2 + C2; /* region-2 row and smem column */
     float     d2, u, v;
     const float d1c = sm.d[qy][qx];
+    const float flc = sm.fn[0][ly][lxc], frc = sm.fn[1][ly][lxc], ftc = sm.fn[2][ly][lxc], fbc = sm.fn[3][ly][lxc];
     if (io.pl_one)
-      water_cell<true>(c, d1c, sm.fn[0][ly][lxc], sm.fn[1][ly][lxc], sm.fn[2][ly][lxc], sm.fn[3][ly][lxc],
-                       sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc], sm.fn[3][lys][lxc], d2, u, v);
+      water_cell<true>(c, d1c, flc, frc, ftc, fbc, sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc],
+                       sm.fn[3][lys][lxc], d2, u, v);
     else
-      water_cell<false>(c, d1c, sm.fn[0][ly][lxc], sm.fn[1][ly][lxc], sm.fn[2][ly][lxc], sm.fn[3][ly][lxc],
-                        sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc], sm.fn[3][lys][lxc], d2, u, v);
+      water_cell<false>(c, d1c, flc, frc, ftc, fbc, sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc],
+                        sm.fn[3][lys][lxc], d2, u, v);
     float zo, so;
     if (io.kexp_one)
       erosion_cell<true>(c, sm.z[qy][qx], sm.s[ly][sc1], sm.z[qy][qx - 1], sm.z[qy][qx + 1], sm.z[qy - 1][qx],
@@ -281,6 +274,11 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
                           sm.s[ly + 1][sc1], d2, u, v, zo, so);
     const size_t k = (size_t)gy * nx + gx;
     const float  de = fmul(d2, c.keep);
+    /* the cell's new fluxes, stored here where a warp writes whole rows */
+    io.out.fl[k] = flc;
+    io.out.fr[k] = frc;
+    io.out.ft[k] = ftc;
+    io.out.fb[k] = fbc;
     io.out.z[k] = zo;
     io.out.d[k] = de;
     io.s1[k] = so;
