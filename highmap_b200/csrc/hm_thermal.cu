@@ -173,6 +173,99 @@ __global__ void __launch_bounds__(SW_NT)
   }
 }
 
+/* The same sweep with two adjacent columns per lane (a warp owns 64
+ * columns): z, talus and bedrock move as 8-byte pairs, and one pair of
+ * shuffles per row serves both cells, which halves the per-cell load,
+ * shuffle and address work.  Needs an even nx and 8-byte aligned grids;
+ * identical bits to k_thermal_sweep. */
+constexpr int S2_NT = 128; /* 4 warps; a warp owns 64 columns */
+constexpr int S2_P = 4;    /* rows whose loads are issued together */
+
+template <bool TMAP, int BED>
+__global__ void __launch_bounds__(S2_NT)
+    k_thermal_sweep2(const float *__restrict__ a,
+                     float *__restrict__ b,
+                     int nx,
+                     int ny,
+                     const float *__restrict__ talus,
+                     float talus_value,
+                     const float *__restrict__ bedrock,
+                     int first)
+{
+  const int lane = threadIdx.x & 31;
+  const int wx = (blockIdx.x * (S2_NT / 32) + (threadIdx.x >> 5)) * 64;
+  if (wx >= nx) return; /* the whole warp: no CTA barrier in this kernel */
+  const int  gx = wx + 2 * lane; /* first of the lane's two columns (nx is even) */
+  const bool live = gx < nx;
+  const int  gxc = live ? gx : nx - 2;
+  /* lanes 0 and 31 also load the column west / east of the warp */
+  const int  hx = lane == 0 ? max(wx - 1, 0) : (lane == 31 ? min(wx + 64, nx - 1) : gxc);
+  const int  y0 = blockIdx.y * SW_H;
+  const int  y1 = min(ny, y0 + SW_H);
+
+  /* per row: the pair (x, y), the west neighbour of x and the east one of y */
+  float vx[S2_P + 2], vy[S2_P + 2], vw[S2_P + 2], ve[S2_P + 2];
+  auto load = [&](int r, int q) {
+    const float *row = a + (size_t)r * nx;
+    const float2 t = __ldg(reinterpret_cast<const float2 *>(row + gxc));
+    vx[q] = t.x;
+    vy[q] = t.y;
+    vw[q] = __ldg(row + hx); /* the halo value until the shuffles */
+  };
+  auto exchange = [&](int q) {
+    const float up = __shfl_up_sync(0xffffffffu, vy[q], 1), dn = __shfl_down_sync(0xffffffffu, vx[q], 1);
+    ve[q] = lane == 31 ? vw[q] : dn;
+    vw[q] = lane == 0 ? vw[q] : up;
+  };
+  load(max(y0 - 1, 0), 0);
+  load(y0, 1);
+  exchange(0);
+  exchange(1);
+  for (int j0 = y0; j0 < y1; j0 += S2_P)
+  {
+    float2 tl[S2_P], bd[S2_P];
+#pragma unroll
+    for (int q = 0; q < S2_P; q++)
+    {
+      load(min(j0 + 1 + q, ny - 1), q + 2);
+      const size_t o = (size_t)min(j0 + q, ny - 1) * nx + gxc;
+      tl[q] = TMAP ? __ldg(reinterpret_cast<const float2 *>(talus + o)) : make_float2(talus_value, talus_value);
+      bd[q] = BED != BED_NONE ? __ldg(reinterpret_cast<const float2 *>(bedrock + o)) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 2; q < S2_P + 2; q++) exchange(q);
+#pragma unroll
+    for (int q = 0; q < S2_P; q++)
+    {
+      const int j = j0 + q;
+      if (!live || j >= y1) continue;
+      float2 out;
+      /* apply_boundaries, _common_index.cl:106-132, for each of the two cells */
+      if (gx == 0) out.x = vy[q + 1];
+      else if (j == 0) out.x = vx[q + 2];
+      else if (j == ny - 1) out.x = vx[q];
+      else
+        out.x = thermal_cell<BED>(vx[q + 1], vw[q + 1], vx[q + 2], vx[q], vy[q + 1], vw[q], vw[q + 2], vy[q],
+                                  vy[q + 2], tl[q].x, bd[q].x, first != 0);
+      if (gx + 1 == nx - 1) out.y = vx[q + 1];
+      else if (j == 0) out.y = vy[q + 2];
+      else if (j == ny - 1) out.y = vy[q];
+      else
+        out.y = thermal_cell<BED>(vy[q + 1], vx[q + 1], vy[q + 2], vy[q], ve[q + 1], vx[q], vx[q + 2], ve[q],
+                                  ve[q + 2], tl[q].y, bd[q].y, first != 0);
+      *reinterpret_cast<float2 *>(b + (size_t)j * nx + gx) = out;
+    }
+    vx[0] = vx[S2_P];
+    vy[0] = vy[S2_P];
+    vw[0] = vw[S2_P];
+    ve[0] = ve[S2_P];
+    vx[1] = vx[S2_P + 1];
+    vy[1] = vy[S2_P + 1];
+    vw[1] = vw[S2_P + 1];
+    ve[1] = ve[S2_P + 1];
+  }
+}
+
 /* ------------------------------------------------------------------ */
 /* several steps per launch (temporal blocking)                       */
 /* ------------------------------------------------------------------ */
@@ -351,8 +444,9 @@ static int kernel_bed_mode(const float *bed, int bed_mode, bool auto_bed)
   return bed ? (bed_mode == HM_BEDROCK_LITERAL ? BED_LITERAL : BED_INTENDED) : BED_NONE;
 }
 
-/* one-step kernel: 0 = column sweep (k_thermal_sweep), 1 = one cell per
- * thread (k_thermal_step) */
+/* one-step kernel: 0 = column sweep (k_thermal_sweep2 with column pairs
+ * where the grid allows 8-byte access, else k_thermal_sweep), 1 = one cell
+ * per thread (k_thermal_step) */
 static int g_step_kernel = 0;
 
 template <bool TMAP, int BED>
@@ -361,6 +455,13 @@ static void launch_step(const float *a, float *b, int nx, int ny, const float *t
 {
   if (g_step_kernel == 0)
   {
+    auto al8 = [](const void *p) { return ((uintptr_t)p & 7u) == 0; };
+    if (nx % 2 == 0 && al8(a) && al8(b) && (!TMAP || al8(talus)) && (BED == BED_NONE || al8(bed)))
+    {
+      dim3 grid((nx + 2 * S2_NT - 1) / (2 * S2_NT), (ny + SW_H - 1) / SW_H);
+      k_thermal_sweep2<TMAP, BED><<<grid, S2_NT, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
+      return;
+    }
     dim3 grid((nx + SW_NT - 1) / SW_NT, (ny + SW_H - 1) / SW_H);
     k_thermal_sweep<TMAP, BED><<<grid, SW_NT, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
     return;

@@ -110,6 +110,30 @@ def test_device_api_matches_host_api(gpu):
     assert np.array_equal(dz.cpu().numpy(), h)
 
 
+@pytest.mark.parametrize("offset", [0, 1])
+@pytest.mark.parametrize("nx", [512, 390, 391])
+def test_device_buffer_alignment(gpu, offset, nx):
+    """Even rows on 8-byte aligned grids go through the column-pair sweep,
+    odd rows or grids one float off alignment through the one-column
+    sweep; every case gives the oracle's bits."""
+    import torch
+    ny = 70
+    z0 = fbm(nx, ny, seed=7)
+    talus = ((0.5 + fbm(nx, ny, seed=8)) / nx).astype(np.float32)
+    bed = (0.3 * z0).astype(np.float32)
+    want, _ = po.thermal(z0, talus, 21, bedrock=bed)
+
+    def dev(x):
+        buf = torch.zeros(x.size + 1, device="cuda")
+        t = buf[offset:offset + x.size].view(x.shape)
+        t.copy_(torch.from_numpy(x))
+        return t
+    dz, dt, db = dev(z0), dev(talus), dev(bed)
+    gpu.thermal_device(dz, dt, 21, bedrock=db, time_block=1)
+    torch.cuda.synchronize()
+    assert np.array_equal(dz.cpu().numpy(), want)
+
+
 def test_bad_arguments_raise(gpu):
     z = np.zeros((2, 8), np.float32)
     with pytest.raises(gpu.HMError):
