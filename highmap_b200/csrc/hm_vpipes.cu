@@ -363,20 +363,10 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
     if (io.u_out && !io.v_out) io.v_out = v_buf;
     if (io.v_out && !io.u_out) io.u_out = u_buf;
     io.parity = parity;
-    if (tma)
-    {
-      const FweMaps &m = maps[cur == &A ? 0 : 1];
-      if (io.maintain) k_vp_fwe_tma<true><<<g1, FT_NT, 0, s>>>(io, m, c, sc, partials);
-      else k_vp_fwe_tma<false><<<g1, FT_NT, 0, s>>>(io, m, c, sc, partials);
-      HM_LAUNCH_CHECK("k_vp_fwe_tma");
-    }
-    else
-    {
-      if (io.maintain) k_vp_fwe<true><<<g1, FT_NT, 0, s>>>(io, c, sc, partials);
-      else k_vp_fwe<false><<<g1, FT_NT, 0, s>>>(io, c, sc, partials);
-      HM_LAUNCH_CHECK("k_vp_fwe");
-    }
-    k_vp_advect<<<g2, 256, 0, s>>>(s1, u_buf, v_buf, nxt->s, c);
+    const int rc = tma ? launch_fwe_tma(io, maps[cur == &A ? 0 : 1], c, sc, partials, g1, s)
+                       : launch_fwe_cp_async(io, c, sc, partials, g1, s);
+    if (rc) return rc;
+    k_vp_advect<ADV_R><<<g2, 256, 0, s>>>(s1, u_buf, v_buf, nxt->s, c);
     HM_LAUNCH_CHECK("k_vp_advect");
     VpFields *t = cur;
     cur = nxt;

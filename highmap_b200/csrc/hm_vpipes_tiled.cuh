@@ -37,6 +37,16 @@ constexpr int FT_NT = 256;                     /* threads per CTA             */
 constexpr int FT_W2 = FT_TX + 4, FT_H2 = FT_TY + 4; /* z, depth region (halo 2) */
 constexpr int FT_W1 = FT_TX + 2, FT_H1 = FT_TY + 2; /* s, fluxes region (halo 1) */
 
+/* Step options as kernel template flags.  FWE_GENERIC kernels read every
+ * option from FweIo / VpConst at run time; the others have pipe length 1
+ * and discharge exponent 1 built in and the three bits below fixed, so
+ * the branches on options vanish from the cell loops (about 6 % of the
+ * step at 4096^2).  Both forms compute the same bits. */
+constexpr int FWE_DIFF = 1;      /* flux diffusion                     */
+constexpr int FWE_RAINMAP = 2;   /* a rain map scales rain and top-up   */
+constexpr int FWE_RAINSTEP = 4;  /* rain added every step               */
+constexpr int FWE_GENERIC = 8;   /* options read at run time            */
+
 /* Shared-memory layout of the staged fields.
  *   cp.async staging (TMA = false): region 2 (columns x0-2 .. x0+33, rows
  *     y0-2 .. y0+17) as [20][36]; region 1 (x0-1 .. x0+32, y0-1 .. y0+16) as
@@ -181,26 +191,31 @@ __device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int n
 /* One tile of the step on staged fields: depth at the start of the step,
  * flow on the tile plus a 1-cell ring into shared memory, then water and
  * erosion on the tile, which also store the tile's new fluxes. */
-template <bool MAINTAIN, bool TMA>
+template <bool MAINTAIN, bool TMA, int F>
 __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials,
                                             int bx, int by, int nbx, int nby, FweSmem<TMA> &sm)
 {
   static_assert(FT_TX == 32, "a lane is a column of the tile");
   using L = FweLayout<TMA>;
-  constexpr int C1 = L::C1, C2 = L::C2;
-  const int     tid = threadIdx.x;
-  const int     nx = c.nx, ny = c.ny;
-  const int     x0 = bx * FT_TX, y0 = by * FT_TY;
-  const float   add = MAINTAIN ? sc->add[io.parity] : 0.f;
-  const float   rvol = MAINTAIN ? sc->rvol : 1.f;
-  const bool    rain_step = c.rps != 0.f;
+  constexpr int  C1 = L::C1, C2 = L::C2;
+  constexpr bool GEN = (F & FWE_GENERIC) != 0;
+  const int      tid = threadIdx.x;
+  const int      nx = c.nx, ny = c.ny;
+  const int      x0 = bx * FT_TX, y0 = by * FT_TY;
+  const float    add = MAINTAIN ? sc->add[io.parity] : 0.f;
+  const float    rvol = MAINTAIN ? sc->rvol : 1.f;
+  const bool     rain_step = GEN ? c.rps != 0.f : (F & FWE_RAINSTEP) != 0;
+  const bool     rain_map = GEN ? io.rain != nullptr : (F & FWE_RAINMAP) != 0;
+  const bool     diffusion = GEN ? io.diffusion != 0 : (F & FWE_DIFF) != 0;
+  const bool     pl_one = GEN ? io.pl_one != 0 : true;
+  const bool     kexp_one = GEN ? io.kexp_one != 0 : true;
 
   /* stored depth -> depth at the start of the step (own elements) */
   for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
   {
     const int   ly = e / FT_W2, lx = e - ly * FT_W2;
     float      &d = sm.d[ly][lx + C2];
-    const float rn = io.rain ? __ldg(io.rain + (size_t)clampi(y0 - 2 + ly, 0, ny - 1) * nx +
+    const float rn = rain_map ? __ldg(io.rain + (size_t)clampi(y0 - 2 + ly, 0, ny - 1) * nx +
                                     clampi(x0 - 2 + lx, 0, nx - 1))
                              : 1.f;
     d = rain_step ? depth_d1<MAINTAIN, true>(d, rn, add, rvol, c.rps)
@@ -218,14 +233,14 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
     const float zc = sm.z[qy][qx], dc = sm.d[qy][qx];
     const float zw = sm.z[qy][qx - 1], dw = sm.d[qy][qx - 1], ze = sm.z[qy][qx + 1], de = sm.d[qy][qx + 1];
     const float zs = sm.z[qy + 1][qx], ds = sm.d[qy + 1][qx], zn = sm.z[qy - 1][qx], dn = sm.d[qy - 1][qx];
-    if (io.diffusion)
+    if (diffusion)
     {
-      if (io.pl_one) flow_cell<true, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
+      if (pl_one) flow_cell<true, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
       else flow_cell<true, false>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
     }
     else
     {
-      if (io.pl_one) flow_cell<false, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
+      if (pl_one) flow_cell<false, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
       else flow_cell<false, false>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
     }
     sm.fn[0][ly][lx] = fl;
@@ -257,14 +272,14 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
     float     d2, u, v;
     const float d1c = sm.d[qy][qx];
     const float flc = sm.fn[0][ly][lxc], frc = sm.fn[1][ly][lxc], ftc = sm.fn[2][ly][lxc], fbc = sm.fn[3][ly][lxc];
-    if (io.pl_one)
+    if (pl_one)
       water_cell<true>(c, d1c, flc, frc, ftc, fbc, sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc],
                        sm.fn[3][lys][lxc], d2, u, v);
     else
       water_cell<false>(c, d1c, flc, frc, ftc, fbc, sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc],
                         sm.fn[3][lys][lxc], d2, u, v);
     float zo, so;
-    if (io.kexp_one)
+    if (kexp_one)
       erosion_cell<true>(c, sm.z[qy][qx], sm.s[ly][sc1], sm.z[qy][qx - 1], sm.z[qy][qx + 1], sm.z[qy - 1][qx],
                          sm.z[qy + 1][qx], sm.s[ly][sc1 - 1], sm.s[ly][sc1 + 1], sm.s[ly - 1][sc1],
                          sm.s[ly + 1][sc1], d2, u, v, zo, so);
@@ -301,20 +316,20 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
   }
 }
 
-template <bool MAINTAIN>
+template <bool MAINTAIN, int F>
 __global__ void __launch_bounds__(FT_NT) k_vp_fwe(FweIo io, VpConst c, VpScalars *sc, double *partials)
 {
   __shared__ FweSmem<false> sm;
   fwe_stage_cp_async(io, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm);
   __syncthreads();
-  fwe_compute<MAINTAIN, false>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  fwe_compute<MAINTAIN, false, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
 /* The same step with the input tiles fetched by TMA.  A tile whose loads
  * time out sets bit 0 of sc->error and writes nothing; with the volume
  * top-up it still takes part in the grid-wide sum (adding zero) so the
  * last block's finish is not left waiting for it. */
-template <bool MAINTAIN>
+template <bool MAINTAIN, int F>
 __global__ void __launch_bounds__(FT_NT)
     k_vp_fwe_tma(FweIo io, const __grid_constant__ FweMaps maps, VpConst c, VpScalars *sc, double *partials)
 {
@@ -332,7 +347,7 @@ __global__ void __launch_bounds__(FT_NT)
     }
     return;
   }
-  fwe_compute<MAINTAIN, true>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  fwe_compute<MAINTAIN, true, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
 /* advection of one cell: s_new = bilinear(s1, (i - dt u, j - dt v)) */
@@ -346,6 +361,44 @@ __device__ __forceinline__ float advect_cell(const float *__restrict__ s1, int i
   return blend(t, __ldg(s1 + r0 + t.i0), __ldg(s1 + r0 + t.i1), __ldg(s1 + r1 + t.i0), __ldg(s1 + r1 + t.i1));
 }
 
+/* Launch one k_vp_fwe (tma false) or k_vp_fwe_tma (maps != NULL) step on
+ * stream s with the kernel specialised for the step's options
+ * (hm_vpipes_fwe_cp_async.cu, hm_vpipes_fwe_tma.cu). */
+int launch_fwe_cp_async(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials, dim3 grid,
+                        cudaStream_t s);
+int launch_fwe_tma(const FweIo &io, const FweMaps &maps, const VpConst &c, VpScalars *sc, double *partials,
+                   dim3 grid, cudaStream_t s);
+
+/* template flags of a step's options */
+inline int fwe_flags(const FweIo &io, const VpConst &c)
+{
+  if (!io.pl_one || !io.kexp_one) return FWE_GENERIC;
+  return (io.diffusion ? FWE_DIFF : 0) | (io.rain ? FWE_RAINMAP : 0) | (c.rps != 0.f ? FWE_RAINSTEP : 0);
+}
+
+/* Launch the kernel K<MAINTAIN, F> for run-time (maintain, f), f one of
+ * the eight fixed-option words or FWE_GENERIC; `launch` receives the
+ * kernel's address. */
+template <template <bool, int> class K, class Launch>
+int fwe_dispatch(bool maintain, int f, Launch launch)
+{
+#define HM_FWE_CASE(FF)                                                                                                \
+  case FF: return maintain ? launch(K<true, FF>::fn()) : launch(K<false, FF>::fn());
+  switch (f)
+  {
+    HM_FWE_CASE(0)
+    HM_FWE_CASE(1)
+    HM_FWE_CASE(2)
+    HM_FWE_CASE(3)
+    HM_FWE_CASE(4)
+    HM_FWE_CASE(5)
+    HM_FWE_CASE(6)
+    HM_FWE_CASE(7)
+  default: return maintain ? launch(K<true, FWE_GENERIC>::fn()) : launch(K<false, FWE_GENERIC>::fn());
+  }
+#undef HM_FWE_CASE
+}
+
 /* Advection over the grid: block x covers 256 columns, and each thread
  * takes ADV_R consecutive rows of its column at a time, so that the
  * velocity loads of all ADV_R rows, then all their 4 ADV_R gathers, are in
@@ -353,6 +406,7 @@ __device__ __forceinline__ float advect_cell(const float *__restrict__ s1, int i
  * rounds of loads). */
 constexpr int ADV_R = 4;
 
+template <int R>
 __global__ void __launch_bounds__(256) k_vp_advect(const float *__restrict__ s1,
                                                     const float *__restrict__ u,
                                                     const float *__restrict__ v,
@@ -361,20 +415,20 @@ __global__ void __launch_bounds__(256) k_vp_advect(const float *__restrict__ s1,
 {
   const int i = blockIdx.x * 256 + threadIdx.x;
   if (i >= c.nx) return;
-  for (int jb = blockIdx.y * ADV_R; jb < c.ny; jb += gridDim.y * ADV_R)
+  for (int jb = blockIdx.y * R; jb < c.ny; jb += gridDim.y * R)
   {
-    float uu[ADV_R], vv[ADV_R];
+    float uu[R], vv[R];
 #pragma unroll
-    for (int q = 0; q < ADV_R; q++)
+    for (int q = 0; q < R; q++)
     {
       const size_t k = (size_t)min(jb + q, c.ny - 1) * c.nx + i;
       uu[q] = __ldg(u + k);
       vv[q] = __ldg(v + k);
     }
-    Tap   t[ADV_R];
-    float g[ADV_R][4];
+    Tap   t[R];
+    float g[R][4];
 #pragma unroll
-    for (int q = 0; q < ADV_R; q++)
+    for (int q = 0; q < R; q++)
     {
       const int    j = min(jb + q, c.ny - 1);
       const float  x = fsub((float)i, fmul(c.dt, uu[q]));
@@ -387,7 +441,7 @@ __global__ void __launch_bounds__(256) k_vp_advect(const float *__restrict__ s1,
       g[q][3] = __ldg(s1 + r1 + t[q].i1);
     }
 #pragma unroll
-    for (int q = 0; q < ADV_R; q++)
+    for (int q = 0; q < R; q++)
       if (jb + q < c.ny) s_out[(size_t)(jb + q) * c.nx + i] = blend(t[q], g[q][0], g[q][1], g[q][2], g[q][3]);
   }
 }
