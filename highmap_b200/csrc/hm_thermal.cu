@@ -13,9 +13,11 @@
  * lerp(z0, z, mask) (HighMap/include/highmap/operator.hpp:405-418).
  *
  * Kernels
- *   k_thermal_step    one step per launch, one cell per thread; HBM bound:
- *                     reads z (9-point, reuse through L1/L2), talus and
- *                     bedrock, writes z: 12 B/cell (16 B with bedrock).
+ *   k_thermal_sweep2  one step per launch: a warp walks down rows of 64
+ *                     columns (two per lane), neighbours by warp shuffles;
+ *                     reads z, talus and bedrock once, writes z: 12 B/cell
+ *                     (16 B with bedrock).  Even nx, 8-byte aligned grids.
+ *   k_thermal_sweep   the same with one column per lane (any grid).
  *   k_thermal_tb      up to 8 steps per launch (temporal blocking): a
  *                     strip of columns streams down the grid; each time
  *                     level keeps a 4-row ring in shared memory, so HBM
@@ -36,44 +38,7 @@
 namespace hm
 {
 
-/* ------------------------------------------------------------------ */
-/* one step per launch                                                */
-/* ------------------------------------------------------------------ */
-
 __device__ __forceinline__ int clamp_col(int g, int n) { return g < 0 ? 0 : (g > n - 1 ? n - 1 : g); }
-
-constexpr int STEP_BX = 64;
-constexpr int STEP_BY = 4;
-
-template <bool TMAP, int BED>
-__global__ void __launch_bounds__(STEP_BX *STEP_BY)
-    k_thermal_step(const float *__restrict__ a,
-                   float *__restrict__ b,
-                   int nx,
-                   int ny,
-                   const float *__restrict__ talus,
-                   float talus_value,
-                   const float *__restrict__ bedrock,
-                   int first)
-{
-  const int i = blockIdx.x * STEP_BX + threadIdx.x;
-  const int j = blockIdx.y * STEP_BY + threadIdx.y;
-  if (i >= nx || j >= ny) return;
-  const size_t idx = (size_t)j * nx + i;
-  /* apply_boundaries, _common_index.cl:106-132 */
-  if (i == 0) { b[idx] = __ldg(a + idx + 1); return; }
-  if (i == nx - 1) { b[idx] = __ldg(a + idx - 1); return; }
-  if (j == 0) { b[idx] = __ldg(a + idx + nx); return; }
-  if (j == ny - 1) { b[idx] = __ldg(a + idx - nx); return; }
-
-  const float *up = a + idx - nx;
-  const float *mid = a + idx;
-  const float *dn = a + idx + nx;
-  const float  t = TMAP ? __ldg(talus + idx) : talus_value;
-  const float  zb = BED != BED_NONE ? __ldg(bedrock + idx) : 0.f;
-  b[idx] = thermal_cell<BED>(__ldg(mid), __ldg(mid - 1), __ldg(dn), __ldg(up), __ldg(mid + 1),
-                             __ldg(up - 1), __ldg(dn - 1), __ldg(up + 1), __ldg(dn + 1), t, zb, first != 0);
-}
 
 /* ------------------------------------------------------------------ */
 /* one step per launch, column sweep                                  */
@@ -89,8 +54,8 @@ constexpr int SW_H = 16;   /* output rows per CTA (a multiple of SW_P)      */
  * shuffles, so a cell costs two coalesced loads per 32 cells instead of
  * nine loads.  The loads of SW_P rows (z, talus, bedrock) are issued
  * before any of them is used, which keeps enough bytes in flight to cover
- * the HBM latency.  Cell rule and border copies as k_thermal_step, so the
- * two kernels give identical bits. */
+ * the HBM latency.  Cell rule and border copies as the reference kernel
+ * (thermal.cl:26-100 in Jacobi form). */
 template <bool TMAP, int BED>
 __global__ void __launch_bounds__(SW_NT)
     k_thermal_sweep(const float *__restrict__ a,
@@ -294,7 +259,7 @@ __device__ __forceinline__ void tb_cp_async4(float *smem, const float *gmem)
  *
  * Each cell follows the rule of the one-step kernel (border copy, then
  * the talus exchange with bedrock), so T steps here are bit-identical to
- * T launches of k_thermal_step. */
+ * T one-step launches. */
 template <bool TMAP, int BED>
 __global__ void __launch_bounds__(TB_TPB)
     k_thermal_tb(const float *__restrict__ a,
@@ -444,31 +409,21 @@ static int kernel_bed_mode(const float *bed, int bed_mode, bool auto_bed)
   return bed ? (bed_mode == HM_BEDROCK_LITERAL ? BED_LITERAL : BED_INTENDED) : BED_NONE;
 }
 
-/* one-step kernel: 0 = column sweep (k_thermal_sweep2 with column pairs
- * where the grid allows 8-byte access, else k_thermal_sweep), 1 = one cell
- * per thread (k_thermal_step) */
-static int g_step_kernel = 0;
-
+/* one Jacobi step: the column-pair sweep where the grid allows 8-byte
+ * access (even nx, 8-byte aligned grids), else the one-column sweep */
 template <bool TMAP, int BED>
 static void launch_step(const float *a, float *b, int nx, int ny, const float *talus, float tv,
                         const float *bed, int first, cudaStream_t s)
 {
-  if (g_step_kernel == 0)
+  auto al8 = [](const void *p) { return ((uintptr_t)p & 7u) == 0; };
+  if (nx % 2 == 0 && al8(a) && al8(b) && (!TMAP || al8(talus)) && (BED == BED_NONE || al8(bed)))
   {
-    auto al8 = [](const void *p) { return ((uintptr_t)p & 7u) == 0; };
-    if (nx % 2 == 0 && al8(a) && al8(b) && (!TMAP || al8(talus)) && (BED == BED_NONE || al8(bed)))
-    {
-      dim3 grid((nx + 2 * S2_NT - 1) / (2 * S2_NT), (ny + SW_H - 1) / SW_H);
-      k_thermal_sweep2<TMAP, BED><<<grid, S2_NT, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
-      return;
-    }
-    dim3 grid((nx + SW_NT - 1) / SW_NT, (ny + SW_H - 1) / SW_H);
-    k_thermal_sweep<TMAP, BED><<<grid, SW_NT, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
+    dim3 grid((nx + 2 * S2_NT - 1) / (2 * S2_NT), (ny + SW_H - 1) / SW_H);
+    k_thermal_sweep2<TMAP, BED><<<grid, S2_NT, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
     return;
   }
-  dim3 block(STEP_BX, STEP_BY);
-  dim3 grid((nx + STEP_BX - 1) / STEP_BX, (ny + STEP_BY - 1) / STEP_BY);
-  k_thermal_step<TMAP, BED><<<grid, block, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
+  dim3 grid((nx + SW_NT - 1) / SW_NT, (ny + SW_H - 1) / SW_H);
+  k_thermal_sweep<TMAP, BED><<<grid, SW_NT, 0, s>>>(a, b, nx, ny, talus, tv, bed, first);
 }
 
 template <bool TMAP>
@@ -618,7 +573,7 @@ int thermal_core(int device,
     if (tb == 1)
     {
       step_dispatch(src, dst, nx, ny, talus, talus_value, bed, mode, done == 0, s);
-      HM_LAUNCH_CHECK("k_thermal_step");
+      HM_LAUNCH_CHECK("k_thermal_sweep");
     }
     else
     {
