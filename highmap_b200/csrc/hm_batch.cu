@@ -6,16 +6,19 @@
  * hmap::gpu::hydraulic_vpipes); a node-graph editor evaluating many
  * erosion nodes calls them one after another.  Small grids cannot fill a
  * B200 on their own, so here every admitted job's grid is cut into tiles
- * and the tiles of all jobs form one packed list:
- *   vpipes tiles  : strips of 120 output columns x 64 rows (the fused step
- *                   of hm_vpipes_fused.cuh, one tile per CTA pass);
- *   thermal tiles : strips of 128 columns x 32 rows (one Jacobi step).
+ * and the tiles of all jobs form packed lists:
+ *   vpipes tiles  : 32 x 16 tiles of the flow / water / erosion step
+ *                   (fwe_compute of hm_vpipes_tiled.cuh, cp.async staging),
+ *                   then advection tiles of 256 columns x 16 rows;
+ *   thermal tiles : 16 rows of 512 columns, a warp per 64 (column pairs,
+ *                   for even rows on aligned grids) or of 256 columns, a
+ *                   warp per 32 (hm_thermal_sweep.cuh).
  * A round advances every active job by one step: one persistent launch
- * whose CTAs (as many as fit on the device) take tiles from an atomic
- * counter, vpipes tiles first, then a fix-up launch for deferred advection
- * samples.  Jobs are listed by remaining steps, longest first, so the
- * active tiles of every round are a prefix of each list.  A job's step s
- * reads state copy s & 1 and writes the other; per-job volume sums use the
+ * whose CTAs (as many as fit on the device) take vpipes and thermal tiles
+ * from an atomic counter, then one persistent launch over the advection
+ * tiles.  Jobs are listed by remaining steps, longest first, so the active
+ * tiles of every round are a prefix of each list.  A job's step s reads
+ * state copy s & 1 and writes the other; per-job volume sums use the
  * deterministic last-tile finish of hm_reduce.cuh.  hm_batch_run captures
  * all rounds of a batch into one CUDA graph.
  *
@@ -25,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -34,33 +38,37 @@
 #include "hm_internal.h"
 #include "hm_thermal.h"
 #include "hm_thermal_math.cuh"
+#include "hm_thermal_sweep.cuh"
 #include "hm_vpipes.h"
-#include "hm_vpipes_fused.cuh"
+#include "hm_vpipes_tiled.cuh"
 
 namespace hm
 {
 
-constexpr int BT = 128;  /* threads per CTA                          */
-constexpr int BR = 2;    /* staged advection radius of vpipes tiles   */
-constexpr int VP_H = 64; /* output rows of a vpipes tile              */
-constexpr int TH_H = 32; /* rows of a thermal tile                    */
-constexpr int VP_W = FusedLayout<BT, BR>::W;
-constexpr int TH_W = BT;
+constexpr int BT = FT_NT;  /* threads per CTA (8 warps)                  */
+constexpr int TH_W = 256;  /* thermal tile: a warp per 32 columns        */
+constexpr int TH_H = 16;   /* rows of a thermal tile                     */
+constexpr int AD_W = 256;  /* advection tile: a thread per column        */
+constexpr int AD_H = 16;   /* rows of an advection tile                  */
 
 /* device-side description of one job */
 struct BJob
 {
   int       kind, nx, ny, iters;
   long long start; /* global round of the job's first step */
-  int       nbx, nby;
+  int       nbx, nby;   /* fwe or thermal tiles */
+  int       anx, any;   /* advection tiles (vpipes) */
   /* thermal: tz[s & 1] holds step s */
   float       *tz[2];
   const float *talus;
   float        tv;
   const float *bed;
   int          bed_mode;
-  /* vpipes: cp[s & 1] holds step s */
+  int          pairs; /* column-pair sweep (even nx, 8-byte aligned grids) */
+  /* vpipes: cp[s & 1] holds step s; s1, u, v carry a step's eroded
+   * sediment and velocity from the fwe tiles to the advection tiles */
   VpFields     cp[2];
+  float       *s1, *u, *v;
   VpConst      c;
   int          maintain, diffusion, pl_one, kexp_one;
   const float *rain;
@@ -71,95 +79,88 @@ struct BJob
 
 /* ---- kernels ------------------------------------------------------- */
 
+/* the fwe inputs of step `step` of vpipes job J */
+__device__ __forceinline__ void job_io(const BJob &J, int step, FweIo &io)
+{
+  const int       par = step & 1;
+  const VpFields &in = J.cp[par], &out = J.cp[par ^ 1];
+  io.in = VpState{in.z, in.d, in.s, in.fl, in.fr, in.ft, in.fb};
+  io.out = VpStateOut{out.z, out.d, out.s, out.fl, out.fr, out.ft, out.fb, nullptr, nullptr};
+  io.s1 = J.s1;
+  io.u = J.u;
+  io.v = J.v;
+  io.rain = J.rain;
+  io.parity = par;
+  io.maintain = J.maintain;
+  io.diffusion = J.diffusion;
+  io.pl_one = J.pl_one;
+  io.kexp_one = J.kexp_one;
+  const bool last = step == J.iters - 1;
+  io.u_out = last ? J.u_out : nullptr;
+  io.v_out = last ? J.v_out : nullptr;
+  if (io.u_out && !io.v_out) io.v_out = J.v;
+  if (io.v_out && !io.u_out) io.u_out = J.u;
+}
+
 template <bool TMAP, int BED>
 __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int by)
 {
-  const int    nx = J.nx, ny = J.ny;
-  const int    i = bx * TH_W + threadIdx.x;
-  const int    y0 = by * TH_H, y1 = min(ny, y0 + TH_H);
-  const float *__restrict__ a = J.tz[par];
-  float *__restrict__ b = J.tz[par ^ 1];
-  const float *__restrict__ talus = J.talus;
-  const float *__restrict__ bed = J.bed;
-  const float  tv = J.tv;
-  if (i >= nx) return;
-  for (int j = y0; j < y1; j++)
+  const int y0 = by * TH_H, y1 = min(J.ny, y0 + TH_H);
+  if (J.pairs)
   {
-    const size_t idx = (size_t)j * nx + i;
-    /* apply_boundaries, _common_index.cl:106-132 */
-    if (i == 0) { b[idx] = __ldg(a + idx + 1); continue; }
-    if (i == nx - 1) { b[idx] = __ldg(a + idx - 1); continue; }
-    if (j == 0) { b[idx] = __ldg(a + idx + nx); continue; }
-    if (j == ny - 1) { b[idx] = __ldg(a + idx - nx); continue; }
-    const float *up = a + idx - nx, *mid = a + idx, *dn = a + idx + nx;
-    const float  t = TMAP ? __ldg(talus + idx) : tv;
-    const float  zb = BED != BED_NONE ? __ldg(bed + idx) : 0.f;
-    b[idx] = thermal_cell<BED>(__ldg(mid), __ldg(mid - 1), __ldg(dn), __ldg(up), __ldg(mid + 1), __ldg(up - 1),
-                               __ldg(dn - 1), __ldg(up + 1), __ldg(dn + 1), t, zb);
+    const int wx = bx * 2 * TH_W + (threadIdx.x >> 5) * 64;
+    if (wx < J.nx) /* whole warp */
+      thermal_sweep2_warp<TMAP, BED>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
+    return;
   }
+  const int wx = bx * TH_W + (threadIdx.x >> 5) * 32;
+  if (wx < J.nx) /* whole warp */
+    thermal_sweep_warp<TMAP, BED>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
 }
 
-__device__ __forceinline__ VpStep job_step(const BJob &J, int par, int step, long long round)
-{
-  VpStep st;
-  const VpFields &in = J.cp[par], &out = J.cp[par ^ 1];
-  st.in = VpState{in.z, in.d, in.s, in.fl, in.fr, in.ft, in.fb};
-  const bool last = step == J.iters - 1;
-  st.out = VpStateOut{out.z, out.d, out.s, out.fl, out.fr, out.ft, out.fb, last ? J.u_out : nullptr,
-                      last ? J.v_out : nullptr};
-  st.rain = J.rain;
-  st.parity = par;
-  st.dparity = (int)(round & 1);
-  st.H = VP_H;
-  st.maintain = J.maintain;
-  st.diffusion = J.diffusion;
-  st.pl_one = J.pl_one;
-  st.kexp_one = J.kexp_one;
-  return st;
-}
-
-/* One round: every active tile of the packed lists, taken by persistent
- * CTAs from an atomic counter. */
-__global__ void __launch_bounds__(BT)
+/* One round, first launch: every active vpipes fwe tile and thermal tile,
+ * taken by persistent CTAs from an atomic counter. */
+__global__ void __launch_bounds__(BT, 3)
     k_batch_round(const BJob *__restrict__ jobs,
                   const int4 *__restrict__ vt,
                   int nv,
                   const int4 *__restrict__ tt,
                   int nt,
                   long long round,
-                  unsigned *counter,
-                  VpDefer df)
+                  unsigned *counter)
 {
-  extern __shared__ float smem[];
-  __shared__ int     s_tile;
-  /* the current vpipes tile's job descriptor, staged in shared memory once
-   * per tile (kept in a local struct, it lands on the stack and every use
-   * in the row loop becomes a local-memory load) */
-  __shared__ VpStep  s_st;
+  __shared__ FweSmem<false> sm;
+  __shared__ int            s_tile;
+  /* the current vpipes tile's step description, staged once per tile */
+  __shared__ FweIo   s_io;
   __shared__ VpConst s_c;
   for (;;)
   {
-    if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
-    __syncthreads();
-    const int t = s_tile;
-    if (t < nv && threadIdx.x == 0)
+    __syncthreads(); /* the previous tile is done with the shared state */
+    if (threadIdx.x == 0)
     {
-      const BJob &J = jobs[vt[t].x];
-      const int   step = (int)(round - J.start);
-      s_st = job_step(J, step & 1, step, round);
-      s_c = J.c;
+      const int t = (int)atomicAdd(counter, 1u);
+      s_tile = t;
+      if (t < nv)
+      {
+        const BJob &J = jobs[vt[t].x];
+        job_io(J, (int)(round - J.start), s_io);
+        s_c = J.c;
+      }
     }
     __syncthreads();
+    const int t = s_tile;
     if (t >= nv + nt) return;
     if (t < nv)
     {
       const int4  tl = vt[t];
       const BJob &J = jobs[tl.x];
-      VpScalars  *sc = J.sc;
-      double     *partials = J.partials;
-      const int   nbx = J.nbx, nby = J.nby;
-      if (s_st.maintain) vp_tile<BT, BR, true>(s_st, s_c, sc, partials, df, (unsigned)tl.x, tl.y, tl.z, nbx, nby, smem);
-      else vp_tile<BT, BR, false>(s_st, s_c, sc, partials, df, (unsigned)tl.x, tl.y, tl.z, nbx, nby, smem);
+      fwe_stage_cp_async(s_io, J.nx, J.ny, tl.y * FT_TX, tl.z * FT_TY, sm);
+      __syncthreads();
+      if (J.maintain)
+        fwe_compute<true, false, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
+      else
+        fwe_compute<false, false, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
     }
     else
     {
@@ -183,25 +184,28 @@ __global__ void __launch_bounds__(BT)
   }
 }
 
-/* Deferred advection samples of the round, any job; re-arms the other
- * round parity's counter. */
-__global__ void __launch_bounds__(128) k_batch_fixup(const BJob *__restrict__ jobs, long long round, VpDefer df)
+/* One round, second launch: the advection tiles of the active vpipes jobs
+ * (s of the new state from this step's s1, u, v). */
+__global__ void __launch_bounds__(BT, 4)
+    k_batch_advect(const BJob *__restrict__ jobs, const int4 *__restrict__ at, int na, long long round,
+                   unsigned *counter)
 {
-  const int      dpar = (int)(round & 1);
-  const unsigned n = min(df.count[dpar], df.cap);
-  if (blockIdx.x == 0 && threadIdx.x == 0) df.count[dpar ^ 1] = 0u;
-  for (unsigned e = blockIdx.x * 128 + threadIdx.x; e < n; e += gridDim.x * 128)
+  __shared__ int s_tile;
+  for (;;)
   {
-    const Deferred d = df.list[e];
-    const BJob    &J = jobs[d.job];
-    const int      step = (int)(round - J.start);
-    const int      par = step & 1;
-    const VpStep   st = job_step(J, par, step, round);
-    const float    add = J.maintain ? J.sc->add[par] : 0.f;
-    const float    rvol = J.maintain ? J.sc->rvol : 1.f;
-    const Glob     g{st, J.c, add, rvol};
-    const int      gj = (int)(d.k / (unsigned)J.nx), gi = (int)(d.k - (unsigned)gj * (unsigned)J.nx);
-    st.out.s[d.k] = advect_global(g, gi, gj, d.u, d.v);
+    __syncthreads();
+    if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= na) return;
+    const int4  tl = at[t];
+    const BJob &J = jobs[tl.x];
+    const int   par = (int)((round - J.start) & 1);
+    const int   i = tl.y * AD_W + (int)threadIdx.x;
+    if (i >= J.nx) continue;
+    const int y1 = min(J.ny, (tl.z + 1) * AD_H);
+    for (int jb = tl.z * AD_H; jb < y1; jb += ADV_R)
+      advect_rows<ADV_R>(J.s1, J.u, J.v, J.cp[par ^ 1].s, J.c, i, jb);
   }
 }
 
@@ -230,9 +234,9 @@ size_t job_bytes(const hm_job &j)
 {
   const size_t n = align_up((size_t)j.nx * j.ny, 64) * sizeof(float);
   if (j.kind == HM_JOB_THERMAL) return n * (1 + (j.deposition_map ? 1 : 0));
-  const size_t tiles = (size_t)((j.nx + hm::VP_W - 1) / hm::VP_W) * ((j.ny + hm::VP_H - 1) / hm::VP_H);
+  const size_t tiles = (size_t)((j.nx + hm::FT_TX - 1) / hm::FT_TX) * ((j.ny + hm::FT_TY - 1) / hm::FT_TY);
   const size_t parts = std::max(tiles, hm::vpipes_init_partials());
-  return n * 13 + align_up(parts * sizeof(double), 256) + align_up(sizeof(hm::VpScalars), 256);
+  return n * 16 + align_up(parts * sizeof(double), 256) + align_up(sizeof(hm::VpScalars), 256);
 }
 
 int check_job(const hm_job &j)
@@ -255,6 +259,11 @@ int check_job(const hm_job &j)
 
 } // namespace
 
+namespace
+{
+struct TileLists;
+}
+
 struct hm_batch
 {
   hm_context       *ctx = nullptr;
@@ -262,8 +271,8 @@ struct hm_batch
   cudaStream_t      stream = nullptr;
   std::vector<HJob> jobs;
   long long         round = 0;
-  int               grid_cap = 0; /* persistent CTAs */
-  size_t            smem = 0;
+  int               grid_cap = 0; /* persistent CTAs of k_batch_round  */
+  int               grid_cap_adv = 0; /* persistent CTAs of k_batch_advect */
   /* device tables */
   hm::BJob         *d_jobs = nullptr;
   size_t            d_jobs_cap = 0;
@@ -271,10 +280,10 @@ struct hm_batch
   size_t            d_tiles_cap = 0;
   unsigned         *d_counters = nullptr;
   size_t            counters_cap = 0;
-  hm::Deferred     *d_defer = nullptr;
-  unsigned         *d_defer_count = nullptr;
-  unsigned          defer_cap = 0;
-  bool              dirty = true;
+  bool              dirty = true;       /* job table needs an upload       */
+  bool              tiles_dirty = true; /* tile lists need a rebuild        */
+  TileLists        *lists = nullptr;
+  cudaMemPool_t     pool = nullptr;     /* job state; keeps freed memory    */
 };
 
 namespace
@@ -343,6 +352,7 @@ int finalize_job(hm_batch *b, HJob &h)
     }
   }
   h.finished = true;
+  b->tiles_dirty = true;
   return HM_OK;
 }
 
@@ -355,54 +365,73 @@ int finalize_job(hm_batch *b, HJob &h)
  *   commit : step counts. */
 struct Plan
 {
-  std::vector<int>  act;
-  std::vector<int>  vrem, trem;
-  size_t            nv = 0, nt = 0;
-  int               N = 0;
+  std::vector<int> act; /* active jobs, longest remaining first           */
+  std::vector<int> rem; /* their remaining steps                          */
+  int              N = 0;
+};
+
+/* Packed tile lists of the active jobs (cached in the batch, rebuilt and
+ * uploaded only when a job is admitted or finishes): vpipes fwe tiles,
+ * thermal tiles, vpipes advection tiles, each in the order of act; cum*[m]
+ * counts the tiles of the first m jobs, so the tiles of the jobs that still
+ * have steps left at a round are a prefix of each list. */
+struct TileLists
+{
+  std::vector<int>    act;
+  std::vector<size_t> vcum, tcum, acum;
 };
 
 int plan_rounds(hm_batch *b, int rounds, Plan &pl)
 {
-  for (size_t k = 0; k < b->jobs.size(); k++)
-    if (b->jobs[k].live && !b->jobs[k].finished) pl.act.push_back((int)k);
   auto remaining = [&](int k) { return b->jobs[k].desc.iterations - b->jobs[k].steps; };
-  std::stable_sort(pl.act.begin(), pl.act.end(), [&](int x, int y) { return remaining(x) > remaining(y); });
+  int  st;
+  if (b->tiles_dirty)
+  {
+    TileLists &tl = *b->lists;
+    tl.act.clear();
+    for (size_t k = 0; k < b->jobs.size(); k++)
+      if (b->jobs[k].live && !b->jobs[k].finished) tl.act.push_back((int)k);
+    /* every active job advances by the same number of steps per round, so
+     * this order holds until the set of jobs changes */
+    std::stable_sort(tl.act.begin(), tl.act.end(), [&](int x, int y) { return remaining(x) > remaining(y); });
+    std::vector<int4> vt, tt, at;
+    tl.vcum.assign(1, 0);
+    tl.tcum.assign(1, 0);
+    tl.acum.assign(1, 0);
+    for (int k : tl.act)
+    {
+      const HJob &h = b->jobs[k];
+      for (int by = 0; by < h.dev.nby; by++)
+        for (int bx = 0; bx < h.dev.nbx; bx++)
+          (h.desc.kind == HM_JOB_VPIPES ? vt : tt).push_back(make_int4(k, bx, by, 0));
+      if (h.desc.kind == HM_JOB_VPIPES)
+        for (int by = 0; by < h.dev.any; by++)
+          for (int bx = 0; bx < h.dev.anx; bx++) at.push_back(make_int4(k, bx, by, 0));
+      tl.vcum.push_back(vt.size());
+      tl.tcum.push_back(tt.size());
+      tl.acum.push_back(at.size());
+    }
+    std::vector<int4> all(vt);
+    all.insert(all.end(), tt.begin(), tt.end());
+    all.insert(all.end(), at.begin(), at.end());
+    if ((st = grow(&b->d_tiles, &b->d_tiles_cap, std::max<size_t>(all.size(), 1), b->stream))) return st;
+    /* pageable source: the call returns once the data is staged */
+    if (!all.empty())
+      HM_CUDA_TRY(
+          cudaMemcpyAsync(b->d_tiles, all.data(), all.size() * sizeof(int4), cudaMemcpyHostToDevice, b->stream));
+    b->tiles_dirty = false;
+  }
+  pl.act = b->lists->act;
   int maxrem = 0;
-  for (int k : pl.act) maxrem = std::max(maxrem, remaining(k));
-  pl.N = std::min(rounds, maxrem);
-
-  /* packed tile lists: vpipes then thermal, each longest-remaining first */
-  std::vector<int4> vt, tt;
   for (int k : pl.act)
   {
-    const HJob &h = b->jobs[k];
-    for (int by = 0; by < h.dev.nby; by++)
-      for (int bx = 0; bx < h.dev.nbx; bx++)
-      {
-        if (h.desc.kind == HM_JOB_VPIPES)
-        {
-          vt.push_back(make_int4(k, bx, by, 0));
-          pl.vrem.push_back(remaining(k));
-        }
-        else
-        {
-          tt.push_back(make_int4(k, bx, by, 0));
-          pl.trem.push_back(remaining(k));
-        }
-      }
+    pl.rem.push_back(std::max(0, remaining(k)));
+    maxrem = std::max(maxrem, pl.rem.back());
   }
-  pl.nv = vt.size();
-  pl.nt = tt.size();
-  int st;
+  pl.N = std::min(rounds, maxrem);
   if ((st = upload_jobs(b))) return st;
   if (pl.N == 0) return HM_OK;
-  if ((st = grow(&b->d_tiles, &b->d_tiles_cap, std::max<size_t>(pl.nv + pl.nt, 1), b->stream))) return st;
-  if ((st = grow(&b->d_counters, &b->counters_cap, (size_t)pl.N, b->stream))) return st;
-  std::vector<int4> all(vt);
-  all.insert(all.end(), tt.begin(), tt.end());
-  /* pageable source: the call returns once the data is staged */
-  if (!all.empty())
-    HM_CUDA_TRY(cudaMemcpyAsync(b->d_tiles, all.data(), all.size() * sizeof(int4), cudaMemcpyHostToDevice, b->stream));
+  if ((st = grow(&b->d_counters, &b->counters_cap, 2 * (size_t)pl.N, b->stream))) return st;
   return HM_OK;
 }
 
@@ -410,23 +439,26 @@ int launch_rounds(hm_batch *b, const Plan &pl)
 {
   if (pl.N > 0)
   {
-    HM_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, (size_t)pl.N * sizeof(unsigned), b->stream));
-    hm::VpDefer df{b->d_defer, b->d_defer_count, b->defer_cap};
-    size_t      iv = pl.nv, it = pl.nt;
+    HM_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, 2 * (size_t)pl.N * sizeof(unsigned), b->stream));
+    const TileLists &tl = *b->lists;
+    const size_t     nv = tl.vcum.back(), nt = tl.tcum.back();
+    size_t           m = pl.act.size();
     for (int r = 0; r < pl.N; r++)
     {
-      /* tiles whose job still has steps left at this round */
-      while (iv > 0 && pl.vrem[iv - 1] <= r) iv--;
-      while (it > 0 && pl.trem[it - 1] <= r) it--;
+      /* the jobs (a prefix of act) that still have steps left at this round */
+      while (m > 0 && pl.rem[m - 1] <= r) m--;
+      const size_t iv = tl.vcum[m], it = tl.tcum[m], ia = tl.acum[m];
       const int total = (int)(iv + it);
       const int grid = std::max(1, std::min(b->grid_cap, total));
-      hm::k_batch_round<<<grid, hm::BT, b->smem, b->stream>>>(b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + pl.nv,
-                                                              (int)it, b->round + r, b->d_counters + r, df);
+      hm::k_batch_round<<<grid, hm::BT, 0, b->stream>>>(b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it,
+                                                        b->round + r, b->d_counters + 2 * r);
       HM_LAUNCH_CHECK("k_batch_round");
-      if (iv > 0)
+      if (ia > 0)
       {
-        hm::k_batch_fixup<<<2 * 148, 128, 0, b->stream>>>(b->d_jobs, b->round + r, df);
-        HM_LAUNCH_CHECK("k_batch_fixup");
+        const int grid2 = std::max(1, std::min(b->grid_cap_adv, (int)ia));
+        hm::k_batch_advect<<<grid2, hm::BT, 0, b->stream>>>(b->d_jobs, b->d_tiles + nv + nt, (int)ia,
+                                                            b->round + r, b->d_counters + 2 * r + 1);
+        HM_LAUNCH_CHECK("k_batch_advect");
       }
     }
   }
@@ -477,22 +509,49 @@ int hm_batch_create(hm_context *ctx, hm_batch **out)
   if (!b) return hm::fail(HM_ERR_OUT_OF_MEMORY, "hm_batch_create: host allocation failed");
   b->ctx = ctx;
   b->device = ctx->device;
-  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  /* the highest stream priority: a batch of small jobs runs beside plain
+   * solves of large grids (the served form) and its rounds go first */
+  int lo_prio = 0, hi_prio = 0;
+  cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+  cudaError_t e = cudaStreamCreateWithPriority(&b->stream, cudaStreamNonBlocking, hi_prio);
   if (e != cudaSuccess)
   {
     delete b;
     return hm::cuda_fail(e, "hm_batch_create: cudaStreamCreate");
   }
-  b->smem = hm::FusedLayout<hm::BT, hm::BR>::SMEM;
-  int per_sm = 0, sms = 0;
-  HM_CUDA_TRY(cudaFuncSetAttribute(hm::k_batch_round, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
-  HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hm::k_batch_round, hm::BT, b->smem));
+  b->lists = new (std::nothrow) TileLists();
+  if (!b->lists)
+  {
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return hm::fail(HM_ERR_OUT_OF_MEMORY, "hm_batch_create: host allocation failed");
+  }
+  /* job state comes from a pool of the batch's own that keeps freed memory
+   * for the next admission (the served form admits and releases jobs all
+   * the time; mapping fresh memory for each would cost milliseconds) */
+  {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = b->device;
+    e = cudaMemPoolCreate(&b->pool, &props);
+    if (e != cudaSuccess)
+    {
+      delete b->lists;
+      cudaStreamDestroy(b->stream);
+      delete b;
+      return hm::cuda_fail(e, "hm_batch_create: cudaMemPoolCreate");
+    }
+    cuuint64_t keep = ~(cuuint64_t)0;
+    HM_CUDA_TRY(cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  int per_sm = 0, per_sm_adv = 0, sms = 0;
+  HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hm::k_batch_round, hm::BT, 0));
+  HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_adv, hm::k_batch_advect, hm::BT, 0));
   HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
   b->grid_cap = std::max(1, per_sm) * std::max(1, sms);
-  b->defer_cap = 1u << 16;
-  HM_CUDA_TRY(cudaMallocAsync((void **)&b->d_defer, b->defer_cap * sizeof(hm::Deferred), b->stream));
-  HM_CUDA_TRY(cudaMallocAsync((void **)&b->d_defer_count, 2 * sizeof(unsigned), b->stream));
-  HM_CUDA_TRY(cudaMemsetAsync(b->d_defer_count, 0, 2 * sizeof(unsigned), b->stream));
+  b->grid_cap_adv = std::max(1, per_sm_adv) * std::max(1, sms);
   *out = b;
   return HM_OK;
 }
@@ -509,7 +568,7 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
   HJob h;
   h.desc = *job;
   h.bytes = job_bytes(*job);
-  cudaError_t e = cudaMallocAsync(&h.mem, h.bytes, b->stream);
+  cudaError_t e = cudaMallocFromPoolAsync(&h.mem, h.bytes, b->pool, b->stream);
   if (e != cudaSuccess)
   {
     cudaGetLastError();
@@ -526,14 +585,17 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
   d.start = b->round;
   if (job->kind == HM_JOB_THERMAL)
   {
-    d.nbx = (job->nx + hm::TH_W - 1) / hm::TH_W;
-    d.nby = (job->ny + hm::TH_H - 1) / hm::TH_H;
     d.tz[0] = job->z;
     d.tz[1] = base;
     d.talus = job->talus;
     d.tv = job->talus_value;
     d.bed = job->bedrock;
     d.bed_mode = job->bedrock_mode;
+    auto al8 = [](const void *p) { return ((uintptr_t)p & 7u) == 0; };
+    d.pairs = job->nx % 2 == 0 && al8(d.tz[0]) && al8(d.tz[1]) && (!d.talus || al8(d.talus)) && (!d.bed || al8(d.bed));
+    const int tw = d.pairs ? 2 * hm::TH_W : hm::TH_W;
+    d.nbx = (job->nx + tw - 1) / tw;
+    d.nby = (job->ny + hm::TH_H - 1) / hm::TH_H;
     if (job->deposition_map)
     {
       h.z0 = base + na;
@@ -545,8 +607,10 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
   {
     hm_vpipes_params p = job->vpipes;
     p.iterations = job->iterations;
-    d.nbx = (job->nx + hm::VP_W - 1) / hm::VP_W;
-    d.nby = (job->ny + hm::VP_H - 1) / hm::VP_H;
+    d.nbx = (job->nx + hm::FT_TX - 1) / hm::FT_TX;
+    d.nby = (job->ny + hm::FT_TY - 1) / hm::FT_TY;
+    d.anx = (job->nx + hm::AD_W - 1) / hm::AD_W;
+    d.any = (job->ny + hm::AD_H - 1) / hm::AD_H;
     hm::VpFields A{job->z, base + 0 * na, base + 1 * na, base + 2 * na, base + 3 * na, base + 4 * na, base + 5 * na};
     hm::VpFields B{base + 6 * na, base + 7 * na, base + 8 * na, base + 9 * na, base + 10 * na, base + 11 * na,
                    base + 12 * na};
@@ -560,7 +624,10 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
     d.rain = job->rain_map;
     d.u_out = job->vel_u;
     d.v_out = job->vel_v;
-    d.partials = (double *)(base + 13 * na);
+    d.s1 = base + 13 * na;
+    d.u = base + 14 * na;
+    d.v = base + 15 * na;
+    d.partials = (double *)(base + 16 * na);
     const size_t tiles = (size_t)d.nbx * d.nby;
     const size_t parts = std::max(tiles, hm::vpipes_init_partials());
     d.sc = (hm::VpScalars *)((char *)d.partials + align_up(parts * sizeof(double), 256));
@@ -571,32 +638,7 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
   h.live = true;
   b->jobs.push_back(h);
   b->dirty = true;
-  /* deferred-advection list: room for 1/32 of the admitted vpipes cells
-   * (the same share as a single solve); overflowing samples would be
-   * resolved inline, stalling their CTA */
-  if (job->kind == HM_JOB_VPIPES)
-  {
-    size_t cells = 0;
-    for (const HJob &x : b->jobs)
-      if (x.live && x.desc.kind == HM_JOB_VPIPES) cells += (size_t)x.desc.nx * x.desc.ny;
-    const size_t want = std::max<size_t>(1u << 16, cells / 32);
-    if (want > b->defer_cap)
-    {
-      /* the list is empty between rounds: reallocation only has to be
-       * ordered after the work already queued */
-      HM_CUDA_TRY(cudaFreeAsync(b->d_defer, b->stream));
-      b->d_defer = nullptr;
-      const size_t cap = want + want / 2;
-      e = cudaMallocAsync((void **)&b->d_defer, cap * sizeof(hm::Deferred), b->stream);
-      if (e != cudaSuccess)
-      {
-        cudaGetLastError();
-        b->defer_cap = 0;
-        return hm::cuda_fail(e, "hm_batch_add: deferred list allocation");
-      }
-      b->defer_cap = (unsigned)cap;
-    }
-  }
+  b->tiles_dirty = true;
   *job_id = (int)b->jobs.size() - 1;
   if (job->iterations == 0) return finalize_job(b, b->jobs.back());
   return HM_OK;
@@ -659,10 +701,10 @@ int hm_batch_destroy(hm_batch *b)
   if (b->d_jobs) cudaFreeAsync(b->d_jobs, b->stream);
   if (b->d_tiles) cudaFreeAsync(b->d_tiles, b->stream);
   if (b->d_counters) cudaFreeAsync(b->d_counters, b->stream);
-  if (b->d_defer) cudaFreeAsync(b->d_defer, b->stream);
-  if (b->d_defer_count) cudaFreeAsync(b->d_defer_count, b->stream);
   cudaStreamSynchronize(b->stream);
   cudaStreamDestroy(b->stream);
+  if (b->pool) cudaMemPoolDestroy(b->pool);
+  delete b->lists;
   delete b;
   return HM_OK;
 }

@@ -33,6 +33,7 @@
 #include "hm_internal.h"
 #include "hm_thermal.h"
 #include "hm_thermal_math.cuh"
+#include "hm_thermal_sweep.cuh"
 #include "hm_tune.h"
 
 namespace hm
@@ -45,17 +46,10 @@ __device__ __forceinline__ int clamp_col(int g, int n) { return g < 0 ? 0 : (g >
 /* ------------------------------------------------------------------ */
 
 constexpr int SW_NT = 256; /* 8 warps; a warp owns 32 columns              */
-constexpr int SW_P = 8;    /* rows whose loads are issued together          */
 constexpr int SW_H = 16;   /* output rows per CTA (a multiple of SW_P)      */
 
-/* One Jacobi step.  A warp walks down SW_H rows of its 32 columns; every
- * row of z is loaded once per warp (lanes 0 and 31 also load the column
- * just outside the warp) and the west / east neighbours come from warp
- * shuffles, so a cell costs two coalesced loads per 32 cells instead of
- * nine loads.  The loads of SW_P rows (z, talus, bedrock) are issued
- * before any of them is used, which keeps enough bytes in flight to cover
- * the HBM latency.  Cell rule and border copies as the reference kernel
- * (thermal.cl:26-100 in Jacobi form). */
+/* One Jacobi step, a warp per 32 columns and SW_H rows
+ * (hm_thermal_sweep.cuh). */
 template <bool TMAP, int BED>
 __global__ void __launch_bounds__(SW_NT)
     k_thermal_sweep(const float *__restrict__ a,
@@ -67,84 +61,15 @@ __global__ void __launch_bounds__(SW_NT)
                     const float *__restrict__ bedrock,
                     int first)
 {
-  const int lane = threadIdx.x & 31;
   const int wx = (blockIdx.x * (SW_NT / 32) + (threadIdx.x >> 5)) * 32;
   if (wx >= nx) return; /* the whole warp: no CTA barrier in this kernel */
-  const int  gx = wx + lane;
-  const bool live = gx < nx;
-  const int  gxc = live ? gx : nx - 1;
-  /* lanes 0 and 31 also load the column west / east of the warp */
-  const int  hx = lane == 0 ? max(wx - 1, 0) : (lane == 31 ? min(wx + 32, nx - 1) : gxc);
-  const int  y0 = blockIdx.y * SW_H;
-  const int  y1 = min(ny, y0 + SW_H);
-
-  float vc[SW_P + 2], vl[SW_P + 2], vr[SW_P + 2];
-  {
-    const float *r0 = a + (size_t)max(y0 - 1, 0) * nx, *r1 = a + (size_t)y0 * nx;
-    vc[0] = __ldg(r0 + gxc);
-    vl[0] = __ldg(r0 + hx);
-    vc[1] = __ldg(r1 + gxc);
-    vl[1] = __ldg(r1 + hx);
-#pragma unroll
-    for (int q = 0; q < 2; q++)
-    {
-      const float up = __shfl_up_sync(0xffffffffu, vc[q], 1), dn = __shfl_down_sync(0xffffffffu, vc[q], 1);
-      vr[q] = lane == 31 ? vl[q] : dn;
-      vl[q] = lane == 0 ? vl[q] : up;
-    }
-  }
-  for (int j0 = y0; j0 < y1; j0 += SW_P)
-  {
-    float tl[SW_P], bd[SW_P];
-#pragma unroll
-    for (int q = 0; q < SW_P; q++)
-    {
-      const float *r = a + (size_t)min(j0 + 1 + q, ny - 1) * nx;
-      vc[q + 2] = __ldg(r + gxc);
-      vl[q + 2] = __ldg(r + hx); /* the halo value until the shuffles below */
-      const size_t o = (size_t)min(j0 + q, ny - 1) * nx + gxc;
-      tl[q] = TMAP ? __ldg(talus + o) : talus_value;
-      bd[q] = BED != BED_NONE ? __ldg(bedrock + o) : 0.f;
-    }
-#pragma unroll
-    for (int q = 2; q < SW_P + 2; q++)
-    {
-      const float up = __shfl_up_sync(0xffffffffu, vc[q], 1), dn = __shfl_down_sync(0xffffffffu, vc[q], 1);
-      vr[q] = lane == 31 ? vl[q] : dn;
-      vl[q] = lane == 0 ? vl[q] : up;
-    }
-#pragma unroll
-    for (int q = 0; q < SW_P; q++)
-    {
-      const int j = j0 + q;
-      if (!live || j >= y1) continue;
-      float out;
-      /* apply_boundaries, _common_index.cl:106-132 */
-      if (gx == 0) out = vr[q + 1];
-      else if (gx == nx - 1) out = vl[q + 1];
-      else if (j == 0) out = vc[q + 2];
-      else if (j == ny - 1) out = vc[q];
-      else
-        out = thermal_cell<BED>(vc[q + 1], vl[q + 1], vc[q + 2], vc[q], vr[q + 1], vl[q], vl[q + 2], vr[q], vr[q + 2],
-                                tl[q], bd[q], first != 0);
-      b[(size_t)j * nx + gx] = out;
-    }
-    vc[0] = vc[SW_P];
-    vl[0] = vl[SW_P];
-    vr[0] = vr[SW_P];
-    vc[1] = vc[SW_P + 1];
-    vl[1] = vl[SW_P + 1];
-    vr[1] = vr[SW_P + 1];
-  }
+  const int y0 = blockIdx.y * SW_H;
+  thermal_sweep_warp<TMAP, BED>(a, b, nx, ny, talus, talus_value, bedrock, first, wx, y0, min(ny, y0 + SW_H));
 }
 
-/* The same sweep with two adjacent columns per lane (a warp owns 64
- * columns): z, talus and bedrock move as 8-byte pairs, and one pair of
- * shuffles per row serves both cells, which halves the per-cell load,
- * shuffle and address work.  Needs an even nx and 8-byte aligned grids;
- * identical bits to k_thermal_sweep. */
+/* One Jacobi step, a warp per 64 columns (two per lane) and SW_H rows
+ * (hm_thermal_sweep.cuh); even nx, 8-byte aligned grids. */
 constexpr int S2_NT = 128; /* 4 warps; a warp owns 64 columns */
-constexpr int S2_P = 4;    /* rows whose loads are issued together */
 
 template <bool TMAP, int BED>
 __global__ void __launch_bounds__(S2_NT)
@@ -157,78 +82,10 @@ __global__ void __launch_bounds__(S2_NT)
                      const float *__restrict__ bedrock,
                      int first)
 {
-  const int lane = threadIdx.x & 31;
   const int wx = (blockIdx.x * (S2_NT / 32) + (threadIdx.x >> 5)) * 64;
   if (wx >= nx) return; /* the whole warp: no CTA barrier in this kernel */
-  const int  gx = wx + 2 * lane; /* first of the lane's two columns (nx is even) */
-  const bool live = gx < nx;
-  const int  gxc = live ? gx : nx - 2;
-  /* lanes 0 and 31 also load the column west / east of the warp */
-  const int  hx = lane == 0 ? max(wx - 1, 0) : (lane == 31 ? min(wx + 64, nx - 1) : gxc);
-  const int  y0 = blockIdx.y * SW_H;
-  const int  y1 = min(ny, y0 + SW_H);
-
-  /* per row: the pair (x, y), the west neighbour of x and the east one of y */
-  float vx[S2_P + 2], vy[S2_P + 2], vw[S2_P + 2], ve[S2_P + 2];
-  auto load = [&](int r, int q) {
-    const float *row = a + (size_t)r * nx;
-    const float2 t = __ldg(reinterpret_cast<const float2 *>(row + gxc));
-    vx[q] = t.x;
-    vy[q] = t.y;
-    vw[q] = __ldg(row + hx); /* the halo value until the shuffles */
-  };
-  auto exchange = [&](int q) {
-    const float up = __shfl_up_sync(0xffffffffu, vy[q], 1), dn = __shfl_down_sync(0xffffffffu, vx[q], 1);
-    ve[q] = lane == 31 ? vw[q] : dn;
-    vw[q] = lane == 0 ? vw[q] : up;
-  };
-  load(max(y0 - 1, 0), 0);
-  load(y0, 1);
-  exchange(0);
-  exchange(1);
-  for (int j0 = y0; j0 < y1; j0 += S2_P)
-  {
-    float2 tl[S2_P], bd[S2_P];
-#pragma unroll
-    for (int q = 0; q < S2_P; q++)
-    {
-      load(min(j0 + 1 + q, ny - 1), q + 2);
-      const size_t o = (size_t)min(j0 + q, ny - 1) * nx + gxc;
-      tl[q] = TMAP ? __ldg(reinterpret_cast<const float2 *>(talus + o)) : make_float2(talus_value, talus_value);
-      bd[q] = BED != BED_NONE ? __ldg(reinterpret_cast<const float2 *>(bedrock + o)) : make_float2(0.f, 0.f);
-    }
-#pragma unroll
-    for (int q = 2; q < S2_P + 2; q++) exchange(q);
-#pragma unroll
-    for (int q = 0; q < S2_P; q++)
-    {
-      const int j = j0 + q;
-      if (!live || j >= y1) continue;
-      float2 out;
-      /* apply_boundaries, _common_index.cl:106-132, for each of the two cells */
-      if (gx == 0) out.x = vy[q + 1];
-      else if (j == 0) out.x = vx[q + 2];
-      else if (j == ny - 1) out.x = vx[q];
-      else
-        out.x = thermal_cell<BED>(vx[q + 1], vw[q + 1], vx[q + 2], vx[q], vy[q + 1], vw[q], vw[q + 2], vy[q],
-                                  vy[q + 2], tl[q].x, bd[q].x, first != 0);
-      if (gx + 1 == nx - 1) out.y = vx[q + 1];
-      else if (j == 0) out.y = vy[q + 2];
-      else if (j == ny - 1) out.y = vy[q];
-      else
-        out.y = thermal_cell<BED>(vy[q + 1], vx[q + 1], vy[q + 2], vy[q], ve[q + 1], vx[q], vx[q + 2], ve[q],
-                                  ve[q + 2], tl[q].y, bd[q].y, first != 0);
-      *reinterpret_cast<float2 *>(b + (size_t)j * nx + gx) = out;
-    }
-    vx[0] = vx[S2_P];
-    vy[0] = vy[S2_P];
-    vw[0] = vw[S2_P];
-    ve[0] = ve[S2_P];
-    vx[1] = vx[S2_P + 1];
-    vy[1] = vy[S2_P + 1];
-    vw[1] = vw[S2_P + 1];
-    ve[1] = ve[S2_P + 1];
-  }
+  const int y0 = blockIdx.y * SW_H;
+  thermal_sweep2_warp<TMAP, BED>(a, b, nx, ny, talus, talus_value, bedrock, first, wx, y0, min(ny, y0 + SW_H));
 }
 
 /* ------------------------------------------------------------------ */

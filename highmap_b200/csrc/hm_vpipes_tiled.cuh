@@ -406,6 +406,45 @@ int fwe_dispatch(bool maintain, int f, Launch launch)
  * rounds of loads). */
 constexpr int ADV_R = 4;
 
+/* Advection of rows jb .. jb+R-1 of column i (rows past the grid are
+ * loaded clamped and not stored). */
+template <int R>
+__device__ __forceinline__ void advect_rows(const float *__restrict__ s1,
+                                            const float *__restrict__ u,
+                                            const float *__restrict__ v,
+                                            float *__restrict__ s_out,
+                                            const VpConst &c,
+                                            int i,
+                                            int jb)
+{
+  float uu[R], vv[R];
+#pragma unroll
+  for (int q = 0; q < R; q++)
+  {
+    const size_t k = (size_t)min(jb + q, c.ny - 1) * c.nx + i;
+    uu[q] = __ldg(u + k);
+    vv[q] = __ldg(v + k);
+  }
+  Tap   t[R];
+  float g[R][4];
+#pragma unroll
+  for (int q = 0; q < R; q++)
+  {
+    const int    j = min(jb + q, c.ny - 1);
+    const float  x = fsub((float)i, fmul(c.dt, uu[q]));
+    const float  y = fsub((float)j, fmul(c.dt, vv[q]));
+    t[q] = linear_tap(x, y, c.nx, c.ny);
+    const size_t r0 = (size_t)t[q].j0 * c.nx, r1 = (size_t)t[q].j1 * c.nx;
+    g[q][0] = __ldg(s1 + r0 + t[q].i0);
+    g[q][1] = __ldg(s1 + r0 + t[q].i1);
+    g[q][2] = __ldg(s1 + r1 + t[q].i0);
+    g[q][3] = __ldg(s1 + r1 + t[q].i1);
+  }
+#pragma unroll
+  for (int q = 0; q < R; q++)
+    if (jb + q < c.ny) s_out[(size_t)(jb + q) * c.nx + i] = blend(t[q], g[q][0], g[q][1], g[q][2], g[q][3]);
+}
+
 template <int R>
 __global__ void __launch_bounds__(256) k_vp_advect(const float *__restrict__ s1,
                                                     const float *__restrict__ u,
@@ -415,35 +454,7 @@ __global__ void __launch_bounds__(256) k_vp_advect(const float *__restrict__ s1,
 {
   const int i = blockIdx.x * 256 + threadIdx.x;
   if (i >= c.nx) return;
-  for (int jb = blockIdx.y * R; jb < c.ny; jb += gridDim.y * R)
-  {
-    float uu[R], vv[R];
-#pragma unroll
-    for (int q = 0; q < R; q++)
-    {
-      const size_t k = (size_t)min(jb + q, c.ny - 1) * c.nx + i;
-      uu[q] = __ldg(u + k);
-      vv[q] = __ldg(v + k);
-    }
-    Tap   t[R];
-    float g[R][4];
-#pragma unroll
-    for (int q = 0; q < R; q++)
-    {
-      const int    j = min(jb + q, c.ny - 1);
-      const float  x = fsub((float)i, fmul(c.dt, uu[q]));
-      const float  y = fsub((float)j, fmul(c.dt, vv[q]));
-      t[q] = linear_tap(x, y, c.nx, c.ny);
-      const size_t r0 = (size_t)t[q].j0 * c.nx, r1 = (size_t)t[q].j1 * c.nx;
-      g[q][0] = __ldg(s1 + r0 + t[q].i0);
-      g[q][1] = __ldg(s1 + r0 + t[q].i1);
-      g[q][2] = __ldg(s1 + r1 + t[q].i0);
-      g[q][3] = __ldg(s1 + r1 + t[q].i1);
-    }
-#pragma unroll
-    for (int q = 0; q < R; q++)
-      if (jb + q < c.ny) s_out[(size_t)(jb + q) * c.nx + i] = blend(t[q], g[q][0], g[q][1], g[q][2], g[q][3]);
-  }
+  for (int jb = blockIdx.y * R; jb < c.ny; jb += gridDim.y * R) advect_rows<R>(s1, u, v, s_out, c, i, jb);
 }
 
 } // namespace hm

@@ -6,11 +6,14 @@ call at a time with the plain device path (hm_thermal_device /
 hm_vpipes_device), both on device-resident inputs.
 
 Served form: a request loop, as an interactive node-graph editor would
-drive it: requests arrive as a Poisson stream, are admitted into an open
-batch while their device state fits an HBM budget, advance together a few
-rounds per tick (continuous batching), and are retired when done; latency
-is completion minus arrival.  The same stream served first-come
-first-served by the plain path is the comparison point.
+drive it: requests arrive as a Poisson stream; small ones are admitted
+into an open batch while their device state fits an HBM budget, advance
+together a few rounds per tick (continuous batching) on a high-priority
+stream and are retired when done, while large ones, which fill the GPU on
+their own, run one at a time through the plain path on a low-priority
+stream beside them; latency is completion minus arrival.  The same stream
+served first-come first-served by the plain path is the comparison
+point.
 
 Inputs are seeded synthetic fBm fields (highmap_b200.inputs).
 """
@@ -157,34 +160,78 @@ class FieldPool:
         return f[oy:oy + ny, ox:ox + nx].contiguous()
 
 
-def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=8):
-    """Continuous batching: returns per-request latencies (s) and totals."""
+def _bytes_plain(r):
+    """Device workspace a plain solve of request r needs (its grid and the
+    solver's scratch), for the admission budget."""
+    n = r["nx"] * r["ny"] * 4
+    return n * (2 if r["kind"] == "thermal" else 17)
+
+
+def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=64, large_cells=1024 * 1024):
+    """Size-aware continuous batching: returns per-request latencies (s) and
+    totals.
+
+    Requests of at least `large_cells` cells fill the GPU on their own:
+    they go, first come first served, through the plain device path on a
+    low-priority stream (one at a time; their state stays in the solver's
+    workspace).  Smaller requests are admitted into an open batch while
+    their device state fits the HBM budget, advance together a few rounds
+    per tick on the batch's high-priority stream, which runs beside the
+    large solve, and retire when done.  A tick runs until the next batched
+    job completes, at most `rounds_per_tick` rounds (which bounds how long
+    an arrival waits for admission)."""
     import torch
-    b = B.Batch(G.Context(torch.cuda.current_device()))
+    dev = torch.cuda.current_device()
+    b = B.Batch(G.Context(dev))
+    big_ctx = G.Context(dev)
+    big_stream = torch.cuda.Stream(priority=0)  # lowest priority
     pending = list(reqs)
-    waiting = []  # arrived, not admitted (FIFO)
-    active = {}   # job id -> (request, tensor, job)
+    waiting = []     # arrived small requests, not admitted (FIFO)
+    big_queue = []   # arrived large requests (FIFO)
+    big = None       # (request, z, done event) of the running large solve
+    active = {}      # job id -> (request, tensor, job)
     lat = {}
     t0 = time.perf_counter()
     cells = 0
-    while pending or waiting or active:
+    while pending or waiting or active or big_queue or big:
         now = time.perf_counter() - t0
         while pending and pending[0]["arrival"] <= now:
-            waiting.append(pending.pop(0))
+            r = pending.pop(0)
+            (big_queue if r["nx"] * r["ny"] >= large_cells else waiting).append(r)
+        # the large lane: start the next large solve when the lane is free
+        if big is not None and big[2].query():
+            r = big[0]
+            lat[r["id"]] = time.perf_counter() - t0 - r["arrival"]
+            cells += r["nx"] * r["ny"] * r["iterations"]
+            big = None
+        if big is None and big_queue:
+            r = big_queue.pop(0)
+            z = pool.take(r["id"], r["nx"], r["ny"])
+            torch.cuda.current_stream().synchronize()
+            _plain(r, z, big_ctx, big_stream.cuda_stream)
+            ev = torch.cuda.Event()
+            ev.record(big_stream)
+            big = (r, z, ev)
+        big_bytes = _bytes_plain(big[0]) if big is not None else 0
         while waiting:
             r = waiting[0]
             z = pool.take(r["id"], r["nx"], r["ny"])
             job = _job(r, z)
-            if active and b.bytes_in_use() + B.job_bytes(job) > budget_bytes:
+            if active and b.bytes_in_use() + B.job_bytes(job) + big_bytes > budget_bytes:
                 break
             waiting.pop(0)
+            # the window copy runs on torch's stream, the batch on its own
+            torch.cuda.current_stream().synchronize()
             jid = b.add(job)
             active[jid] = (r, z, job)
         if not active:
-            if pending:
+            if big is not None:
+                time.sleep(0.0002)
+            elif pending:
                 time.sleep(max(0.0, min(0.01, pending[0]["arrival"] - now)))
             continue
-        b.step(rounds_per_tick)
+        nearest = min(r["iterations"] - b.status(jid)[0] for jid, (r, _, _) in active.items())
+        b.step(max(1, min(nearest, rounds_per_tick)))
         b.synchronize()
         done_t = time.perf_counter() - t0
         for jid in list(active):
@@ -195,6 +242,7 @@ def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=8):
                 b.release(jid)
     total = time.perf_counter() - t0
     b.close()
+    big_ctx.close()
     return lat, cells, total
 
 
@@ -249,6 +297,7 @@ def run_serve_benchmark(n_requests=200, rates=(2.0, 8.0, 32.0), seed=0, check=3)
     for r in reqs:
         z = pool.take(r["id"], r["nx"], r["ny"])
         zs.append(z)
+        torch.cuda.current_stream().synchronize()
         ids.append(b.add(_job(r, z)))
     while not all(b.status(i)[1] for i in ids):
         b.step(16)

@@ -132,6 +132,35 @@ def test_staggered_admission(gpu):
     b.close()
 
 
+def test_vpipes_admitted_after_thermal_only_rounds(gpu):
+    """A vpipes job admitted after rounds in which only thermal jobs ran
+    (its predecessor finished and was released, as in the served form)
+    starts with a clean deferred-advection list: the rounds without vpipes
+    tiles re-arm the list's count, so no entry of the released job is
+    replayed.  Both later jobs match the oracle."""
+    import torch
+    from highmap_b200 import batch as B
+    specs = [("vpipes", 250, 250, 12, dict(params=FAST, outputs=True)),
+             ("thermal", 300, 300, 60, dict(talus=0.01)),
+             ("vpipes", 260, 240, 15, dict(params=FAST, outputs=True))]
+    jobs, cases = _make(specs, seed0=90)
+    b = B.Batch()
+    first = b.add(jobs[0])
+    therm = b.add(jobs[1])
+    while not b.status(first)[1]:
+        b.step(1)
+    b.synchronize()
+    b.release(first)
+    b.step(5)  # thermal only
+    second = b.add(jobs[2])
+    while not (b.status(therm)[1] and b.status(second)[1]):
+        b.step(4)
+    b.synchronize()
+    torch.cuda.synchronize()
+    _verify(cases[1:])
+    b.close()
+
+
 def test_job_bytes_accounts_state(gpu):
     import torch
     from highmap_b200 import batch as B
