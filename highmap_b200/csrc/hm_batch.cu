@@ -71,6 +71,7 @@ struct BJob
   float       *s1, *u, *v;
   VpConst      c;
   int          maintain, diffusion, pl_one, kexp_one;
+  int          vec; /* pair stores (even nx, 8-byte aligned outputs) */
   const float *rain;
   float       *u_out, *v_out;
   VpScalars   *sc;
@@ -100,6 +101,7 @@ __device__ __forceinline__ void job_io(const BJob &J, int step, FweIo &io)
   io.v_out = last ? J.v_out : nullptr;
   if (io.u_out && !io.v_out) io.v_out = J.v;
   if (io.v_out && !io.u_out) io.u_out = J.u;
+  io.vec = J.vec;
 }
 
 template <bool TMAP, int BED>
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(BT, 3)
                   long long round,
                   unsigned *counter)
 {
-  __shared__ FweSmem<false> sm;
+  __shared__ FweSmem sm;
   __shared__ int            s_tile;
   /* the current vpipes tile's step description, staged once per tile */
   __shared__ FweIo   s_io;
@@ -158,9 +160,9 @@ __global__ void __launch_bounds__(BT, 3)
       fwe_stage_cp_async(s_io, J.nx, J.ny, tl.y * FT_TX, tl.z * FT_TY, sm);
       __syncthreads();
       if (J.maintain)
-        fwe_compute<true, false, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
+        fwe_compute<true, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
       else
-        fwe_compute<false, false, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
+        fwe_compute<false, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
     }
     else
     {
@@ -627,6 +629,8 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
     d.s1 = base + 13 * na;
     d.u = base + 14 * na;
     d.v = base + 15 * na;
+    d.vec = job->nx % 2 == 0 && ((uintptr_t)job->z & 7u) == 0 && ((uintptr_t)job->vel_u & 7u) == 0 &&
+            ((uintptr_t)job->vel_v & 7u) == 0;
     d.partials = (double *)(base + 16 * na);
     const size_t tiles = (size_t)d.nbx * d.nby;
     const size_t parts = std::max(tiles, hm::vpipes_init_partials());

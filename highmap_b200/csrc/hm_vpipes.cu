@@ -348,6 +348,15 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
   io.s1 = s1;
   io.u = u_buf;
   io.v = v_buf;
+  {
+    /* pair stores: an even row length and 8-byte aligned outputs */
+    auto al8 = [](const void *q) { return ((uintptr_t)q & 7u) == 0; };
+    const void *outs[] = {A.z, A.d, A.fl, A.fr, A.ft, A.fb, B.z, B.d, B.fl, B.fr, B.ft, B.fb, s1, u_buf, v_buf,
+                          vel_u, vel_v};
+    bool        ok = nx % 2 == 0;
+    for (const void *q : outs) ok = ok && al8(q);
+    io.vec = ok ? 1 : 0;
+  }
   const dim3 g1((nx + FT_TX - 1) / FT_TX, (ny + FT_TY - 1) / FT_TY);
   const int  row_groups = (ny + ADV_R - 1) / ADV_R;
   const dim3 g2((nx + 255) / 256, row_groups < 65535 ? row_groups : 65535);

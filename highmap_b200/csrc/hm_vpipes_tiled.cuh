@@ -47,34 +47,24 @@ constexpr int FWE_RAINMAP = 2;   /* a rain map scales rain and top-up   */
 constexpr int FWE_RAINSTEP = 4;  /* rain added every step               */
 constexpr int FWE_GENERIC = 8;   /* options read at run time            */
 
-/* Shared-memory layout of the staged fields.
- *   cp.async staging (TMA = false): region 2 (columns x0-2 .. x0+33, rows
- *     y0-2 .. y0+17) as [20][36]; region 1 (x0-1 .. x0+32, y0-1 .. y0+16) as
- *     [18][34]; element (0, 0) is the region's first cell.
- *   TMA staging (TMA = true): every box starts at column x0-4 (a TMA box
- *     must start on a 16-byte boundary) and is 40 columns wide; region 2
- *     starts at row y0-2, region 1 at y0-1.  Region-2 column q sits at
- *     q + 2, region-1 column l at l + 3.  Each array is padded to 20 rows
- *     so every box starts 128-byte aligned. */
-template <bool TMA>
-struct FweLayout
-{
-  static constexpr int W2 = TMA ? 40 : FT_W2;
-  static constexpr int W1 = TMA ? 40 : FT_W1;
-  static constexpr int H1 = TMA ? FT_H2 : FT_H1; /* allocated rows of region-1 arrays */
-  static constexpr int C2 = TMA ? 2 : 0;         /* column of region-2 cell 0         */
-  static constexpr int C1 = TMA ? 3 : 0;         /* column of region-1 cell 0         */
-};
+/* Shared-memory layout of the staged fields, one for both staging modes.
+ * Every array row covers the 40 columns x0-4 .. x0+35 (a TMA box must start
+ * on a 16-byte boundary, so the boxes start at x0-4), column c holding
+ * global column x0-4+c.  z and d hold rows y0-2 .. y0+17 (region 2: the
+ * tile and a 2-cell halo), s, the old fluxes fo and the new fluxes fn rows
+ * y0-1 .. y0+16 (region 1: a 1-cell halo).  The tile's own columns sit at
+ * 4 .. 35, so cell pairs (2k, 2k+1) of the tile are 8-byte aligned in
+ * every array.  Each staged array is padded to 20 rows so every box starts
+ * 128-byte aligned. */
+constexpr int FW = 40;
 
-template <bool TMA>
 struct FweSmem
 {
-  using L = FweLayout<TMA>;
-  alignas(128) float z[FT_H2][L::W2];
-  alignas(128) float d[FT_H2][L::W2];
-  alignas(128) float s[L::H1][L::W1];
-  alignas(128) float fo[4][L::H1][L::W1];
-  float    fn[4][FT_H1][FT_W1];
+  alignas(128) float z[FT_H2][FW];
+  alignas(128) float d[FT_H2][FW];
+  alignas(128) float s[FT_H2][FW];
+  alignas(128) float fo[4][FT_H2][FW];
+  alignas(16) float fn[4][FT_H1][FW];
   uint64_t bar;
 };
 
@@ -88,6 +78,7 @@ struct FweIo
   int          parity;
   int          maintain, diffusion, pl_one, kexp_one;
   float       *u_out, *v_out; /* last step: velocity outputs, nullable */
+  int          vec;           /* nx even and every output 8-byte aligned: pair stores */
 };
 
 /* tensor maps of the seven input fields of one step (TMA staging):
@@ -103,26 +94,25 @@ constexpr unsigned FWE_TMA_BYTES = 4u * 40u * (2u * FT_H2 + 5u * FT_H1);
 /* cp.async staging: z, d on the halo-2 region; s and old fluxes on the
  * halo-1 region; loads clamped to the grid, so every raw neighbour read is
  * the reference's clamp-to-edge read */
-__device__ __forceinline__ void fwe_stage_cp_async(const FweIo &io, int nx, int ny, int x0, int y0,
-                                                   FweSmem<false> &sm)
+__device__ __forceinline__ void fwe_stage_cp_async(const FweIo &io, int nx, int ny, int x0, int y0, FweSmem &sm)
 {
   const int tid = threadIdx.x;
   for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
   {
     const int    ly = e / FT_W2, lx = e - ly * FT_W2;
     const size_t k = (size_t)clampi(y0 - 2 + ly, 0, ny - 1) * nx + clampi(x0 - 2 + lx, 0, nx - 1);
-    cp_async4(&sm.z[ly][lx], io.in.z + k);
-    cp_async4(&sm.d[ly][lx], io.in.d + k);
+    cp_async4(&sm.z[ly][lx + 2], io.in.z + k);
+    cp_async4(&sm.d[ly][lx + 2], io.in.d + k);
   }
   for (int e = tid; e < FT_W1 * FT_H1; e += FT_NT)
   {
     const int    ly = e / FT_W1, lx = e - ly * FT_W1;
     const size_t k = (size_t)clampi(y0 - 1 + ly, 0, ny - 1) * nx + clampi(x0 - 1 + lx, 0, nx - 1);
-    cp_async4(&sm.s[ly][lx], io.in.s + k);
-    cp_async4(&sm.fo[0][ly][lx], io.in.fl + k);
-    cp_async4(&sm.fo[1][ly][lx], io.in.fr + k);
-    cp_async4(&sm.fo[2][ly][lx], io.in.ft + k);
-    cp_async4(&sm.fo[3][ly][lx], io.in.fb + k);
+    cp_async4(&sm.s[ly][lx + 3], io.in.s + k);
+    cp_async4(&sm.fo[0][ly][lx + 3], io.in.fl + k);
+    cp_async4(&sm.fo[1][ly][lx + 3], io.in.fr + k);
+    cp_async4(&sm.fo[2][ly][lx + 3], io.in.ft + k);
+    cp_async4(&sm.fo[3][ly][lx + 3], io.in.fb + k);
   }
   cp_async_commit();
   cp_async_wait<0>();
@@ -135,8 +125,7 @@ __device__ __forceinline__ void fwe_stage_cp_async(const FweIo &io, int nx, int 
  * box; the edge test depends only on the tile, so the barrier inside it is
  * uniform).  Returns false, uniformly across the CTA, if the loads did not
  * complete in time. */
-__device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int ny, int x0, int y0,
-                                              FweSmem<true> &sm)
+__device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int ny, int x0, int y0, FweSmem &sm)
 {
   const int tid = threadIdx.x;
   if (tid == 0)
@@ -188,16 +177,35 @@ __device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int n
   return true;
 }
 
-/* One tile of the step on staged fields: depth at the start of the step,
- * flow on the tile plus a 1-cell ring into shared memory, then water and
- * erosion on the tile, which also store the tile's new fluxes. */
-template <bool MAINTAIN, bool TMA, int F>
-__device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials,
-                                            int bx, int by, int nbx, int nby, FweSmem<TMA> &sm)
+__device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ void   sts2(float *p, float a, float b) { *reinterpret_cast<float2 *>(p) = make_float2(a, b); }
+
+/* Store the values of a cell pair (columns gx, gx + 1 of row offset k = the
+ * pair's first cell): one 8-byte store when both cells are in the grid and
+ * the grids allow it, else one or two 4-byte stores. */
+__device__ __forceinline__ void st_pair(float *p, size_t k, float a, float b, bool second, bool vec)
 {
-  static_assert(FT_TX == 32, "a lane is a column of the tile");
-  using L = FweLayout<TMA>;
-  constexpr int  C1 = L::C1, C2 = L::C2;
+  if (second && vec)
+    *reinterpret_cast<float2 *>(p + k) = make_float2(a, b);
+  else
+  {
+    p[k] = a;
+    if (second) p[k + 1] = b;
+  }
+}
+
+/* One tile of the step on staged fields, two adjacent cells per thread:
+ * depth at the start of the step, flow on the tile plus a 1-cell ring into
+ * shared memory, then water and erosion on the tile, which also store the
+ * tile's new fluxes.  A pair reads its centre values as 8-byte words and
+ * shares its inner neighbours, so a cell costs about half the shared-memory
+ * and store instructions of one cell per thread; the arithmetic of each
+ * cell is unchanged. */
+template <bool MAINTAIN, int F>
+__device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials,
+                                            int bx, int by, int nbx, int nby, FweSmem &sm)
+{
+  static_assert(FT_TX == 32 && FT_TY == 16 && FT_NT == 256, "one cell pair per thread in the water pass");
   constexpr bool GEN = (F & FWE_GENERIC) != 0;
   const int      tid = threadIdx.x;
   const int      nx = c.nx, ny = c.ny;
@@ -210,29 +218,38 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
   const bool     pl_one = GEN ? io.pl_one != 0 : true;
   const bool     kexp_one = GEN ? io.kexp_one != 0 : true;
 
-  /* stored depth -> depth at the start of the step (own elements) */
-  for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
+  /* stored depth -> depth at the start of the step, region 2 (columns
+   * x0-2 .. x0+33 = smem 2 .. 37), 18 pairs per row */
+  for (int e = tid; e < 18 * FT_H2; e += FT_NT)
   {
-    const int   ly = e / FT_W2, lx = e - ly * FT_W2;
-    float      &d = sm.d[ly][lx + C2];
-    const float rn = rain_map ? __ldg(io.rain + (size_t)clampi(y0 - 2 + ly, 0, ny - 1) * nx +
-                                    clampi(x0 - 2 + lx, 0, nx - 1))
-                             : 1.f;
-    d = rain_step ? depth_d1<MAINTAIN, true>(d, rn, add, rvol, c.rps)
-                  : depth_d1<MAINTAIN, false>(d, rn, add, rvol, c.rps);
+    const int q = e / 18, cc = 2 + 2 * (e - q * 18);
+    float2    dd = lds2(&sm.d[q][cc]);
+    float     r0 = 1.f, r1 = 1.f;
+    if (rain_map)
+    {
+      const size_t row = (size_t)clampi(y0 - 2 + q, 0, ny - 1) * nx;
+      r0 = __ldg(io.rain + row + clampi(x0 - 4 + cc, 0, nx - 1));
+      r1 = __ldg(io.rain + row + clampi(x0 - 3 + cc, 0, nx - 1));
+    }
+    if (rain_step)
+    {
+      dd.x = depth_d1<MAINTAIN, true>(dd.x, r0, add, rvol, c.rps);
+      dd.y = depth_d1<MAINTAIN, true>(dd.y, r1, add, rvol, c.rps);
+    }
+    else
+    {
+      dd.x = depth_d1<MAINTAIN, false>(dd.x, r0, add, rvol, c.rps);
+      dd.y = depth_d1<MAINTAIN, false>(dd.y, r1, add, rvol, c.rps);
+    }
+    sts2(&sm.d[q][cc], dd.x, dd.y);
   }
   __syncthreads();
 
-  /* flow pass on the tile and a 1-cell ring (region-1 coordinates) */
-  for (int e = tid; e < FT_W1 * FT_H1; e += FT_NT)
-  {
-    const int ly = e / FT_W1, lx = e - ly * FT_W1;
-    const int qy = ly + 1, qx = lx + 1 + C2; /* region-2 row and smem column of the cell */
-    const int l1 = lx + C1;
-    float     fl = sm.fo[0][ly][l1], fr = sm.fo[1][ly][l1], ft = sm.fo[2][ly][l1], fb = sm.fo[3][ly][l1];
-    const float zc = sm.z[qy][qx], dc = sm.d[qy][qx];
-    const float zw = sm.z[qy][qx - 1], dw = sm.d[qy][qx - 1], ze = sm.z[qy][qx + 1], de = sm.d[qy][qx + 1];
-    const float zs = sm.z[qy + 1][qx], ds = sm.d[qy + 1][qx], zn = sm.z[qy - 1][qx], dn = sm.d[qy - 1][qx];
+  /* flow pass on region 1 (columns x0-1 .. x0+32 = smem 3 .. 36, rows
+   * y0-1 .. y0+16): items 0 .. 287 are the 16 pairs (smem 4 .. 35) of each
+   * of the 18 rows, items 288 .. 323 the two ring columns 3 and 36 */
+  auto flow1 = [&](float zc, float dc, float zw, float dw, float ze, float de, float zs, float ds, float zn,
+                   float dn, float &fl, float &fr, float &ft, float &fb) {
     if (diffusion)
     {
       if (pl_one) flow_cell<true, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
@@ -243,68 +260,107 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
       if (pl_one) flow_cell<false, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
       else flow_cell<false, false>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
     }
-    sm.fn[0][ly][lx] = fl;
-    sm.fn[1][ly][lx] = fr;
-    sm.fn[2][ly][lx] = ft;
-    sm.fn[3][ly][lx] = fb;
+  };
+  for (int e = tid; e < 16 * FT_H1 + 2 * FT_H1; e += FT_NT)
+  {
+    if (e < 16 * FT_H1)
+    {
+      const int    l = e >> 4, cc = 4 + 2 * (e & 15), q = l + 1;
+      const float2 zc = lds2(&sm.z[q][cc]), dc = lds2(&sm.d[q][cc]);
+      const float2 zn = lds2(&sm.z[q - 1][cc]), dn = lds2(&sm.d[q - 1][cc]);
+      const float2 zs = lds2(&sm.z[q + 1][cc]), ds = lds2(&sm.d[q + 1][cc]);
+      const float  zw = sm.z[q][cc - 1], dw = sm.d[q][cc - 1], ze = sm.z[q][cc + 2], de = sm.d[q][cc + 2];
+      float2       fl = lds2(&sm.fo[0][l][cc]), fr = lds2(&sm.fo[1][l][cc]), ft = lds2(&sm.fo[2][l][cc]),
+             fb = lds2(&sm.fo[3][l][cc]);
+      flow1(zc.x, dc.x, zw, dw, zc.y, dc.y, zs.x, ds.x, zn.x, dn.x, fl.x, fr.x, ft.x, fb.x);
+      flow1(zc.y, dc.y, zc.x, dc.x, ze, de, zs.y, ds.y, zn.y, dn.y, fl.y, fr.y, ft.y, fb.y);
+      sts2(&sm.fn[0][l][cc], fl.x, fl.y);
+      sts2(&sm.fn[1][l][cc], fr.x, fr.y);
+      sts2(&sm.fn[2][l][cc], ft.x, ft.y);
+      sts2(&sm.fn[3][l][cc], fb.x, fb.y);
+    }
+    else
+    {
+      const int r = e - 16 * FT_H1, l = r >> 1, cc = (r & 1) ? 36 : 3, q = l + 1;
+      float     fl = sm.fo[0][l][cc], fr = sm.fo[1][l][cc], ft = sm.fo[2][l][cc], fb = sm.fo[3][l][cc];
+      flow1(sm.z[q][cc], sm.d[q][cc], sm.z[q][cc - 1], sm.d[q][cc - 1], sm.z[q][cc + 1], sm.d[q][cc + 1],
+            sm.z[q + 1][cc], sm.d[q + 1][cc], sm.z[q - 1][cc], sm.d[q - 1][cc], fl, fr, ft, fb);
+      sm.fn[0][l][cc] = fl;
+      sm.fn[1][l][cc] = fr;
+      sm.fn[2][l][cc] = ft;
+      sm.fn[3][l][cc] = fb;
+    }
   }
   __syncthreads();
 
-  /* water and erosion on the tile: warp w takes rows w, w + 8, ...; a lane
-   * is a column */
+  /* water and erosion on the tile: thread t takes row t / 16 and the pair
+   * of tile columns 2 (t % 16), 2 (t % 16) + 1 */
   double    part = 0.0;
-  const int lane = tid & 31, w = tid >> 5;
-  const int gx = x0 + lane;
-  /* region-1 columns of the clamped x neighbours (new fluxes are derived:
-   * outside the grid they are the edge cell's own values) */
-  const int lxc = lane + 1;
-  const int lxw = clampi(gx - 1, 0, nx - 1) - (x0 - 1);
-  const int lxe = clampi(gx + 1, 0, nx - 1) - (x0 - 1);
-  const int sc1 = lxc + C1; /* smem column of the cell in region-1 arrays */
-  for (int ty = w; ty < FT_TY; ty += FT_NT / 32)
+  const int ty = tid >> 4, pk = tid & 15;
+  const int gy = y0 + ty, gx = x0 + 2 * pk;
+  const int cc = 4 + 2 * pk; /* smem column of the first cell */
+  if (gx < nx && gy < ny)
   {
-    const int gy = y0 + ty;
-    if (gx >= nx || gy >= ny) continue;
-    const int ly = ty + 1;
-    const int lyn = clampi(gy - 1, 0, ny - 1) - (y0 - 1);
-    const int lys = clampi(gy + 1, 0, ny - 1) - (y0 - 1);
-    const int qy = ty + 2, qx = lane + 2 + C2; /* region-2 row and smem column */
-    float     d2, u, v;
-    const float d1c = sm.d[qy][qx];
-    const float flc = sm.fn[0][ly][lxc], frc = sm.fn[1][ly][lxc], ftc = sm.fn[2][ly][lxc], fbc = sm.fn[3][ly][lxc];
+    const bool second = gx + 1 < nx;
+    const int  l = ty + 1, q = ty + 2;
+    /* flux neighbours: rows and columns clamped to the grid (new fluxes are
+     * derived: outside the grid they are the edge cell's own values) */
+    const int  ln = clampi(gy - 1, 0, ny - 1) - (y0 - 1);
+    const int  ls = clampi(gy + 1, 0, ny - 1) - (y0 - 1);
+    const int  cw0 = gx > 0 ? cc - 1 : cc;          /* west of the first cell  */
+    const int  ce0 = second ? cc + 1 : cc;          /* east of the first cell  */
+    const int  ce1 = gx + 2 < nx ? cc + 2 : cc + 1; /* east of the second cell */
+    const float2 flc = lds2(&sm.fn[0][l][cc]), frc = lds2(&sm.fn[1][l][cc]), ftc = lds2(&sm.fn[2][l][cc]),
+                 fbc = lds2(&sm.fn[3][l][cc]);
+    const float2 ftn = lds2(&sm.fn[2][ln][cc]), fbs = lds2(&sm.fn[3][ls][cc]);
+    const float  frw0 = sm.fn[1][l][cw0], fle0 = sm.fn[0][l][ce0], fle1 = sm.fn[0][l][ce1];
+    const float2 d1 = lds2(&sm.d[q][cc]);
+    float        d2a, ua, va, d2b, ub, vb;
     if (pl_one)
-      water_cell<true>(c, d1c, flc, frc, ftc, fbc, sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc],
-                       sm.fn[3][lys][lxc], d2, u, v);
+    {
+      water_cell<true>(c, d1.x, flc.x, frc.x, ftc.x, fbc.x, frw0, fle0, ftn.x, fbs.x, d2a, ua, va);
+      water_cell<true>(c, d1.y, flc.y, frc.y, ftc.y, fbc.y, frc.x, fle1, ftn.y, fbs.y, d2b, ub, vb);
+    }
     else
-      water_cell<false>(c, d1c, flc, frc, ftc, fbc, sm.fn[1][ly][lxw], sm.fn[0][ly][lxe], sm.fn[2][lyn][lxc],
-                        sm.fn[3][lys][lxc], d2, u, v);
-    float zo, so;
+    {
+      water_cell<false>(c, d1.x, flc.x, frc.x, ftc.x, fbc.x, frw0, fle0, ftn.x, fbs.x, d2a, ua, va);
+      water_cell<false>(c, d1.y, flc.y, frc.y, ftc.y, fbc.y, frc.x, fle1, ftn.y, fbs.y, d2b, ub, vb);
+    }
+    const float2 zc = lds2(&sm.z[q][cc]), zn = lds2(&sm.z[q - 1][cc]), zs = lds2(&sm.z[q + 1][cc]);
+    const float  zw = sm.z[q][cc - 1], ze = sm.z[q][cc + 2];
+    const float2 s0 = lds2(&sm.s[l][cc]), sn = lds2(&sm.s[l - 1][cc]), ss = lds2(&sm.s[l + 1][cc]);
+    const float  sw = sm.s[l][cc - 1], se = sm.s[l][cc + 2];
+    float        zoa, soa, zob, sob;
     if (kexp_one)
-      erosion_cell<true>(c, sm.z[qy][qx], sm.s[ly][sc1], sm.z[qy][qx - 1], sm.z[qy][qx + 1], sm.z[qy - 1][qx],
-                         sm.z[qy + 1][qx], sm.s[ly][sc1 - 1], sm.s[ly][sc1 + 1], sm.s[ly - 1][sc1],
-                         sm.s[ly + 1][sc1], d2, u, v, zo, so);
+    {
+      erosion_cell<true>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
+      erosion_cell<true>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+    }
     else
-      erosion_cell<false>(c, sm.z[qy][qx], sm.s[ly][sc1], sm.z[qy][qx - 1], sm.z[qy][qx + 1], sm.z[qy - 1][qx],
-                          sm.z[qy + 1][qx], sm.s[ly][sc1 - 1], sm.s[ly][sc1 + 1], sm.s[ly - 1][sc1],
-                          sm.s[ly + 1][sc1], d2, u, v, zo, so);
+    {
+      erosion_cell<false>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
+      erosion_cell<false>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+    }
     const size_t k = (size_t)gy * nx + gx;
-    const float  de = fmul(d2, c.keep);
-    /* the cell's new fluxes, stored here where a warp writes whole rows */
-    io.out.fl[k] = flc;
-    io.out.fr[k] = frc;
-    io.out.ft[k] = ftc;
-    io.out.fb[k] = fbc;
-    io.out.z[k] = zo;
-    io.out.d[k] = de;
-    io.s1[k] = so;
-    io.u[k] = u;
-    io.v[k] = v;
+    const bool   vec = io.vec != 0;
+    const float  dea = fmul(d2a, c.keep), deb = fmul(d2b, c.keep);
+    /* the cells' new fluxes, stored here where a warp writes whole rows */
+    st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
+    st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
+    st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
+    st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
+    st_pair(io.out.z, k, zoa, zob, second, vec);
+    st_pair(io.out.d, k, dea, deb, second, vec);
+    st_pair(io.s1, k, soa, sob, second, vec);
+    st_pair(io.u, k, ua, ub, second, vec);
+    st_pair(io.v, k, va, vb, second, vec);
     if (io.u_out)
     {
-      io.u_out[k] = u;
-      io.v_out[k] = v;
+      st_pair(io.u_out, k, ua, ub, second, vec);
+      st_pair(io.v_out, k, va, vb, second, vec);
     }
-    part += (double)de;
+    part = (double)dea;
+    if (second) part += (double)deb;
   }
 
   if (MAINTAIN)
@@ -319,10 +375,10 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
 template <bool MAINTAIN, int F>
 __global__ void __launch_bounds__(FT_NT) k_vp_fwe(FweIo io, VpConst c, VpScalars *sc, double *partials)
 {
-  __shared__ FweSmem<false> sm;
+  __shared__ FweSmem sm;
   fwe_stage_cp_async(io, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm);
   __syncthreads();
-  fwe_compute<MAINTAIN, false, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
 /* The same step with the input tiles fetched by TMA.  A tile whose loads
@@ -333,7 +389,7 @@ template <bool MAINTAIN, int F>
 __global__ void __launch_bounds__(FT_NT)
     k_vp_fwe_tma(FweIo io, const __grid_constant__ FweMaps maps, VpConst c, VpScalars *sc, double *partials)
 {
-  __shared__ FweSmem<true> sm;
+  __shared__ FweSmem sm;
   if (!fwe_stage_tma(maps, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm))
   {
     if (threadIdx.x == 0) atomicOr(&sc->error, 1u);
@@ -347,7 +403,7 @@ __global__ void __launch_bounds__(FT_NT)
     }
     return;
   }
-  fwe_compute<MAINTAIN, true, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
 /* advection of one cell: s_new = bilinear(s1, (i - dt u, j - dt v)) */
