@@ -148,6 +148,59 @@ int hm_thermal_auto_bedrock_device(hm_context *ctx, float *z, int nx, int ny, co
                           opts, (float *)ws, (cudaStream_t)stream, true);
 }
 
+int hm_flow_simulation(hm_context *ctx, const float *z, int nx, int ny, float water_height, const float *depth_map,
+                       int iterations, float dt, int flux_diffusion, float flux_diffusion_strength,
+                       float dry_out_ratio, float *water_depth)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_flow_simulation: ctx is NULL");
+  int st = hm::flow_check_args(z, depth_map, water_depth, nx, ny, iterations, dt);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const size_t n = (size_t)nx * ny;
+  const size_t nbytes = n * sizeof(float);
+  const size_t total = 3 * align_up(nbytes, 256) + align_up(hm::flow_scratch_bytes(nx, ny), 256);
+  void        *ws = nullptr;
+  if ((st = hm::workspace(ctx, total, &ws))) return st;
+  Slab         sl{(char *)ws};
+  float       *dz = sl.take(n);
+  float       *dm = sl.take(n);
+  float       *dd = sl.take(n);
+  void        *scr = sl.take_bytes(hm::flow_scratch_bytes(nx, ny));
+  cudaStream_t s = ctx->stream;
+  HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
+  HM_CUDA_TRY(cudaMemcpyAsync(dm, depth_map, nbytes, cudaMemcpyHostToDevice, s));
+  st = hm::flow_simulation_core(dz, nx, ny, water_height, dm, iterations, dt, flux_diffusion, flux_diffusion_strength,
+                                dry_out_ratio, dd, scr, s);
+  if (st)
+  {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  HM_CUDA_TRY(cudaMemcpyAsync(water_depth, dd, nbytes, cudaMemcpyDeviceToHost, s));
+  unsigned dev_error = 0;
+  HM_CUDA_TRY(
+      cudaMemcpyAsync(&dev_error, hm::flow_error_word(scr, nx, ny), sizeof dev_error, cudaMemcpyDeviceToHost, s));
+  HM_CUDA_TRY(cudaStreamSynchronize(s));
+  if (dev_error) return hm::fail(HM_ERR_TIMEOUT, "hm_flow_simulation: tile loads timed out on the device");
+  return HM_OK;
+}
+
+int hm_flow_simulation_device(hm_context *ctx, const float *z, int nx, int ny, float water_height,
+                              const float *depth_map, int iterations, float dt, int flux_diffusion,
+                              float flux_diffusion_strength, float dry_out_ratio, float *water_depth, void *stream)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_flow_simulation_device: ctx is NULL");
+  int st = hm::flow_check_args(z, depth_map, water_depth, nx, ny, iterations, dt);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::flow_scratch_bytes(nx, ny), &ws))) return st;
+  return hm::flow_simulation_core(z, nx, ny, water_height, depth_map, iterations, dt, flux_diffusion,
+                                  flux_diffusion_strength, dry_out_ratio, water_depth, ws, (cudaStream_t)stream);
+}
+
 int hm_vpipes(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_params *params, const float *rain_map,
               float *water_depth, float *sediment, float *vel_u, float *vel_v)
 {

@@ -102,6 +102,7 @@ __device__ __forceinline__ void job_io(const BJob &J, int step, FweIo &io)
   if (io.u_out && !io.v_out) io.v_out = J.v;
   if (io.v_out && !io.u_out) io.u_out = J.u;
   io.vec = J.vec;
+  io.flow_only = 0;
 }
 
 template <bool TMAP, int BED>

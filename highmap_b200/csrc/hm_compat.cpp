@@ -6,6 +6,7 @@
  *   thermal          HighMap/src/erosion/thermal_gpu.cpp:17-96
  *   thermal_auto_bedrock  HighMap/src/erosion/thermal_gpu.cpp:98-152
  *   hydraulic_vpipes HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
+ *   flow_simulation  HighMap/src/hydrology/flow_simulation.cpp:26-110
  *   init_opencl      HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134
  * The reference functions return void and report problems only through
  * their logger; here a failed call leaves z untouched, prints the status
@@ -13,6 +14,7 @@
  * are resized to z's shape and overwritten, as `*p = d` does in the
  * reference.  Each thread uses its own context on device 0.
  */
+#include <algorithm>
 #include <cstdio>
 #include <memory>
 #include <string>
@@ -161,6 +163,33 @@ void thermal_auto_bedrock(Array &z, const Array *p_mask, const Array &talus, int
 void thermal_auto_bedrock(Array &z, float talus, int iterations, Array *p_deposition_map)
 {
   thermal_impl(z, nullptr, nullptr, talus, iterations, nullptr, p_deposition_map, true);
+}
+
+Array flow_simulation(const Array &z, float water_height, const Array &depth_map, int iterations, float dt,
+                      bool flux_diffusion, float flux_diffusion_strength, float dry_out_ratio)
+{
+  const char *fn = "hmap::gpu::flow_simulation";
+  Array       out;
+  shape_like(&out, z);
+  std::fill(out.vector.begin(), out.vector.end(), 0.f);
+  if (!same_shape(&depth_map, z) || z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
+  {
+    report(HM_ERR_INVALID_ARGUMENT, fn);
+    g_err += "arrays of different shapes";
+    return out;
+  }
+  hm_context *ctx = context();
+  if (!ctx)
+  {
+    report(HM_ERR_NO_DEVICE, fn);
+    return out;
+  }
+  std::vector<float> d(z.vector.size());
+  int st = hm_flow_simulation(ctx, z.vector.data(), z.shape.x, z.shape.y, water_height, depth_map.vector.data(),
+                              iterations, dt, flux_diffusion ? 1 : 0, flux_diffusion_strength, dry_out_ratio,
+                              d.data());
+  if (report(st, fn)) out.vector.swap(d);
+  return out;
 }
 
 void hydraulic_vpipes(Array &z, float water_height, bool maintain_water_volume, float evap_rate, int iterations,

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "hm_internal.h"
 #include "hm_reduce.cuh"
@@ -319,7 +320,7 @@ static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 /* tensor maps of one state copy; false if the grid or buffers do not meet
  * the TMA rules (row pitch and bases 16-byte aligned, boxes no larger than
  * the grid) */
-static bool fwe_maps(const VpFields &f, int nx, int ny, FweMaps *m)
+bool fwe_maps(const VpFields &f, int nx, int ny, FweMaps *m)
 {
   if (nx % 4 != 0 || nx < 40 || ny < FT_H2) return false;
   const float *all[7] = {f.z, f.d, f.s, f.fl, f.fr, f.ft, f.fb};
@@ -340,6 +341,7 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
   FweMaps      maps[2];
   const bool   tma = allow_tma && fwe_maps(A, nx, ny, &maps[0]) && fwe_maps(B, nx, ny, &maps[1]);
   FweIo        io;
+  memset(&io, 0, sizeof io);
   io.rain = rain;
   io.maintain = p.maintain_water_volume != 0;
   io.diffusion = p.flux_diffusion != 0;

@@ -23,6 +23,15 @@ int     vpipes_init(const VpFields &A, const float *rain, size_t n, float init_d
 /* device address of the solve's error word (bit 0: a tile's TMA loads
  * timed out and the tile was skipped) inside the scratch of vpipes_core */
 const unsigned *vpipes_error_word(const void *scratch_buf, int nx, int ny);
+/* flow_simulation (hm_flow.cu): device pointers, ordered on s; scratch of
+ * flow_scratch_bytes; water_depth receives the final depth */
+int             flow_check_args(const float *z, const float *depth_map, const float *out, int nx, int ny,
+                                int iterations, float dt);
+size_t          flow_scratch_bytes(int nx, int ny);
+int             flow_simulation_core(const float *z, int nx, int ny, float water_height, const float *depth_map,
+                                     int iterations, float dt, int flux_diffusion, float flux_diffusion_strength,
+                                     float dry_out_ratio, float *water_depth, void *scratch, cudaStream_t s);
+const unsigned *flow_error_word(const void *scratch, int nx, int ny);
 /* fp64 partial-sum slots vpipes_init needs */
 size_t  vpipes_init_partials();
 /* water-depth output: stored depth plus the top-up of the last step */

@@ -46,6 +46,8 @@ constexpr int FWE_DIFF = 1;      /* flux diffusion                     */
 constexpr int FWE_RAINMAP = 2;   /* a rain map scales rain and top-up   */
 constexpr int FWE_RAINSTEP = 4;  /* rain added every step               */
 constexpr int FWE_GENERIC = 8;   /* options read at run time            */
+constexpr int FWE_FLOWONLY = 16; /* flow and water passes only (flow_simulation): no
+                                  * erosion, terrain fixed, writes depth and fluxes */
 
 /* Shared-memory layout of the staged fields, one for both staging modes.
  * Every array row covers the 40 columns x0-4 .. x0+35 (a TMA box must start
@@ -79,6 +81,7 @@ struct FweIo
   int          maintain, diffusion, pl_one, kexp_one;
   float       *u_out, *v_out; /* last step: velocity outputs, nullable */
   int          vec;           /* nx even and every output 8-byte aligned: pair stores */
+  int          flow_only;     /* flow_simulation step (FWE_FLOWONLY kernels) */
 };
 
 /* tensor maps of the seven input fields of one step (TMA staging):
@@ -207,6 +210,7 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
 {
   static_assert(FT_TX == 32 && FT_TY == 16 && FT_NT == 256, "one cell pair per thread in the water pass");
   constexpr bool GEN = (F & FWE_GENERIC) != 0;
+  constexpr bool FLOW_ONLY = (F & FWE_FLOWONLY) != 0;
   const int      tid = threadIdx.x;
   const int      nx = c.nx, ny = c.ny;
   const int      x0 = bx * FT_TX, y0 = by * FT_TY;
@@ -326,41 +330,55 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
       water_cell<false>(c, d1.x, flc.x, frc.x, ftc.x, fbc.x, frw0, fle0, ftn.x, fbs.x, d2a, ua, va);
       water_cell<false>(c, d1.y, flc.y, frc.y, ftc.y, fbc.y, frc.x, fle1, ftn.y, fbs.y, d2b, ub, vb);
     }
-    const float2 zc = lds2(&sm.z[q][cc]), zn = lds2(&sm.z[q - 1][cc]), zs = lds2(&sm.z[q + 1][cc]);
-    const float  zw = sm.z[q][cc - 1], ze = sm.z[q][cc + 2];
-    const float2 s0 = lds2(&sm.s[l][cc]), sn = lds2(&sm.s[l - 1][cc]), ss = lds2(&sm.s[l + 1][cc]);
-    const float  sw = sm.s[l][cc - 1], se = sm.s[l][cc + 2];
-    float        zoa, soa, zob, sob;
-    if (kexp_one)
+    const size_t k = (size_t)gy * nx + gx;
+    const bool   vec = io.vec != 0;
+    if (FLOW_ONLY)
     {
-      erosion_cell<true>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
-      erosion_cell<true>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+      /* flow_simulation: the depth after the water pass is the next step's
+       * depth as it is (no evaporation, no erosion; the terrain is fixed) */
+      st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
+      st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
+      st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
+      st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
+      st_pair(io.out.d, k, d2a, d2b, second, vec);
+      (void)ua, (void)ub, (void)va, (void)vb;
     }
     else
     {
-      erosion_cell<false>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
-      erosion_cell<false>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+      const float2 zc = lds2(&sm.z[q][cc]), zn = lds2(&sm.z[q - 1][cc]), zs = lds2(&sm.z[q + 1][cc]);
+      const float  zw = sm.z[q][cc - 1], ze = sm.z[q][cc + 2];
+      const float2 s0 = lds2(&sm.s[l][cc]), sn = lds2(&sm.s[l - 1][cc]), ss = lds2(&sm.s[l + 1][cc]);
+      const float  sw = sm.s[l][cc - 1], se = sm.s[l][cc + 2];
+      float        zoa, soa, zob, sob;
+      if (kexp_one)
+      {
+        erosion_cell<true>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
+        erosion_cell<true>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+      }
+      else
+      {
+        erosion_cell<false>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
+        erosion_cell<false>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+      }
+      const float  dea = fmul(d2a, c.keep), deb = fmul(d2b, c.keep);
+      /* the cells' new fluxes, stored here where a warp writes whole rows */
+      st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
+      st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
+      st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
+      st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
+      st_pair(io.out.z, k, zoa, zob, second, vec);
+      st_pair(io.out.d, k, dea, deb, second, vec);
+      st_pair(io.s1, k, soa, sob, second, vec);
+      st_pair(io.u, k, ua, ub, second, vec);
+      st_pair(io.v, k, va, vb, second, vec);
+      if (io.u_out)
+      {
+        st_pair(io.u_out, k, ua, ub, second, vec);
+        st_pair(io.v_out, k, va, vb, second, vec);
+      }
+      part = (double)dea;
+      if (second) part += (double)deb;
     }
-    const size_t k = (size_t)gy * nx + gx;
-    const bool   vec = io.vec != 0;
-    const float  dea = fmul(d2a, c.keep), deb = fmul(d2b, c.keep);
-    /* the cells' new fluxes, stored here where a warp writes whole rows */
-    st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
-    st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
-    st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
-    st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
-    st_pair(io.out.z, k, zoa, zob, second, vec);
-    st_pair(io.out.d, k, dea, deb, second, vec);
-    st_pair(io.s1, k, soa, sob, second, vec);
-    st_pair(io.u, k, ua, ub, second, vec);
-    st_pair(io.v, k, va, vb, second, vec);
-    if (io.u_out)
-    {
-      st_pair(io.u_out, k, ua, ub, second, vec);
-      st_pair(io.v_out, k, va, vb, second, vec);
-    }
-    part = (double)dea;
-    if (second) part += (double)deb;
   }
 
   if (MAINTAIN)
@@ -425,9 +443,15 @@ int launch_fwe_cp_async(const FweIo &io, const VpConst &c, VpScalars *sc, double
 int launch_fwe_tma(const FweIo &io, const FweMaps &maps, const VpConst &c, VpScalars *sc, double *partials,
                    dim3 grid, cudaStream_t s);
 
+/* tensor maps of one state copy (hm_vpipes.cu); false if the grid or the
+ * buffers do not meet the TMA rules (row pitch and bases 16-byte aligned,
+ * boxes no larger than the grid) */
+bool fwe_maps(const VpFields &f, int nx, int ny, FweMaps *m);
+
 /* template flags of a step's options */
 inline int fwe_flags(const FweIo &io, const VpConst &c)
 {
+  if (io.flow_only) return FWE_FLOWONLY | (io.diffusion ? FWE_DIFF : 0);
   if (!io.pl_one || !io.kexp_one) return FWE_GENERIC;
   return (io.diffusion ? FWE_DIFF : 0) | (io.rain ? FWE_RAINMAP : 0) | (c.rps != 0.f ? FWE_RAINSTEP : 0);
 }
@@ -450,6 +474,8 @@ int fwe_dispatch(bool maintain, int f, Launch launch)
     HM_FWE_CASE(5)
     HM_FWE_CASE(6)
     HM_FWE_CASE(7)
+    HM_FWE_CASE(FWE_FLOWONLY)
+    HM_FWE_CASE(FWE_FLOWONLY | FWE_DIFF)
   default: return maintain ? launch(K<true, FWE_GENERIC>::fn()) : launch(K<false, FWE_GENERIC>::fn());
   }
 #undef HM_FWE_CASE

@@ -161,6 +161,23 @@ def thermal_auto_bedrock(z: np.ndarray, talus, iterations: int = 10, deposition_
                                             _ptr(deposition_map), C.byref(opts)))
 
 
+def flow_simulation(z: np.ndarray, water_height: float, depth_map: np.ndarray, iterations: int, dt: float = 0.5,
+                    flux_diffusion: bool = True, flux_diffusion_strength: float = 0.01, dry_out_ratio: float = 0.0,
+                    ctx: Context | None = None) -> np.ndarray:
+    """Water depth of the pipe model's flow and water passes on the fixed
+    terrain z (hmap::gpu::flow_simulation, flow_simulation.cpp:26-110)."""
+    _grid(z, "z")
+    shape = z.shape
+    ny, nx = shape
+    _grid(depth_map, "depth_map", shape)
+    out = np.empty_like(z)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_flow_simulation(ctx.handle, _ptr(z), nx, ny, C.c_float(water_height), _ptr(depth_map),
+                                       int(iterations), C.c_float(dt), int(bool(flux_diffusion)),
+                                       C.c_float(flux_diffusion_strength), C.c_float(dry_out_ratio), _ptr(out)))
+    return out
+
+
 def vpipes_params(**kw) -> VpipesParams:
     p = VpipesParams()
     L.lib().hm_vpipes_default_params(C.byref(p))
@@ -257,6 +274,18 @@ def thermal_auto_bedrock_device(z, talus, iterations: int = 10, deposition_map=N
                                                    _tptr(deposition_map, "deposition_map", z.shape),
                                                    _tptr(mask, "mask", z.shape), C.byref(opts),
                                                    _stream(stream)))
+
+
+def flow_simulation_device(z, water_height: float, depth_map, iterations: int, out, dt: float = 0.5,
+                           flux_diffusion: bool = True, flux_diffusion_strength: float = 0.01,
+                           dry_out_ratio: float = 0.0, ctx: Context | None = None, stream=None) -> None:
+    ny, nx = z.shape
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_flow_simulation_device(ctx.handle, _tptr(z, "z"), nx, ny, C.c_float(water_height),
+                                              _tptr(depth_map, "depth_map", z.shape), int(iterations),
+                                              C.c_float(dt), int(bool(flux_diffusion)),
+                                              C.c_float(flux_diffusion_strength), C.c_float(dry_out_ratio),
+                                              _tptr(out, "out", z.shape), _stream(stream)))
 
 
 def hydraulic_vpipes_device(z, params: VpipesParams | None = None, rain_map=None, water_depth=None,

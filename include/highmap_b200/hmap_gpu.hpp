@@ -5,6 +5,7 @@
  * HighMap/include/highmap/erosion.hpp:1206-1223 (hydraulic_vpipes),
  * :1784-1801 (thermal, three overloads), :1824-1838 (thermal_auto_bedrock, three
  * overloads)
+ * HighMap/include/highmap/hydrology/hydrology.hpp:875-882 (flow_simulation)
  * and HighMap/include/highmap/opencl/gpu_opencl.hpp:30 (init_opencl).
  * To use HighMap's own hmap::Array, include "highmap/array.hpp" first and
  * define HMAP_B200_EXTERNAL_ARRAY; otherwise this header brings in the
@@ -64,6 +65,17 @@ void thermal_auto_bedrock(Array &z,
                           float  talus,
                           int    iterations = 10,
                           Array *p_deposition_map = nullptr);
+
+/* HighMap/include/highmap/hydrology/hydrology.hpp:875-882; returns the
+ * water depth (an array of zeros of z's shape if the call fails) */
+Array flow_simulation(const Array &z,
+                      float        water_height,
+                      const Array &depth_map,
+                      int          iterations,
+                      float        dt = 0.5f,
+                      bool         flux_diffusion = true,
+                      float        flux_diffusion_strength = 0.01f,
+                      float        dry_out_ratio = 0.f);
 
 void hydraulic_vpipes(Array &z,
                       float  water_height = 1e-2f,

@@ -205,6 +205,47 @@ int hm_thermal_auto_bedrock_device(hm_context               *ctx,
                                    const hm_thermal_options *opts,
                                    void                     *stream);
 
+/* ---- flow simulation ---------------------------------------------------- */
+
+/* Replaces hmap::gpu::flow_simulation(const Array &z, float water_height,
+ * const Array &depth_map, int iterations, float dt, bool flux_diffusion,
+ * float flux_diffusion_strength, float dry_out_ratio)
+ * (HighMap/include/highmap/hydrology/hydrology.hpp:875-882,
+ *  HighMap/src/hydrology/flow_simulation.cpp:26-110): the flow and water
+ * passes of the pipe model (hydraulic_vpipes.cl:5-116) on the fixed terrain
+ * z, water starting at water_height * depth_map, `iterations` steps, then,
+ * if dry_out_ratio != 0, depth = max(0, depth - dry_out_ratio * max(depth))
+ * (water_depth.cpp:40-66).  z and depth_map: nx*ny in; water_depth: nx*ny
+ * out.  dt != 0, iterations >= 0. */
+int hm_flow_simulation(hm_context  *ctx,
+                       const float *z,
+                       int          nx,
+                       int          ny,
+                       float        water_height,
+                       const float *depth_map,
+                       int          iterations,
+                       float        dt,
+                       int          flux_diffusion,
+                       float        flux_diffusion_strength,
+                       float        dry_out_ratio,
+                       float       *water_depth);
+
+/* The same on device buffers, ordered on `stream` (a cudaStream_t, NULL =
+ * legacy default stream); returns without synchronising. */
+int hm_flow_simulation_device(hm_context  *ctx,
+                              const float *z,
+                              int          nx,
+                              int          ny,
+                              float        water_height,
+                              const float *depth_map,
+                              int          iterations,
+                              float        dt,
+                              int          flux_diffusion,
+                              float        flux_diffusion_strength,
+                              float        dry_out_ratio,
+                              float       *water_depth,
+                              void        *stream);
+
 /* No counterpart in the reference (which allocates its OpenCL buffers on
  * every call).  Thermal erosion on device buffers for callers that cannot
  * allocate device memory when they run it (an application whose own pool

@@ -122,6 +122,34 @@ int hmo_vpipes_f64(double                  *z,
                    double                  *vel_u,
                    double                  *vel_v);
 
+/* flow_simulation (HighMap/src/hydrology/flow_simulation.cpp:26-110):
+ * water depth after `iterations` flow and water passes of the pipe model
+ * (hydraulic_vpipes.cl:5-116, gravity, pipe area and length 1) on the fixed
+ * terrain z, starting from water_height * depth_map, then the optional
+ * dry-out (water_depth.cpp:40-66). */
+int hmo_flow_simulation_f32(const float *z,
+                            int          nx,
+                            int          ny,
+                            float        water_height,
+                            const float *depth_map,
+                            int          iterations,
+                            float        dt,
+                            int          flux_diffusion,
+                            float        flux_diffusion_strength,
+                            float        dry_out_ratio,
+                            float       *water_depth);
+int hmo_flow_simulation_f64(const double *z,
+                            int           nx,
+                            int           ny,
+                            double        water_height,
+                            const double *depth_map,
+                            int           iterations,
+                            double        dt,
+                            int           flux_diffusion,
+                            double        flux_diffusion_strength,
+                            double        dry_out_ratio,
+                            double       *water_depth);
+
 /* OpenCL linear sampler with mirrored-repeat addressing, evaluated on an
  * nx x ny texel grid at unnormalised coordinate (x, y) (texel centres at
  * k + 0.5).  Exposed for the tests of the advection pass. */

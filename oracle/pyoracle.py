@@ -146,6 +146,37 @@ def vpipes(z, params: VpipesParams, rain_map=None, dtype=np.float32):
     return (z, *outs)
 
 
+def flow_simulation(z, water_height, depth_map, iterations, dt=0.5, flux_diffusion=True,
+                    flux_diffusion_strength=0.01, dry_out_ratio=0.0, dtype=np.float32):
+    """Oracle flow_simulation; returns the water depth."""
+    z = _grid(z, dtype)
+    ny, nx = z.shape
+    dm = _grid(depth_map, dtype)
+    out = np.empty_like(z)
+    fn = _lib().hmo_flow_simulation_f32 if dtype == np.float32 else _lib().hmo_flow_simulation_f64
+    S = C.c_float if dtype == np.float32 else C.c_double
+    rc = fn(_p(z), nx, ny, S(water_height), _p(dm), int(iterations), S(dt), int(bool(flux_diffusion)),
+            S(flux_diffusion_strength), S(dry_out_ratio), _p(out))
+    if rc:
+        raise ValueError("oracle flow_simulation rejected its arguments (status %d)" % rc)
+    return out
+
+
+def ref_flow_simulation(z, water_height, depth_map, iterations, dt=0.5, flux_diffusion=True,
+                        flux_diffusion_strength=0.01, dry_out_ratio=0.0):
+    """The reference's flow and water pass kernel text driven as flow_simulation."""
+    z = _grid(z, np.float32)
+    ny, nx = z.shape
+    dm = _grid(depth_map, np.float32)
+    out = np.empty_like(z)
+    rc = _ref().ref_flow_simulation(_p(z), nx, ny, C.c_float(water_height), _p(dm), int(iterations),
+                                    C.c_float(dt), int(bool(flux_diffusion)), C.c_float(flux_diffusion_strength),
+                                    C.c_float(dry_out_ratio), _p(out))
+    if rc:
+        raise ValueError("ref flow_simulation rejected its arguments (status %d)" % rc)
+    return out
+
+
 def sample_linear_mirror(s, x, y):
     s = _grid(s, np.float32)
     ny, nx = s.shape

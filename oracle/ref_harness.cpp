@@ -11,6 +11,7 @@
  *   ref_thermal    : HighMap/src/erosion/thermal_gpu.cpp:17-96
  *   ref_thermal_auto_bedrock : thermal_gpu.cpp:98-130
  *   ref_vpipes     : HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
+ *   ref_flow_simulation : HighMap/src/hydrology/flow_simulation.cpp:26-110
  *
  * Work-items run as a host loop (OpenMP over rows).  The in-place thermal
  * kernels are given a private copy of the three rows around the work-item,
@@ -284,6 +285,74 @@ int ref_vpipes(float                   *z,
   if (sediment) std::memcpy(sediment, s.data(), n * sizeof(float));
   if (vel_u) std::memcpy(vel_u, u.data(), n * sizeof(float));
   if (vel_v) std::memcpy(vel_v, v.data(), n * sizeof(float));
+  return 0;
+}
+
+/* flow_simulation, HighMap/src/hydrology/flow_simulation.cpp:26-110, with
+ * the reference's flow and water pass kernels; dry-out as
+ * water_depth.cpp:40-66 after Array::max (methods.cpp) */
+int ref_flow_simulation(const float *z,
+                        int          nx,
+                        int          ny,
+                        float        water_height,
+                        const float *depth_map,
+                        int          iterations,
+                        float        dt,
+                        int          flux_diffusion,
+                        float        flux_diffusion_strength,
+                        float        dry_out_ratio,
+                        float       *water_depth)
+{
+  if (!z || !depth_map || !water_depth || nx < 1 || ny < 1 || iterations < 0) return 1;
+  const size_t       n = (size_t)nx * ny;
+  std::vector<float> zz(z, z + n), d(n), fl(n, 0.f), fr(n, 0.f), ft(n, 0.f), fb(n, 0.f), u(n), v(n);
+  std::vector<float> fl_o(n), fr_o(n), ft_o(n), fb_o(n), d_o(n);
+  for (size_t k = 0; k < n; k++) d[k] = water_height * depth_map[k];
+  auto img = [&](std::vector<float> &a) { return hmref::hm_image{a.data(), nx, ny}; };
+  for (int it = 0; it < iterations; it++)
+  {
+    hmref::hm_image iz = img(zz), i_fl = img(fl), i_fr = img(fr), i_ft = img(ft), i_fb = img(fb), i_d = img(d),
+                    o_fl = img(fl_o), o_fr = img(fr_o), o_ft = img(ft_o), o_fb = img(fb_o), o_d = img(d_o),
+                    i_u = img(u), i_v = img(v);
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < ny; j++)
+    {
+      hmref::g_gid1 = j;
+      for (int i = 0; i < nx; i++)
+      {
+        hmref::g_gid0 = i;
+        hmref::hydraulic_vpipes_flow_pass(&iz, &i_fl, &i_fr, &i_ft, &i_fb, &i_d, &o_fl, &o_fr, &o_ft, &o_fb, nx,
+                                          ny, dt, flux_diffusion ? 1 : 0, flux_diffusion_strength);
+      }
+    }
+    fl.swap(fl_o);
+    fr.swap(fr_o);
+    ft.swap(ft_o);
+    fb.swap(fb_o);
+    i_fl = img(fl), i_fr = img(fr), i_ft = img(ft), i_fb = img(fb);
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < ny; j++)
+    {
+      hmref::g_gid1 = j;
+      for (int i = 0; i < nx; i++)
+      {
+        hmref::g_gid0 = i;
+        hmref::hydraulic_vpipes_water_pass(&iz, &i_fl, &i_fr, &i_ft, &i_fb, &i_d, &o_d, &i_u, &i_v, nx, ny, dt,
+                                           water_height);
+      }
+    }
+    d.swap(d_o);
+  }
+  if (dry_out_ratio != 0.f)
+  {
+    const float dmax = *std::max_element(d.begin(), d.end());
+    for (size_t k = 0; k < n; k++)
+    {
+      d[k] -= dry_out_ratio * dmax;
+      d[k] = std::max(0.f, d[k]);
+    }
+  }
+  std::memcpy(water_depth, d.data(), n * sizeof(float));
   return 0;
 }
 

@@ -6,7 +6,7 @@
  * requested solver, writes the results as raw float32 for the test to
  * compare with the oracle.
  *
- * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes>
+ * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow>
  *        nx ny in.f32 out_prefix
  */
 #include <cstdio>
@@ -76,6 +76,13 @@ int main(int argc, char **argv)
     }
     write_raw(out + "_z.f32", z);
     write_raw(out + "_depo.f32", depo);
+  }
+  else if (mode == "flow")
+  {
+    hmap::Array depth_map(shape, 0.f);
+    for (size_t k = 0; k < z.vector.size(); k++) depth_map.vector[k] = 1.f - z.vector[k];
+    hmap::Array w = hmap::gpu::flow_simulation(z, 0.01f, depth_map, 50, 0.5f, true, 0.01f, 0.05f);
+    write_raw(out + "_water.f32", w);
   }
   else if (mode == "vpipes")
   {

@@ -2,11 +2,12 @@
 
 The reference has no golden vectors or known-answer tests for either
 solver, so these fixtures are outputs of the reference's OpenCL kernels
-(HighMap/src/gpu_opencl/kernels/thermal.cl, hydraulic_vpipes.cl) compiled
+(HighMap/src/gpu_opencl/kernels/thermal.cl, hydraulic_vpipes.cl; the latter's
+flow and water passes also drive flow_simulation) compiled
 for the CPU by oracle/build_oracle.py and driven by oracle/ref_harness.cpp
 (Jacobi form).  Run in a checkout where the reference tree is present:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation]
 
 Each .npz holds the inputs, the parameters and the outputs of one case.
 """
@@ -88,8 +89,27 @@ def vpipes_cases():
         _save(name, **arrays)
 
 
+def flow_simulation_cases():
+    nx, ny = 56, 44
+    z = fbm(nx, ny, seed=6)
+    depth_map = fbm(nx, ny, seed=7)
+    cases = {
+        # defaults of hydrology.hpp:875-882 (dt 0.5, flux diffusion 0.01, no dry-out)
+        "flow_simulation_defaults": dict(water_height=0.01, iterations=60, dt=0.5, flux_diffusion=True,
+                                         flux_diffusion_strength=0.01, dry_out_ratio=0.0),
+        "flow_simulation_dry_out": dict(water_height=0.02, iterations=40, dt=0.3, flux_diffusion=False,
+                                        flux_diffusion_strength=0.01, dry_out_ratio=0.1),
+    }
+    for name, kw in cases.items():
+        out = po.ref_flow_simulation(z, depth_map=depth_map, **kw)
+        _save(name, z=z, depth_map=depth_map, params=np.array(json.dumps(kw)), out_water=out)
+
+
+GROUPS = {"thermal": thermal_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases}
+
 if __name__ == "__main__":
     if not po.ref_available():
         sys.exit("the reference checker oracle/_ref/libhm_ref.so could not be built")
-    thermal_cases()
-    vpipes_cases()
+    # all groups, or the ones named on the command line
+    for g in sys.argv[1:] or list(GROUPS):
+        GROUPS[g]()

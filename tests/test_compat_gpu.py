@@ -80,6 +80,15 @@ def test_auto_bedrock_mask(gpu, example, tmp_path):
     assert np.array_equal(load("depo"), depo)
 
 
+def test_flow_simulation(gpu, example, tmp_path):
+    z = fbm(90, 70, seed=8)
+    load = _run(example, "flow", z, tmp_path)
+    dm = (np.float32(1) - z).astype(np.float32)
+    want = po.flow_simulation(z, 0.01, dm, 50, dt=0.5, flux_diffusion=True, flux_diffusion_strength=0.01,
+                              dry_out_ratio=0.05)
+    assert np.array_equal(load("water"), want)
+
+
 def test_vpipes(gpu, example, tmp_path):
     z = fbm(96, 64, seed=2)
     load = _run(example, "vpipes", z, tmp_path)

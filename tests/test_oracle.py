@@ -77,6 +77,14 @@ def test_vpipes_golden_volume_sum(name):
     assert np.abs(out[2] - g["out_sediment"]).max() <= 1e-4 * rng
 
 
+@pytest.mark.parametrize("name", ["flow_simulation_defaults", "flow_simulation_dry_out"])
+def test_flow_simulation_golden_bit_exact(name):
+    g = _load(name)
+    kw = json.loads(str(g["params"]))
+    out = po.flow_simulation(g["z"], depth_map=g["depth_map"], **kw)
+    assert np.array_equal(out, g["out_water"])
+
+
 def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))}
     assert {"thermal_uniform", "vpipes_defaults", "vpipes_rain_per_step"} <= names
@@ -105,6 +113,16 @@ def test_vpipes_matches_reference_text():
     b = po.ref_vpipes(z, p)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+@ref_only
+def test_flow_simulation_matches_reference_text():
+    z = fbm(61, 47, seed=22)
+    dm = fbm(61, 47, seed=23)
+    for kw in (dict(flux_diffusion=True, dry_out_ratio=0.0), dict(flux_diffusion=False, dry_out_ratio=0.2)):
+        a = po.flow_simulation(z, 0.015, dm, 35, dt=0.4, **kw)
+        b = po.ref_flow_simulation(z, 0.015, dm, 35, dt=0.4, **kw)
+        assert np.array_equal(a, b)
 
 
 def test_flat_field_unchanged():
