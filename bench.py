@@ -61,10 +61,11 @@ def _args():
     ap.add_argument("--size", type=int, default=N_SIDE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=["plain", "batch", "serve", "sweep"], default="plain",
+    ap.add_argument("--form", choices=["plain", "batch", "serve", "sweep", "extras"], default="plain",
                     help="plain: the drop-in headline; batch: 256 mixed jobs batched vs plain calls; "
                          "serve: Poisson request stream, continuous batching vs plain FIFO; "
-                         "sweep: thermal and vpipes at 1024^2..16384^2, 200 iterations, rates and errors")
+                         "sweep: thermal and vpipes at 1024^2..16384^2, 200 iterations, rates and errors; "
+                         "extras: thermal_auto_bedrock and flow_simulation at 4096^2 against their rooflines")
     ap.add_argument("--sizes", default="1024,2048,4096,8192,16384", help="grid sides of the sweep form")
     ap.add_argument("--jobs", type=int, default=256, help="jobs of the batch form")
     ap.add_argument("--requests", type=int, default=100, help="requests per rate of the serve form")
@@ -587,6 +588,84 @@ def run_sweep(a):
     return 0
 
 
+# ---------------------------------------------------------------- extras
+
+AUTO_BEDROCK_BYTES = 16.0  # z in and out, talus, z0 (the bedrock grid is folded away)
+FLOW_BYTES = 44.0          # z, depth and four fluxes in; depth and four fluxes out
+
+
+def run_extras(a):
+    """thermal_auto_bedrock (talus map, 500 iterations) and flow_simulation
+    (depth map, 1000 iterations, reference defaults) on the 4096^2 inputs:
+    device-timed cell-updates/s against the HBM roofline, and the
+    reference's kernel text on the host cores on a bounded sample (a few
+    iterations on the full grid, scaled)."""
+    import numpy as np
+    import torch
+
+    from highmap_b200 import gpu as G
+    from oracle import pyoracle as po
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if not G.init_opencl():
+        raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
+    ctx = G.Context(local)
+    dev = torch.device("cuda", local)
+    peak, peak_kind = _peaks()
+    n = a.size
+    cells = float(n) * n
+    z, talus, _ = _inputs(n)
+    from highmap_b200.inputs import fbm
+    depth_map = fbm(n, n, seed=4)
+    zd = torch.from_numpy(z).to(dev)
+    td = torch.from_numpy(talus).to(dev)
+    dm = torch.from_numpy(depth_map).to(dev)
+    w = torch.empty_like(zd)
+    zt = torch.empty_like(zd)
+    rows = {}
+    for name, iters, bpc, run in (
+            ("thermal_auto_bedrock", 500, AUTO_BEDROCK_BYTES,
+             lambda k: G.thermal_auto_bedrock_device(zt, td, k, ctx=ctx)),
+            ("flow_simulation", 1000, FLOW_BYTES,
+             lambda k: G.flow_simulation_device(zd, 0.01, dm, k, w, ctx=ctx))):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for rep in range(a.warmup + 1):
+            zt.copy_(zd)
+            torch.cuda.synchronize()
+            e0.record()
+            run(iters)
+            e1.record()
+            torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+        rate = cells * iters / t
+        rows[name] = {"iterations": iters, "cell_updates_per_s": rate, "bytes_per_cell_update": bpc,
+                      "gb_per_s": rate * bpc / 1e9, "frac": rate * bpc / 1e9 / peak, "peak": peak,
+                      "peak_kind": peak_kind}
+    # the reference's kernel text on the host cores, a few iterations
+    for name, fn in (("thermal_auto_bedrock", lambda k: po.ref_thermal_auto_bedrock(z, talus, k)),
+                     ("flow_simulation", lambda k: po.ref_flow_simulation(z, 0.01, depth_map, k))):
+        fn(1)
+        k = 8 if name == "thermal_auto_bedrock" else 4
+        t0 = time.perf_counter()
+        fn(k)
+        t = time.perf_counter() - t0
+        rows[name]["cpu_baseline"] = {"value": cells * k / t, "unit": "cell-updates/s", "cores": po.num_threads(),
+                                      "kind": "reference", "sample": "%d iterations on the full %dx%d inputs" %
+                                      (k, n, n)}
+    out = {"metric": "cell-updates/s at %d^2, thermal_auto_bedrock and flow_simulation" % n,
+           "value": rows["flow_simulation"]["cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic", "form": "extras",
+           "config": {"workload": "auto-bedrock thermal (talus map) x500, flow simulation (depth map fBm seed 4, "
+                                  "water height 0.01, dt 0.5, flux diffusion 0.01) x1000", "grid": [n, n]},
+           "rows": rows}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_form(a):
     """The batched or served form on one GPU (rank 0 of a torchrun launch
     runs it; the others exit)."""
@@ -628,6 +707,8 @@ def main():
         return run_reference(a)
     if a.form == "sweep":
         return run_sweep(a)
+    if a.form == "extras":
+        return run_extras(a)
     if a.form != "plain":
         return run_form(a)
     return run_ours(a)
