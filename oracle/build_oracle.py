@@ -4,7 +4,10 @@
   -ffp-contract=off so each float operation rounds once, OpenMP.
 * ``oracle/_ref/libhm_ref.so``: the reference's own kernel text
   (HighMap/src/gpu_opencl/kernels/_common_index.cl, thermal.cl,
-  hydraulic_vpipes.cl) compiled for the CPU behind ``ref_shim.h``, linked
+  hydraulic_vpipes.cl, thermal_ridge.cl, thermal_scree.cl, thermal_schott.cl,
+  thermal_olsen.cl, and the helper functions they call from
+  _common_math.cl and _common_rand.cl) compiled for the CPU behind
+  ``ref_shim.h``, linked
   with the host-driver restatement ``ref_harness.cpp``.  Built only where
   the reference tree is present (``HM_REFERENCE_ROOT``, default
   /root/reference); the kernel files are read in place and streamed to the
@@ -16,6 +19,7 @@ entry module calls the same functions).
 from __future__ import annotations
 
 import os
+import re
 import subprocess
 import sys
 
@@ -23,7 +27,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(HERE, "libhm_oracle.so")
 REF_SO = os.path.join(REF_DIR, "libhm_ref.so")
-KERNEL_FILES = ("_common_index.cl", "thermal.cl", "hydraulic_vpipes.cl")
+KERNEL_FILES = ("_common_index.cl", "thermal.cl", "hydraulic_vpipes.cl", "thermal_ridge.cl", "thermal_scree.cl",
+                "thermal_schott.cl", "thermal_olsen.cl")
+# helpers the sibling talus kernels call, taken function by function from
+# the shared kernel files (the rest of those files is not needed)
+HELPER_FUNCTIONS = (("_common_math.cl", ("almost_unit_identity", "smoothstep3")), ("_common_rand.cl", ("hash21u",)))
 CFLAGS = ["-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-march=x86-64-v2"]
 
 
@@ -64,19 +72,39 @@ def _kernel_text(path: str) -> str:
     return body.replace("(int2)(", "HM_INT2(").replace("(float2)(", "HM_FLOAT2(")
 
 
+def _function_text(path: str, name: str) -> str:
+    """The definition of one function of a kernel file: from the line that
+    declares it to its closing brace."""
+    text = _kernel_text(path)
+    m = re.search(r"^[A-Za-z_][\w ]*\b%s\s*\(" % re.escape(name), text, re.M)
+    if not m:
+        raise RuntimeError("%s not found in %s" % (name, path))
+    start = text.index("{", m.end())
+    depth = 0
+    for k in range(start, len(text)):
+        depth += {"{": 1, "}": -1}.get(text[k], 0)
+        if depth == 0:
+            return text[m.start():k + 1] + "\n"
+    raise RuntimeError("unbalanced braces after %s in %s" % (name, path))
+
+
 def build_ref(force: bool = False) -> str | None:
     """Compile the reference's kernel text into oracle/_ref/libhm_ref.so.
     Returns the path, or None when the reference tree is absent (the GPU
     box uses the library built here)."""
     kdir = os.path.join(reference_root(), "HighMap", "src", "gpu_opencl", "kernels")
     kfiles = [os.path.join(kdir, f) for f in KERNEL_FILES]
-    if not all(os.path.exists(k) for k in kfiles):
+    hfiles = [os.path.join(kdir, f) for f, _ in HELPER_FUNCTIONS]
+    if not all(os.path.exists(k) for k in kfiles + hfiles):
         return REF_SO if os.path.exists(REF_SO) else None
     own = [os.path.join(HERE, f) for f in ("ref_shim.h", "ref_harness.cpp", "hm_oracle.h")]
-    if not (force or _stale(REF_SO, kfiles + own)):
+    if not (force or _stale(REF_SO, kfiles + hfiles + own)):
         return REF_SO
     os.makedirs(REF_DIR, exist_ok=True)
     unit = '#include "ref_shim.h"\nnamespace hmref {\n'
+    for (f, names), path in zip(HELPER_FUNCTIONS, hfiles):
+        for name in names:
+            unit += '#line 1 "%s"\n' % path + _function_text(path, name)
     for k in kfiles:
         unit += '#line 2 "%s"\n' % k + _kernel_text(k)
     unit += "}\n"

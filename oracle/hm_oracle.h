@@ -122,6 +122,36 @@ int hmo_vpipes_f64(double                  *z,
                    double                  *vel_u,
                    double                  *vel_v);
 
+/* Sibling talus stencils (thermal_gpu.cpp:221-396; kernels thermal_ridge.cl,
+ * thermal_scree.cl, thermal_schott.cl, thermal_olsen.cl), Jacobi form.
+ * zmax: scree only; intensity: schott only; deposition_map: |z - z0| for
+ * ridge and schott, max(z - z0, 0) for scree, not written for olsen;
+ * mask: apply_with_mask blend, nullable. */
+#define HMO_RIDGE 0
+#define HMO_SCREE 1
+#define HMO_SCHOTT 2
+#define HMO_OLSEN 3
+int hmo_thermal_sibling_f32(int          rule,
+                            float       *z,
+                            int          nx,
+                            int          ny,
+                            const float *talus,
+                            const float *zmax,
+                            float        intensity,
+                            int          iterations,
+                            float       *deposition_map,
+                            const float *mask);
+int hmo_thermal_sibling_f64(int           rule,
+                            double       *z,
+                            int           nx,
+                            int           ny,
+                            const double *talus,
+                            const double *zmax,
+                            double        intensity,
+                            int           iterations,
+                            double       *deposition_map,
+                            const double *mask);
+
 /* flow_simulation (HighMap/src/hydrology/flow_simulation.cpp:26-110):
  * water depth after `iterations` flow and water passes of the pipe model
  * (hydraulic_vpipes.cl:5-116, gravity, pipe area and length 1) on the fixed

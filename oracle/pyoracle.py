@@ -146,6 +146,41 @@ def vpipes(z, params: VpipesParams, rain_map=None, dtype=np.float32):
     return (z, *outs)
 
 
+RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
+
+
+def thermal_sibling(rule, z, talus, iterations, zmax=None, intensity=0.2, deposition=False, mask=None,
+                    dtype=np.float32):
+    """Oracle ridge / scree / schott / olsen; returns (z, deposition map or None)."""
+    z = _grid(z, dtype).copy()
+    ny, nx = z.shape
+    talus = _grid(talus, dtype)
+    zmax = None if zmax is None else _grid(zmax, dtype)
+    mask = None if mask is None else _grid(mask, dtype)
+    depo = _out(z, deposition)
+    fn = _lib().hmo_thermal_sibling_f32 if dtype == np.float32 else _lib().hmo_thermal_sibling_f64
+    S = C.c_float if dtype == np.float32 else C.c_double
+    rc = fn(int(rule), _p(z), nx, ny, _p(talus), _p(zmax), S(intensity), int(iterations), _p(depo), _p(mask))
+    if rc:
+        raise ValueError("oracle thermal_sibling rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
+def ref_thermal_sibling(rule, z, talus, iterations, zmax=None, intensity=0.2, deposition=False, mask=None):
+    """The reference's thermal_ridge / _scree / _schott / _olsen kernel text, Jacobi form."""
+    z = _grid(z, np.float32).copy()
+    ny, nx = z.shape
+    talus = _grid(talus, np.float32)
+    zmax = None if zmax is None else _grid(zmax, np.float32)
+    mask = None if mask is None else _grid(mask, np.float32)
+    depo = _out(z, deposition)
+    rc = _ref().ref_thermal_sibling(int(rule), _p(z), nx, ny, _p(talus), _p(zmax), C.c_float(intensity),
+                                    int(iterations), _p(depo), _p(mask))
+    if rc:
+        raise ValueError("ref thermal_sibling rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
 def flow_simulation(z, water_height, depth_map, iterations, dt=0.5, flux_diffusion=True,
                     flux_diffusion_strength=0.01, dry_out_ratio=0.0, dtype=np.float32):
     """Oracle flow_simulation; returns the water depth."""

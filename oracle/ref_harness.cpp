@@ -12,6 +12,7 @@
  *   ref_thermal_auto_bedrock : thermal_gpu.cpp:98-130
  *   ref_vpipes     : HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
  *   ref_flow_simulation : HighMap/src/hydrology/flow_simulation.cpp:26-110
+ *   ref_thermal_sibling : HighMap/src/erosion/thermal_gpu.cpp:221-396
  *
  * Work-items run as a host loop (OpenMP over rows).  The in-place thermal
  * kernels are given a private copy of the three rows around the work-item,
@@ -51,6 +52,10 @@ void thermal_auto_bedrock(float       *z,
                           const int    nx,
                           const int    ny,
                           const int    it);
+void thermal_ridge(float *z, const float *talus, const int nx, const int ny);
+void thermal_scree(float *z, const float *talus, const float *zmax, const int nx, const int ny);
+void thermal_schott(float *z, const float *talus, const int nx, const int ny, const float intensity);
+void thermal_olsen(float *z, const float *talus, const int nx, const int ny);
 void hydraulic_vpipes_flow_pass(image2d_t, image2d_t, image2d_t, image2d_t, image2d_t, image2d_t,
                                 image2d_t, image2d_t, image2d_t, image2d_t, const int, const int,
                                 const float, const int, const float);
@@ -87,29 +92,31 @@ void extrapolate_borders(float *z, int ni, int nj)
  * Jacobi form: a is step t, b receives step t+1.  `launch(zw)` runs the
  * kernel for the current work-item with zw addressing the row window. */
 template <class Launch>
-void run_inplace(const float *a, float *b, float *bed, int nx, int ny, Launch launch)
+void run_inplace(const float *a, float *b, float *bed, int nx, int ny, Launch launch, int R = 1)
 {
   (void)bed;
 #pragma omp parallel
   {
-    std::vector<float> win((size_t)3 * nx, NAN);
+    /* rows j-R .. j+R; R = 1 for the 3 x 3 kernels, 3 for thermal_olsen
+     * (radius-2 reads, border cells copied from 3 rows in) */
+    std::vector<float> win((size_t)(2 * R + 1) * nx, NAN);
 #pragma omp for schedule(static)
     for (int j = 0; j < ny; j++)
     {
-      for (int r = -1; r <= 1; r++)
+      for (int r = -R; r <= R; r++)
         if (j + r >= 0 && j + r < ny)
-          std::memcpy(&win[(size_t)(r + 1) * nx], a + (size_t)(j + r) * nx, sizeof(float) * nx);
+          std::memcpy(&win[(size_t)(r + R) * nx], a + (size_t)(j + r) * nx, sizeof(float) * nx);
         else
-          std::fill(win.begin() + (size_t)(r + 1) * nx, win.begin() + (size_t)(r + 2) * nx, NAN);
-      /* zw[(j + r) * nx + i] == win[(r + 1) * nx + i] */
-      float *zw = win.data() - ((ptrdiff_t)j - 1) * (ptrdiff_t)nx;
+          std::fill(win.begin() + (size_t)(r + R) * nx, win.begin() + (size_t)(r + R + 1) * nx, NAN);
+      /* zw[(j + r) * nx + i] == win[(r + R) * nx + i] */
+      float *zw = win.data() - ((ptrdiff_t)j - R) * (ptrdiff_t)nx;
       hmref::g_gid1 = j;
       for (int i = 0; i < nx; i++)
       {
         hmref::g_gid0 = i;
         launch(zw);
-        b[(size_t)j * nx + i] = win[(size_t)nx + i];
-        win[(size_t)nx + i] = a[(size_t)j * nx + i];
+        b[(size_t)j * nx + i] = win[(size_t)R * nx + i];
+        win[(size_t)R * nx + i] = a[(size_t)j * nx + i];
       }
     }
   }
@@ -174,6 +181,53 @@ int ref_thermal_auto_bedrock(float       *z,
   if (deposition_map)
     for (size_t k = 0; k < n; k++) deposition_map[k] = std::max(a[k] - z0[k], 0.f);
   std::memcpy(z, a.data(), n * sizeof(float));
+  return 0;
+}
+
+/* thermal_gpu.cpp:221-396: thermal_ridge / _scree / _schott / _olsen
+ * (rule 0..3 as hmo_thermal_sibling), the masked overloads via
+ * apply_with_mask */
+int ref_thermal_sibling(int          rule,
+                        float       *z,
+                        int          nx,
+                        int          ny,
+                        const float *talus,
+                        const float *zmax,
+                        float        intensity,
+                        int          iterations,
+                        float       *deposition_map,
+                        const float *mask)
+{
+  if (!z || !talus || nx < 3 || ny < 3 || iterations < 0 || rule < 0 || rule > 3) return 1;
+  if (rule == 1 && !zmax) return 1;
+  if (rule == 3 && (nx < 7 || ny < 7)) return 1;
+  const size_t       n = (size_t)nx * ny;
+  std::vector<float> z0(z, z + n), a(z, z + n), b(n);
+  for (int it = 0; it < iterations; it++)
+  {
+    switch (rule)
+    {
+    case 0: run_inplace(a.data(), b.data(), nullptr, nx, ny, [&](float *zw) { hmref::thermal_ridge(zw, talus, nx, ny); }); break;
+    case 1:
+      run_inplace(a.data(), b.data(), nullptr, nx, ny, [&](float *zw) { hmref::thermal_scree(zw, talus, zmax, nx, ny); });
+      break;
+    case 2:
+      run_inplace(a.data(), b.data(), nullptr, nx, ny,
+                  [&](float *zw) { hmref::thermal_schott(zw, talus, nx, ny, intensity); });
+      break;
+    default:
+      run_inplace(a.data(), b.data(), nullptr, nx, ny, [&](float *zw) { hmref::thermal_olsen(zw, talus, nx, ny); }, 3);
+    }
+    std::swap(a, b);
+  }
+  extrapolate_borders(a.data(), nx, ny);
+  if (deposition_map && rule != 3)
+    for (size_t k = 0; k < n; k++)
+      deposition_map[k] = rule == 1 ? std::max(a[k] - z0[k], 0.f) : std::abs(a[k] - z0[k]);
+  if (mask)
+    for (size_t k = 0; k < n; k++) z[k] = z0[k] * (1.f - mask[k]) + a[k] * mask[k];
+  else
+    std::memcpy(z, a.data(), n * sizeof(float));
   return 0;
 }
 

@@ -75,7 +75,8 @@ using std::floor;
 using std::hypot;
 using std::pow;
 
-typedef int sampler_t;
+typedef int      sampler_t;
+typedef unsigned uint;
 
 struct hm_image
 {

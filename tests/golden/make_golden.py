@@ -2,12 +2,13 @@
 
 The reference has no golden vectors or known-answer tests for either
 solver, so these fixtures are outputs of the reference's OpenCL kernels
-(HighMap/src/gpu_opencl/kernels/thermal.cl, hydraulic_vpipes.cl; the latter's
-flow and water passes also drive flow_simulation) compiled
+(HighMap/src/gpu_opencl/kernels/thermal.cl, hydraulic_vpipes.cl, whose flow and
+water passes also drive flow_simulation, and the sibling talus kernels
+thermal_ridge.cl, thermal_scree.cl, thermal_schott.cl, thermal_olsen.cl) compiled
 for the CPU by oracle/build_oracle.py and driven by oracle/ref_harness.cpp
 (Jacobi form).  Run in a checkout where the reference tree is present:
 
-    python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation]
+    python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation] [siblings]
 
 Each .npz holds the inputs, the parameters and the outputs of one case.
 """
@@ -105,7 +106,28 @@ def flow_simulation_cases():
         _save(name, z=z, depth_map=depth_map, params=np.array(json.dumps(kw)), out_water=out)
 
 
-GROUPS = {"thermal": thermal_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases}
+def sibling_cases():
+    nx, ny = 52, 46
+    z = fbm(nx, ny, seed=8)
+    talus = ((0.3 + fbm(nx, ny, seed=9)) / nx).astype(np.float32)
+    zmax = (z + 0.2).astype(np.float32)
+    for rule, name, kw in ((po.RIDGE, "thermal_ridge", dict(iterations=30)),
+                           (po.SCREE, "thermal_scree", dict(iterations=30, zmax=zmax)),
+                           (po.SCHOTT, "thermal_schott", dict(iterations=30, intensity=0.2)),
+                           (po.OLSEN, "thermal_olsen", dict(iterations=30))):
+        zo, depo = po.ref_thermal_sibling(rule, z, talus, deposition=rule != po.OLSEN, **kw)
+        arrays = dict(z=z, talus=talus, iterations=np.int32(kw["iterations"]), out_z=zo)
+        if depo is not None:
+            arrays["out_depo"] = depo
+        if "zmax" in kw:
+            arrays["zmax"] = zmax
+        if "intensity" in kw:
+            arrays["intensity"] = np.float32(kw["intensity"])
+        _save(name, **arrays)
+
+
+GROUPS = {"thermal": thermal_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases,
+          "siblings": sibling_cases}
 
 if __name__ == "__main__":
     if not po.ref_available():

@@ -85,6 +85,21 @@ def test_flow_simulation_golden_bit_exact(name):
     assert np.array_equal(out, g["out_water"])
 
 
+@pytest.mark.parametrize("name,rule", [("thermal_ridge", po.RIDGE), ("thermal_scree", po.SCREE),
+                                       ("thermal_schott", po.SCHOTT), ("thermal_olsen", po.OLSEN)])
+def test_sibling_golden_bit_exact(name, rule):
+    g = _load(name)
+    kw = {}
+    if "zmax" in g:
+        kw["zmax"] = g["zmax"]
+    if "intensity" in g:
+        kw["intensity"] = float(g["intensity"])
+    z, depo = po.thermal_sibling(rule, g["z"], g["talus"], int(g["iterations"]), deposition="out_depo" in g, **kw)
+    assert np.array_equal(z, g["out_z"])
+    if "out_depo" in g:
+        assert np.array_equal(depo, g["out_depo"])
+
+
 def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))}
     assert {"thermal_uniform", "vpipes_defaults", "vpipes_rain_per_step"} <= names
@@ -123,6 +138,21 @@ def test_flow_simulation_matches_reference_text():
         a = po.flow_simulation(z, 0.015, dm, 35, dt=0.4, **kw)
         b = po.ref_flow_simulation(z, 0.015, dm, 35, dt=0.4, **kw)
         assert np.array_equal(a, b)
+
+
+@ref_only
+@pytest.mark.parametrize("rule", [0, 1, 2, 3])
+def test_siblings_match_reference_text(rule):
+    z = fbm(59, 41, seed=24)
+    talus = ((0.3 + fbm(59, 41, seed=25)) / 59).astype(np.float32)
+    zmax = (z + 0.25).astype(np.float32)
+    mask = fbm(59, 41, seed=26)
+    for m in (None, mask):
+        a, da = po.thermal_sibling(rule, z, talus, 20, zmax=zmax, intensity=0.15, deposition=True, mask=m)
+        b, db = po.ref_thermal_sibling(rule, z, talus, 20, zmax=zmax, intensity=0.15, deposition=True, mask=m)
+        assert np.array_equal(a, b)
+        if rule != po.OLSEN:
+            assert np.array_equal(da, db)
 
 
 def test_flat_field_unchanged():
