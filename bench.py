@@ -65,7 +65,7 @@ def _args():
                     help="plain: the drop-in headline; batch: 256 mixed jobs batched vs plain calls; "
                          "serve: Poisson request stream, continuous batching vs plain FIFO; "
                          "sweep: thermal and vpipes at 1024^2..16384^2, 200 iterations, rates and errors; "
-                         "extras: thermal_auto_bedrock and flow_simulation at 4096^2 against their rooflines")
+                         "extras: thermal_auto_bedrock, flow_simulation and the sibling talus stencils at 4096^2")
     ap.add_argument("--sizes", default="1024,2048,4096,8192,16384", help="grid sides of the sweep form")
     ap.add_argument("--jobs", type=int, default=256, help="jobs of the batch form")
     ap.add_argument("--requests", type=int, default=100, help="requests per rate of the serve form")
@@ -595,8 +595,10 @@ FLOW_BYTES = 44.0          # z, depth and four fluxes in; depth and four fluxes 
 
 
 def run_extras(a):
-    """thermal_auto_bedrock (talus map, 500 iterations) and flow_simulation
-    (depth map, 1000 iterations, reference defaults) on the 4096^2 inputs:
+    """thermal_auto_bedrock (talus map, 500 iterations), flow_simulation
+    (depth map, 1000 iterations, reference defaults) and the sibling talus
+    stencils ridge, scree (zmax = z + 0.25), schott and olsen (200
+    iterations each) on the 4096^2 inputs:
     device-timed cell-updates/s against the HBM roofline, and the
     reference's kernel text on the host cores on a bounded sample (a few
     iterations on the full grid, scaled)."""
@@ -644,18 +646,41 @@ def run_extras(a):
         rows[name] = {"iterations": iters, "cell_updates_per_s": rate, "bytes_per_cell_update": bpc,
                       "gb_per_s": rate * bpc / 1e9, "frac": rate * bpc / 1e9 / peak, "peak": peak,
                       "peak_kind": peak_kind}
+    # sibling talus stencils, 200 iterations each
+    zmax = (z + 0.25).astype(np.float32)
+    zmd = torch.from_numpy(zmax).to(dev)
+    sib = (("thermal_ridge", G.RIDGE, 12.0), ("thermal_scree", G.SCREE, 16.0), ("thermal_schott", G.SCHOTT, 12.0),
+           ("thermal_olsen", G.OLSEN, 12.0))
+    for name, rule, bpc in sib:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for rep in range(a.warmup + 1):
+            zt.copy_(zd)
+            torch.cuda.synchronize()
+            e0.record()
+            G.thermal_stencil_device(rule, zt, td, 200, zmax=zmd if rule == G.SCREE else None, ctx=ctx)
+            e1.record()
+            torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+        rate = cells * 200 / t
+        rows[name] = {"iterations": 200, "cell_updates_per_s": rate, "bytes_per_cell_update": bpc,
+                      "gb_per_s": rate * bpc / 1e9, "frac": rate * bpc / 1e9 / peak, "peak": peak,
+                      "peak_kind": peak_kind}
     # the reference's kernel text on the host cores, a few iterations
-    for name, fn in (("thermal_auto_bedrock", lambda k: po.ref_thermal_auto_bedrock(z, talus, k)),
-                     ("flow_simulation", lambda k: po.ref_flow_simulation(z, 0.01, depth_map, k))):
+    refs = [("thermal_auto_bedrock", lambda k: po.ref_thermal_auto_bedrock(z, talus, k)),
+            ("flow_simulation", lambda k: po.ref_flow_simulation(z, 0.01, depth_map, k))]
+    for name, rule, _ in sib:
+        refs.append((name, lambda k, rule=rule: po.ref_thermal_sibling(rule, z, talus, k, zmax=zmax)))
+    for name, fn in refs:
         fn(1)
-        k = 8 if name == "thermal_auto_bedrock" else 4
+        k = 4 if name in ("flow_simulation", "thermal_olsen") else 8
         t0 = time.perf_counter()
         fn(k)
         t = time.perf_counter() - t0
         rows[name]["cpu_baseline"] = {"value": cells * k / t, "unit": "cell-updates/s", "cores": po.num_threads(),
                                       "kind": "reference", "sample": "%d iterations on the full %dx%d inputs" %
                                       (k, n, n)}
-    out = {"metric": "cell-updates/s at %d^2, thermal_auto_bedrock and flow_simulation" % n,
+    out = {"metric": "cell-updates/s at %d^2, thermal_auto_bedrock, flow_simulation, sibling talus stencils" % n,
            "value": rows["flow_simulation"]["cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": 1,
            "higher_is_better": True, "dtype": "f32", "data": "synthetic", "form": "extras",
            "config": {"workload": "auto-bedrock thermal (talus map) x500, flow simulation (depth map fBm seed 4, "

@@ -148,6 +148,86 @@ int hm_thermal_auto_bedrock_device(hm_context *ctx, float *z, int nx, int ny, co
                           opts, (float *)ws, (cudaStream_t)stream, true);
 }
 
+namespace
+{
+int sibling_host(hm_context *ctx, int rule, float *z, int nx, int ny, const float *talus, const float *zmax,
+                 float intensity, int iterations, float *depo, const float *mask)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: ctx is NULL");
+  int st = hm::sibling_check_args(rule, z, nx, ny, talus, zmax, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const size_t n = (size_t)nx * ny;
+  const size_t nbytes = n * sizeof(float);
+  size_t       fields = 2 + (zmax ? 1 : 0) + (depo ? 1 : 0) + (mask ? 1 : 0);
+  size_t total = fields * align_up(nbytes, 256) + align_up(hm::thermal_scratch_floats(nx, ny, true) * 4, 256);
+  void  *ws = nullptr;
+  if ((st = hm::workspace(ctx, total, &ws))) return st;
+  Slab         sl{(char *)ws};
+  float       *dz = sl.take(n);
+  float       *dt = sl.take(n);
+  float       *dzm = zmax ? sl.take(n) : nullptr;
+  float       *dd = depo ? sl.take(n) : nullptr;
+  float       *dm = mask ? sl.take(n) : nullptr;
+  float       *scr = sl.take(hm::thermal_scratch_floats(nx, ny, true));
+  cudaStream_t s = ctx->stream;
+  HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
+  HM_CUDA_TRY(cudaMemcpyAsync(dt, talus, nbytes, cudaMemcpyHostToDevice, s));
+  if (dzm) HM_CUDA_TRY(cudaMemcpyAsync(dzm, zmax, nbytes, cudaMemcpyHostToDevice, s));
+  if (dm) HM_CUDA_TRY(cudaMemcpyAsync(dm, mask, nbytes, cudaMemcpyHostToDevice, s));
+  st = hm::sibling_core(ctx->device, rule, dz, nx, ny, dt, dzm, intensity, iterations, dd, dm, scr, s);
+  if (st)
+  {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  HM_CUDA_TRY(cudaMemcpyAsync(z, dz, nbytes, cudaMemcpyDeviceToHost, s));
+  if (dd) HM_CUDA_TRY(cudaMemcpyAsync(depo, dd, nbytes, cudaMemcpyDeviceToHost, s));
+  HM_CUDA_TRY(cudaStreamSynchronize(s));
+  return HM_OK;
+}
+} // namespace
+
+int hm_thermal_ridge(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
+                     float *deposition_map, const float *mask)
+{
+  return sibling_host(ctx, HM_RIDGE, z, nx, ny, talus, nullptr, 0.f, iterations, deposition_map, mask);
+}
+
+int hm_thermal_scree(hm_context *ctx, float *z, int nx, int ny, const float *talus, const float *zmax,
+                     int iterations, float *deposition_map, const float *mask)
+{
+  return sibling_host(ctx, HM_SCREE, z, nx, ny, talus, zmax, 0.f, iterations, deposition_map, mask);
+}
+
+int hm_thermal_schott(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
+                      float intensity, float *deposition_map, const float *mask)
+{
+  return sibling_host(ctx, HM_SCHOTT, z, nx, ny, talus, nullptr, intensity, iterations, deposition_map, mask);
+}
+
+int hm_thermal_olsen(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
+                     const float *mask)
+{
+  return sibling_host(ctx, HM_OLSEN, z, nx, ny, talus, nullptr, 0.f, iterations, nullptr, mask);
+}
+
+int hm_thermal_stencil_device(hm_context *ctx, int rule, float *z, int nx, int ny, const float *talus,
+                              const float *zmax, float intensity, int iterations, float *deposition_map,
+                              const float *mask, void *stream)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_stencil_device: ctx is NULL");
+  int st = hm::sibling_check_args(rule, z, nx, ny, talus, zmax, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::thermal_scratch_floats(nx, ny, true) * sizeof(float), &ws))) return st;
+  return hm::sibling_core(ctx->device, rule, z, nx, ny, talus, zmax, intensity, iterations, deposition_map, mask,
+                          (float *)ws, (cudaStream_t)stream);
+}
+
 int hm_flow_simulation(hm_context *ctx, const float *z, int nx, int ny, float water_height, const float *depth_map,
                        int iterations, float dt, int flux_diffusion, float flux_diffusion_strength,
                        float dry_out_ratio, float *water_depth)

@@ -7,6 +7,7 @@
  *   thermal_auto_bedrock  HighMap/src/erosion/thermal_gpu.cpp:98-152
  *   hydraulic_vpipes HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
  *   flow_simulation  HighMap/src/hydrology/flow_simulation.cpp:26-110
+ *   thermal_olsen / _ridge / _schott / _scree  HighMap/src/erosion/thermal_gpu.cpp:221-396
  *   init_opencl      HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134
  * The reference functions return void and report problems only through
  * their logger; here a failed call leaves z untouched, prints the status
@@ -163,6 +164,96 @@ void thermal_auto_bedrock(Array &z, const Array *p_mask, const Array &talus, int
 void thermal_auto_bedrock(Array &z, float talus, int iterations, Array *p_deposition_map)
 {
   thermal_impl(z, nullptr, nullptr, talus, iterations, nullptr, p_deposition_map, true);
+}
+
+namespace
+{
+void sibling_impl(int rule, const char *fn, Array &z, const Array *p_mask, const Array &talus, const Array *zmax,
+                  float intensity, int iterations, Array *p_deposition_map)
+{
+  if (!same_shape(&talus, z) || !same_shape(p_mask, z) || !same_shape(zmax, z) ||
+      z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
+  {
+    report(HM_ERR_INVALID_ARGUMENT, fn);
+    g_err += "arrays of different shapes";
+    return;
+  }
+  hm_context *ctx = context();
+  if (!ctx)
+  {
+    report(HM_ERR_NO_DEVICE, fn);
+    return;
+  }
+  std::vector<float> depo;
+  if (p_deposition_map) depo.resize(z.vector.size());
+  std::vector<float> zw(z.vector);
+  float             *dp = p_deposition_map ? depo.data() : nullptr;
+  const float       *mp = p_mask ? p_mask->vector.data() : nullptr;
+  int                st;
+  switch (rule)
+  {
+  case HM_RIDGE: st = hm_thermal_ridge(ctx, zw.data(), z.shape.x, z.shape.y, talus.vector.data(), iterations, dp, mp); break;
+  case HM_SCREE:
+    st = hm_thermal_scree(ctx, zw.data(), z.shape.x, z.shape.y, talus.vector.data(), zmax->vector.data(), iterations,
+                          dp, mp);
+    break;
+  case HM_SCHOTT:
+    st = hm_thermal_schott(ctx, zw.data(), z.shape.x, z.shape.y, talus.vector.data(), iterations, intensity, dp, mp);
+    break;
+  default: st = hm_thermal_olsen(ctx, zw.data(), z.shape.x, z.shape.y, talus.vector.data(), iterations, mp);
+  }
+  if (!report(st, fn)) return;
+  z.vector.swap(zw);
+  if (p_deposition_map)
+  {
+    shape_like(p_deposition_map, z);
+    p_deposition_map->vector.swap(depo);
+  }
+}
+} // namespace
+
+void thermal_olsen(Array &z, const Array &talus, int iterations)
+{
+  sibling_impl(HM_OLSEN, "hmap::gpu::thermal_olsen", z, nullptr, talus, nullptr, 0.f, iterations, nullptr);
+}
+
+void thermal_olsen(Array &z, const Array *p_mask, const Array &talus, int iterations)
+{
+  sibling_impl(HM_OLSEN, "hmap::gpu::thermal_olsen", z, p_mask, talus, nullptr, 0.f, iterations, nullptr);
+}
+
+void thermal_ridge(Array &z, const Array &talus, int iterations, Array *p_deposition_map)
+{
+  sibling_impl(HM_RIDGE, "hmap::gpu::thermal_ridge", z, nullptr, talus, nullptr, 0.f, iterations, p_deposition_map);
+}
+
+void thermal_ridge(Array &z, const Array *p_mask, const Array &talus, int iterations, Array *p_deposition_map)
+{
+  sibling_impl(HM_RIDGE, "hmap::gpu::thermal_ridge", z, p_mask, talus, nullptr, 0.f, iterations, p_deposition_map);
+}
+
+void thermal_schott(Array &z, const Array &talus, int iterations, float intensity, Array *p_deposition_map)
+{
+  sibling_impl(HM_SCHOTT, "hmap::gpu::thermal_schott", z, nullptr, talus, nullptr, intensity, iterations,
+               p_deposition_map);
+}
+
+void thermal_schott(Array &z, const Array *p_mask, const Array &talus, int iterations, float intensity,
+                    Array *p_deposition_map)
+{
+  sibling_impl(HM_SCHOTT, "hmap::gpu::thermal_schott", z, p_mask, talus, nullptr, intensity, iterations,
+               p_deposition_map);
+}
+
+void thermal_scree(Array &z, const Array &talus, const Array &zmax, int iterations, Array *p_deposition_map)
+{
+  sibling_impl(HM_SCREE, "hmap::gpu::thermal_scree", z, nullptr, talus, &zmax, 0.f, iterations, p_deposition_map);
+}
+
+void thermal_scree(Array &z, const Array *p_mask, const Array &talus, const Array &zmax, int iterations,
+                   Array *p_deposition_map)
+{
+  sibling_impl(HM_SCREE, "hmap::gpu::thermal_scree", z, p_mask, talus, &zmax, 0.f, iterations, p_deposition_map);
 }
 
 Array flow_simulation(const Array &z, float water_height, const Array &depth_map, int iterations, float dt,

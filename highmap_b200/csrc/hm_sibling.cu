@@ -1,0 +1,225 @@
+/*
+ * hm_sibling.cu - the sibling talus stencils of thermal erosion on sm_100a:
+ * thermal_ridge, thermal_scree, thermal_schott and thermal_olsen.
+ *
+ * Replaces the drivers of HighMap/src/erosion/thermal_gpu.cpp:221-396 and
+ * the in-place OpenCL kernels thermal_ridge.cl, thermal_scree.cl,
+ * thermal_schott.cl and thermal_olsen.cl (Jacobi form: every read sees
+ * step t, except a work-item's reads of its own cell, which see its own
+ * earlier writes).  After the steps, the thermal finish pass: border
+ * extrapolation, the deposition map (|z - z0| for ridge and schott,
+ * max(z - z0, 0) for scree, none for olsen) and the mask blend.
+ *
+ * Kernel: k_sibling_step, a 32 x 8 tile per CTA with a 2-cell halo of z in
+ * shared memory (olsen reads the neighbours of its neighbours), one cell
+ * per thread.  Arithmetic is explicitly rounded, one rounding per
+ * operation as the reference's fp32 text; division by the diagonal
+ * distance 1.414f is the exact Markstein form of hm_thermal_math.cuh.
+ */
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "hm_internal.h"
+#include "hm_thermal.h"
+#include "hm_thermal_math.cuh"
+
+namespace hm
+{
+
+namespace
+{
+
+constexpr int SB_TX = 32, SB_TY = 8, SB_H = 2; /* tile and halo */
+
+/* smoothstep3 and almost_unit_identity (_common_math.cl:20-23,111-114) */
+__device__ __forceinline__ float smoothstep3(float x)
+{
+  return __fmul_rn(__fmul_rn(x, x), __fsub_rn(3.f, __fmul_rn(2.f, x)));
+}
+__device__ __forceinline__ float almost_unit_identity(float x)
+{
+  return __fmul_rn(__fmul_rn(__fsub_rn(2.f, x), x), x);
+}
+__device__ __forceinline__ float clamp01(float x) { return fminf(fmaxf(x, 0.f), 1.f); }
+
+/* hash21u (_common_rand.cl:19-26) */
+__device__ __forceinline__ unsigned hash21u(unsigned x, unsigned y)
+{
+  unsigned h = x * 0x8da6b343u ^ y * 0xd8163841u;
+  h ^= h >> 13;
+  h *= 0x85ebca6bu;
+  h ^= h >> 16;
+  return h;
+}
+
+/* (val - other) / c for c = 1 or 1.414 */
+__device__ __forceinline__ float slope(float val, float other, bool diag)
+{
+  const float d = __fsub_rn(val, other);
+  return diag ? div_by_diag(d) : d;
+}
+
+template <int RULE>
+__global__ void __launch_bounds__(SB_TX *SB_TY)
+    k_sibling_step(const float *__restrict__ a,
+                   float *__restrict__ b,
+                   int nx,
+                   int ny,
+                   const float *__restrict__ talus,
+                   const float *__restrict__ zmax,
+                   float intensity)
+{
+  __shared__ float t[SB_TY + 2 * SB_H][SB_TX + 2 * SB_H];
+  const int x0 = blockIdx.x * SB_TX, y0 = blockIdx.y * SB_TY;
+  const int tid = threadIdx.y * SB_TX + threadIdx.x;
+  for (int e = tid; e < (SB_TY + 2 * SB_H) * (SB_TX + 2 * SB_H); e += SB_TX * SB_TY)
+  {
+    const int ly = e / (SB_TX + 2 * SB_H), lx = e - ly * (SB_TX + 2 * SB_H);
+    const int gx = min(max(x0 - SB_H + lx, 0), nx - 1), gy = min(max(y0 - SB_H + ly, 0), ny - 1);
+    t[ly][lx] = __ldg(a + (size_t)gy * nx + gx);
+  }
+  __syncthreads();
+  const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
+  if (i >= nx || j >= ny) return;
+  const size_t idx = (size_t)j * nx + i;
+  /* z at (i + dx, j + dy), |dx|, |dy| <= 2 */
+  auto zat = [&](int dx, int dy) -> float { return t[threadIdx.y + SB_H + dy][threadIdx.x + SB_H + dx]; };
+  const int di[8] = {-1, 0, 0, 1, -1, -1, 1, 1};
+  const int dj[8] = {0, 1, -1, 0, -1, 1, -1, 1};
+
+  if (RULE == HM_OLSEN)
+  {
+    /* apply_boundaries_buffer(z, i, j, nx, ny, 3), _common_index.cl:134-152 */
+    const int bw = 3;
+    if (!(i >= bw && i < nx - bw && j >= bw && j < ny - bw))
+    {
+      const int ci = min(max(i, bw), nx - bw - 1), cj = min(max(j, bw), ny - bw - 1);
+      b[idx] = __ldg(a + (size_t)cj * nx + ci);
+      return;
+    }
+    const float    c2 = 1.414213562f;
+    float          self = zat(0, 0);
+    const float    talus_ref = __ldg(talus + idx);
+    const unsigned shift = hash21u((unsigned)i, (unsigned)j) & 7u;
+    for (int k = 0; k < 8; ++k)
+    {
+      const int s = (k + (int)shift) & 7;
+      const int gx = di[s], gy = dj[s]; /* neighbour offset */
+      float     dsum = 0.f, dmax = 0.f, dz[8];
+#pragma unroll
+      for (int p = 0; p < 8; ++p)
+      {
+        const int   px = gx + di[p], py = gy + dj[p];
+        const float zp = (px == 0 && py == 0) ? self : zat(px, py);
+        dz[p] = __fsub_rn(zat(gx, gy), zp);
+        if (dz[p] > __fmul_rn(talus_ref, p < 4 ? 1.f : c2))
+        {
+          dsum = __fadd_rn(dsum, dz[p]);
+          dmax = fmaxf(dmax, dz[p]);
+        }
+      }
+      if (dmax > 0.f)
+      {
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+          if (gx + di[p] == 0 && gy + dj[p] == 0)
+          {
+            const float cp = p < 4 ? 1.f : c2;
+            const float amount =
+                __fdiv_rn(__fmul_rn(__fmul_rn(0.25f, __fsub_rn(dmax, __fmul_rn(talus_ref, cp))), dz[p]), dsum);
+            self = __fadd_rn(self, amount);
+          }
+      }
+    }
+    b[idx] = self;
+    return;
+  }
+
+  /* apply_boundaries, _common_index.cl:106-132: x edges first, then y */
+  if (i == 0) { b[idx] = zat(1, 0); return; }
+  if (i == nx - 1) { b[idx] = zat(-1, 0); return; }
+  if (j == 0) { b[idx] = zat(0, 1); return; }
+  if (j == ny - 1) { b[idx] = zat(0, -1); return; }
+  const float val = zat(0, 0);
+  const float tv = __ldg(talus + idx);
+  if (RULE == HM_SCHOTT)
+  {
+    int up = 0, down = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+    {
+      const float dz = slope(val, zat(di[k], dj[k]), k >= 4);
+      if (dz > tv)
+        down++;
+      else if (dz < -tv)
+        up++;
+    }
+    b[idx] = __fadd_rn(val, __fmul_rn(__fmul_rn(intensity, tv), (float)(up - down)));
+    return;
+  }
+  float sum = 0.f, slope_max = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; k++)
+  {
+    const float dz = slope(val, zat(di[k], dj[k]), k >= 4);
+    if (RULE == HM_RIDGE ? dz > 0.f : dz < 0.f) sum = __fadd_rn(sum, dz);
+    slope_max = fmaxf(slope_max, fabsf(dz));
+  }
+  float amp = smoothstep3(clamp01(__fsub_rn(1.f, __fdiv_rn(tv, slope_max))));
+  if (RULE == HM_SCREE)
+    amp = __fmul_rn(amp, almost_unit_identity(clamp01(__fsub_rn(1.f, __fdiv_rn(val, __ldg(zmax + idx))))));
+  b[idx] = __fadd_rn(val, __fmul_rn(__fmul_rn(0.25f, __fsub_rn(tv, __fmul_rn(0.5f, sum))), amp));
+}
+
+} // namespace
+
+int sibling_check_args(int rule, const float *z, int nx, int ny, const float *talus, const float *zmax, int iterations)
+{
+  if (rule < HM_RIDGE || rule > HM_OLSEN) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: unknown rule");
+  if (!z || !talus) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: z or talus is NULL");
+  if (rule == HM_SCREE && !zmax) return fail(HM_ERR_INVALID_ARGUMENT, "thermal_scree: zmax is NULL");
+  const int nmin = rule == HM_OLSEN ? 7 : 3;
+  if (nx < nmin || ny < nmin)
+    return fail(HM_ERR_INVALID_ARGUMENT, rule == HM_OLSEN ? "thermal_olsen: nx and ny must be >= 7"
+                                                          : "thermal stencil: nx and ny must be >= 3");
+  if ((long long)nx * (long long)ny > (1ll << 34))
+    return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: grid larger than 2^34 cells");
+  if (iterations < 0) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: iterations < 0");
+  return HM_OK;
+}
+
+int sibling_core(int device, int rule, float *z, int nx, int ny, const float *talus, const float *zmax,
+                 float intensity, int iterations, float *depo, const float *mask, float *scratch_buf,
+                 cudaStream_t s)
+{
+  const size_t n = (size_t)nx * ny;
+  float       *tmp = scratch_buf;
+  float       *z0 = scratch_buf + align_up(n, 64);
+  const bool   want_depo = depo && rule != HM_OLSEN;
+  if (want_depo || mask) HM_CUDA_TRY(cudaMemcpyAsync(z0, z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  const dim3   grid((nx + SB_TX - 1) / SB_TX, (ny + SB_TY - 1) / SB_TY), block(SB_TX, SB_TY);
+  const float *src = z;
+  float       *dst = tmp;
+  for (int it = 0; it < iterations; it++)
+  {
+    switch (rule)
+    {
+    case HM_RIDGE: k_sibling_step<HM_RIDGE><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity); break;
+    case HM_SCREE: k_sibling_step<HM_SCREE><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity); break;
+    case HM_SCHOTT:
+      k_sibling_step<HM_SCHOTT><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity);
+      break;
+    default: k_sibling_step<HM_OLSEN><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity);
+    }
+    HM_LAUNCH_CHECK("k_sibling_step");
+    const float *t = src;
+    src = dst;
+    dst = const_cast<float *>(t);
+  }
+  if (src != z) HM_CUDA_TRY(cudaMemcpyAsync(z, src, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  return thermal_finish(device, z, nx, ny, z0, want_depo ? depo : nullptr, mask, s, rule != HM_SCREE);
+}
+
+} // namespace hm

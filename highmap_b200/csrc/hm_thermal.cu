@@ -225,7 +225,8 @@ __global__ void k_thermal_final(float *__restrict__ z,
                                 const float *__restrict__ z0,
                                 float *__restrict__ depo,
                                 const float *__restrict__ mask,
-                                size_t n)
+                                size_t n,
+                                int depo_abs)
 {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
   {
@@ -234,7 +235,7 @@ __global__ void k_thermal_final(float *__restrict__ z,
     if (depo)
     {
       float dz = __fsub_rn(r, o);
-      depo[k] = dz > 0.f ? dz : 0.f;
+      depo[k] = depo_abs ? fabsf(dz) : (dz > 0.f ? dz : 0.f);
     }
     if (mask)
     {
@@ -304,16 +305,17 @@ static void step_dispatch(const float *a, float *b, int nx, int ny, const float 
 }
 
 /* post-processing of a finished thermal solve (z holds the last step):
- * border extrapolation, then the deposition map and the mask blend when
- * asked (z0 = the input heights) */
+ * border extrapolation, then the deposition map (max(z - z0, 0), or
+ * |z - z0| with depo_abs) and the mask blend when asked (z0 = the input
+ * heights) */
 int thermal_finish(int device, float *z, int nx, int ny, const float *z0, float *depo, const float *mask,
-                   cudaStream_t s)
+                   cudaStream_t s, bool depo_abs)
 {
   k_extrapolate<<<1, 1024, 0, s>>>(z, nx, ny);
   HM_LAUNCH_CHECK("k_extrapolate");
   if (depo || mask)
   {
-    k_thermal_final<<<num_sms(device) * 8, 256, 0, s>>>(z, z0, depo, mask, (size_t)nx * ny);
+    k_thermal_final<<<num_sms(device) * 8, 256, 0, s>>>(z, z0, depo, mask, (size_t)nx * ny, depo_abs ? 1 : 0);
     HM_LAUNCH_CHECK("k_thermal_final");
   }
   return HM_OK;

@@ -18,7 +18,15 @@ int    thermal_core(int device, float *z, int nx, int ny, const float *talus, fl
                     float *scratch_buf, cudaStream_t s, bool auto_bed = false);
 /* border extrapolation, deposition map and mask blend after the steps */
 int    thermal_finish(int device, float *z, int nx, int ny, const float *z0, float *depo, const float *mask,
-                      cudaStream_t s);
+                      cudaStream_t s, bool depo_abs = false);
+/* sibling talus stencils (hm_sibling.cu): rule HM_RIDGE .. HM_OLSEN; zmax
+ * for scree, intensity for schott; scratch of thermal_scratch_floats(nx,
+ * ny, true) floats */
+int    sibling_check_args(int rule, const float *z, int nx, int ny, const float *talus, const float *zmax,
+                          int iterations);
+int    sibling_core(int device, int rule, float *z, int nx, int ny, const float *talus, const float *zmax,
+                    float intensity, int iterations, float *depo, const float *mask, float *scratch_buf,
+                    cudaStream_t s);
 } // namespace hm
 
 #endif

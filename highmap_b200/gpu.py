@@ -161,6 +161,70 @@ def thermal_auto_bedrock(z: np.ndarray, talus, iterations: int = 10, deposition_
                                             _ptr(deposition_map), C.byref(opts)))
 
 
+RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
+
+
+def _sibling_host(z, talus, deposition_map, mask):
+    _grid(z, "z", writable=True)
+    shape = z.shape
+    ny, nx = shape
+    _grid(talus, "talus", shape)
+    if deposition_map is not None:
+        _grid(deposition_map, "deposition_map", shape, writable=True)
+    if mask is not None:
+        _grid(mask, "mask", shape)
+    return nx, ny
+
+
+def thermal_ridge(z: np.ndarray, talus: np.ndarray, iterations: int = 10, deposition_map: np.ndarray | None = None,
+                  mask: np.ndarray | None = None, ctx: Context | None = None) -> None:
+    """hmap::gpu::thermal_ridge (thermal_gpu.cpp:274-311), in place."""
+    nx, ny = _sibling_host(z, talus, deposition_map, mask)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_ridge(ctx.handle, _ptr(z), nx, ny, _ptr(talus), int(iterations), _ptr(deposition_map),
+                                     _ptr(mask)))
+
+
+def thermal_scree(z: np.ndarray, talus: np.ndarray, zmax: np.ndarray, iterations: int = 10,
+                  deposition_map: np.ndarray | None = None, mask: np.ndarray | None = None,
+                  ctx: Context | None = None) -> None:
+    """hmap::gpu::thermal_scree (thermal_gpu.cpp:355-396), in place."""
+    nx, ny = _sibling_host(z, talus, deposition_map, mask)
+    _grid(zmax, "zmax", z.shape)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_scree(ctx.handle, _ptr(z), nx, ny, _ptr(talus), _ptr(zmax), int(iterations),
+                                     _ptr(deposition_map), _ptr(mask)))
+
+
+def thermal_schott(z: np.ndarray, talus: np.ndarray, iterations: int = 10, intensity: float = 0.2,
+                   deposition_map: np.ndarray | None = None, mask: np.ndarray | None = None,
+                   ctx: Context | None = None) -> None:
+    """hmap::gpu::thermal_schott (thermal_gpu.cpp:313-353), in place."""
+    nx, ny = _sibling_host(z, talus, deposition_map, mask)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_schott(ctx.handle, _ptr(z), nx, ny, _ptr(talus), int(iterations),
+                                      C.c_float(intensity), _ptr(deposition_map), _ptr(mask)))
+
+
+def thermal_olsen(z: np.ndarray, talus: np.ndarray, iterations: int = 10, mask: np.ndarray | None = None,
+                  ctx: Context | None = None) -> None:
+    """hmap::gpu::thermal_olsen (thermal_gpu.cpp:221-247), in place."""
+    nx, ny = _sibling_host(z, talus, None, mask)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_olsen(ctx.handle, _ptr(z), nx, ny, _ptr(talus), int(iterations), _ptr(mask)))
+
+
+def thermal_stencil_device(rule: int, z, talus, iterations: int = 10, zmax=None, intensity: float = 0.2,
+                           deposition_map=None, mask=None, ctx: Context | None = None, stream=None) -> None:
+    ny, nx = z.shape
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_stencil_device(ctx.handle, int(rule), _tptr(z, "z"), nx, ny,
+                                              _tptr(talus, "talus", z.shape), _tptr(zmax, "zmax", z.shape),
+                                              C.c_float(intensity), int(iterations),
+                                              _tptr(deposition_map, "deposition_map", z.shape),
+                                              _tptr(mask, "mask", z.shape), _stream(stream)))
+
+
 def flow_simulation(z: np.ndarray, water_height: float, depth_map: np.ndarray, iterations: int, dt: float = 0.5,
                     flux_diffusion: bool = True, flux_diffusion_strength: float = 0.01, dry_out_ratio: float = 0.0,
                     ctx: Context | None = None) -> np.ndarray:

@@ -4,7 +4,7 @@
  * Source-compatible with the declarations of
  * HighMap/include/highmap/erosion.hpp:1206-1223 (hydraulic_vpipes),
  * :1784-1801 (thermal, three overloads), :1824-1838 (thermal_auto_bedrock, three
- * overloads)
+ * overloads), :1887-2028 (thermal_olsen, _ridge, _schott, _scree, two overloads each)
  * HighMap/include/highmap/hydrology/hydrology.hpp:875-882 (flow_simulation)
  * and HighMap/include/highmap/opencl/gpu_opencl.hpp:30 (init_opencl).
  * To use HighMap's own hmap::Array, include "highmap/array.hpp" first and
@@ -65,6 +65,48 @@ void thermal_auto_bedrock(Array &z,
                           float  talus,
                           int    iterations = 10,
                           Array *p_deposition_map = nullptr);
+
+/* sibling talus stencils, HighMap/include/highmap/erosion.hpp:1887-2028 */
+void thermal_olsen(Array &z, const Array &talus, int iterations);
+
+void thermal_olsen(Array &z, const Array *p_mask, const Array &talus, int iterations);
+
+void thermal_ridge(Array       &z,
+                   const Array &talus,
+                   int          iterations = 10,
+                   Array       *p_deposition_map = nullptr);
+
+void thermal_ridge(Array       &z,
+                   const Array *p_mask,
+                   const Array &talus,
+                   int          iterations = 10,
+                   Array       *p_deposition_map = nullptr);
+
+void thermal_schott(Array       &z,
+                    const Array &talus,
+                    int          iterations = 10,
+                    float        intensity = 0.2f,
+                    Array       *p_deposition_map = nullptr);
+
+void thermal_schott(Array       &z,
+                    const Array *p_mask,
+                    const Array &talus,
+                    int          iterations = 10,
+                    float        intensity = 0.2f,
+                    Array       *p_deposition_map = nullptr);
+
+void thermal_scree(Array       &z,
+                   const Array &talus,
+                   const Array &zmax,
+                   int          iterations = 10,
+                   Array       *p_deposition_map = nullptr);
+
+void thermal_scree(Array       &z,
+                   const Array *p_mask,
+                   const Array &talus,
+                   const Array &zmax,
+                   int          iterations = 10,
+                   Array       *p_deposition_map = nullptr);
 
 /* HighMap/include/highmap/hydrology/hydrology.hpp:875-882; returns the
  * water depth (an array of zeros of z's shape if the call fails) */

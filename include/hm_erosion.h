@@ -205,6 +205,84 @@ int hm_thermal_auto_bedrock_device(hm_context               *ctx,
                                    const hm_thermal_options *opts,
                                    void                     *stream);
 
+/* ---- sibling talus stencils ---------------------------------------------- */
+
+/* Rules of hm_thermal_stencil_device. */
+#define HM_RIDGE 0
+#define HM_SCREE 1
+#define HM_SCHOTT 2
+#define HM_OLSEN 3
+
+/* Replaces hmap::gpu::thermal_ridge(Array &z, const Array &talus,
+ * int iterations, Array *p_deposition_map) and its masked overload
+ * (HighMap/include/highmap/erosion.hpp:1953-1962,
+ *  HighMap/src/erosion/thermal_gpu.cpp:274-311, kernel thermal_ridge.cl).
+ * Then extrapolate_borders, deposition map |z_out - z_in|, and with a mask
+ * z = lerp(z, result, mask).  mask and deposition_map are nullable. */
+int hm_thermal_ridge(hm_context  *ctx,
+                     float       *z,
+                     int          nx,
+                     int          ny,
+                     const float *talus,
+                     int          iterations,
+                     float       *deposition_map,
+                     const float *mask);
+
+/* Replaces hmap::gpu::thermal_scree(Array &z, const Array &talus,
+ * const Array &zmax, int iterations, Array *p_deposition_map) and its
+ * masked overload (erosion.hpp:2017-2028, thermal_gpu.cpp:355-396, kernel
+ * thermal_scree.cl).  Deposition map max(z_out - z_in, 0). */
+int hm_thermal_scree(hm_context  *ctx,
+                     float       *z,
+                     int          nx,
+                     int          ny,
+                     const float *talus,
+                     const float *zmax,
+                     int          iterations,
+                     float       *deposition_map,
+                     const float *mask);
+
+/* Replaces hmap::gpu::thermal_schott(Array &z, const Array &talus,
+ * int iterations, float intensity, Array *p_deposition_map) and its masked
+ * overload (erosion.hpp:1985-1996, thermal_gpu.cpp:313-353, kernel
+ * thermal_schott.cl).  Deposition map |z_out - z_in|. */
+int hm_thermal_schott(hm_context  *ctx,
+                      float       *z,
+                      int          nx,
+                      int          ny,
+                      const float *talus,
+                      int          iterations,
+                      float        intensity,
+                      float       *deposition_map,
+                      const float *mask);
+
+/* Replaces hmap::gpu::thermal_olsen(Array &z, const Array &talus,
+ * int iterations) and its masked overload (erosion.hpp:1887-1892,
+ * thermal_gpu.cpp:221-247, kernel thermal_olsen.cl).  nx, ny >= 7. */
+int hm_thermal_olsen(hm_context  *ctx,
+                     float       *z,
+                     int          nx,
+                     int          ny,
+                     const float *talus,
+                     int          iterations,
+                     const float *mask);
+
+/* The four on device buffers, ordered on `stream`: rule HM_RIDGE ..
+ * HM_OLSEN; zmax (scree) and intensity (schott) as above; deposition_map
+ * (not written for olsen) and mask nullable. */
+int hm_thermal_stencil_device(hm_context  *ctx,
+                              int          rule,
+                              float       *z,
+                              int          nx,
+                              int          ny,
+                              const float *talus,
+                              const float *zmax,
+                              float        intensity,
+                              int          iterations,
+                              float       *deposition_map,
+                              const float *mask,
+                              void        *stream);
+
 /* ---- flow simulation ---------------------------------------------------- */
 
 /* Replaces hmap::gpu::flow_simulation(const Array &z, float water_height,

@@ -6,7 +6,7 @@
  * requested solver, writes the results as raw float32 for the test to
  * compare with the oracle.
  *
- * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow>
+ * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen>
  *        nx ny in.f32 out_prefix
  */
 #include <cstdio>
@@ -83,6 +83,17 @@ int main(int argc, char **argv)
     for (size_t k = 0; k < z.vector.size(); k++) depth_map.vector[k] = 1.f - z.vector[k];
     hmap::Array w = hmap::gpu::flow_simulation(z, 0.01f, depth_map, 50, 0.5f, true, 0.01f, 0.05f);
     write_raw(out + "_water.f32", w);
+  }
+  else if (mode == "ridge" || mode == "scree" || mode == "schott" || mode == "olsen")
+  {
+    hmap::Array talus(shape, 0.5f / shape.x), zmax(shape), mask(shape, 0.6f), depo;
+    for (size_t k = 0; k < z.vector.size(); k++) zmax.vector[k] = z.vector[k] + 0.2f;
+    if (mode == "ridge") hmap::gpu::thermal_ridge(z, talus, 20, &depo);
+    else if (mode == "scree") hmap::gpu::thermal_scree(z, &mask, talus, zmax, 20, &depo);
+    else if (mode == "schott") hmap::gpu::thermal_schott(z, talus, 20, 0.2f, &depo);
+    else hmap::gpu::thermal_olsen(z, &mask, talus, 20);
+    write_raw(out + "_z.f32", z);
+    if (mode != "olsen") write_raw(out + "_depo.f32", depo);
   }
   else if (mode == "vpipes")
   {

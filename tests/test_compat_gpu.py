@@ -89,6 +89,21 @@ def test_flow_simulation(gpu, example, tmp_path):
     assert np.array_equal(load("water"), want)
 
 
+@pytest.mark.parametrize("mode", ["ridge", "scree", "schott", "olsen"])
+def test_sibling_stencils(gpu, example, tmp_path, mode):
+    z = fbm(72, 60, seed=9)
+    load = _run(example, mode, z, tmp_path)
+    talus = np.full_like(z, np.float32(0.5) / np.float32(72))
+    zmax = (z + np.float32(0.2)).astype(np.float32)
+    mask = np.full_like(z, 0.6) if mode in ("scree", "olsen") else None
+    rule = {"ridge": po.RIDGE, "scree": po.SCREE, "schott": po.SCHOTT, "olsen": po.OLSEN}[mode]
+    want, depo = po.thermal_sibling(rule, z, talus, 20, zmax=zmax, intensity=0.2, deposition=mode != "olsen",
+                                    mask=mask)
+    assert np.array_equal(load("z"), want)
+    if mode != "olsen":
+        assert np.array_equal(load("depo"), depo)
+
+
 def test_vpipes(gpu, example, tmp_path):
     z = fbm(96, 64, seed=2)
     load = _run(example, "vpipes", z, tmp_path)
