@@ -113,12 +113,12 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
   {
     const int wx = bx * 2 * TH_W + (threadIdx.x >> 5) * 64;
     if (wx < J.nx) /* whole warp */
-      thermal_sweep2_warp<TMAP, BED>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
+      thermal_sweep2_warp<TMAP, TalusExchange<BED>>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
     return;
   }
   const int wx = bx * TH_W + (threadIdx.x >> 5) * 32;
   if (wx < J.nx) /* whole warp */
-    thermal_sweep_warp<TMAP, BED>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
+    thermal_sweep_warp<TMAP, TalusExchange<BED>>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
 }
 
 /* One round, first launch: every active vpipes fwe tile and thermal tile,

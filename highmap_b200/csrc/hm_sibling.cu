@@ -24,6 +24,7 @@
 #include "hm_internal.h"
 #include "hm_thermal.h"
 #include "hm_thermal_math.cuh"
+#include "hm_thermal_sweep.cuh"
 
 namespace hm
 {
@@ -61,6 +62,72 @@ __device__ __forceinline__ float slope(float val, float other, bool diag)
   return diag ? div_by_diag(d) : d;
 }
 
+/* The 3 x 3 rules as cell rules of the warp sweeps (hm_thermal_sweep.cuh);
+ * neighbours in the reference's loop order w, s, n, e, nw, sw, ne, se
+ * (HMAP_DI / HMAP_DJ), distance 1.414 for the diagonals. */
+template <int RULE>
+struct SiblingRule
+{
+  static constexpr bool EXTRA = RULE == HM_SCREE; /* zmax */
+  __device__ static __forceinline__ float cell(float c, float w, float s, float n, float e, float nw, float sw,
+                                               float ne, float se, float t, float zmax, bool, float intensity)
+  {
+    const float z8[8] = {w, s, n, e, nw, sw, ne, se};
+    if (RULE == HM_SCHOTT)
+    {
+      int up = 0, down = 0;
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+      {
+        const float dz = slope(c, z8[k], k >= 4);
+        if (dz > t)
+          down++;
+        else if (dz < -t)
+          up++;
+      }
+      return __fadd_rn(c, __fmul_rn(__fmul_rn(intensity, t), (float)(up - down)));
+    }
+    float sum = 0.f, slope_max = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+    {
+      const float dz = slope(c, z8[k], k >= 4);
+      if (RULE == HM_RIDGE ? dz > 0.f : dz < 0.f) sum = __fadd_rn(sum, dz);
+      slope_max = fmaxf(slope_max, fabsf(dz));
+    }
+    float amp = smoothstep3(clamp01(__fsub_rn(1.f, __fdiv_rn(t, slope_max))));
+    if (RULE == HM_SCREE) amp = __fmul_rn(amp, almost_unit_identity(clamp01(__fsub_rn(1.f, __fdiv_rn(c, zmax)))));
+    return __fadd_rn(c, __fmul_rn(__fmul_rn(0.25f, __fsub_rn(t, __fmul_rn(0.5f, sum))), amp));
+  }
+};
+
+constexpr int SS_NT = 256, SS2_NT = 128, SS_H = 16; /* as the thermal sweeps */
+
+template <int RULE>
+__global__ void __launch_bounds__(SS_NT)
+    k_sibling_sweep(const float *__restrict__ a, float *__restrict__ b, int nx, int ny, const float *__restrict__ talus,
+                    const float *__restrict__ zmax, float intensity)
+{
+  const int wx = (blockIdx.x * (SS_NT / 32) + (threadIdx.x >> 5)) * 32;
+  if (wx >= nx) return; /* the whole warp */
+  const int y0 = blockIdx.y * SS_H;
+  thermal_sweep_warp<true, SiblingRule<RULE>>(a, b, nx, ny, talus, 0.f, zmax, 0, wx, y0, min(ny, y0 + SS_H),
+                                              intensity);
+}
+
+template <int RULE>
+__global__ void __launch_bounds__(SS2_NT)
+    k_sibling_sweep2(const float *__restrict__ a, float *__restrict__ b, int nx, int ny,
+                     const float *__restrict__ talus, const float *__restrict__ zmax, float intensity)
+{
+  const int wx = (blockIdx.x * (SS2_NT / 32) + (threadIdx.x >> 5)) * 64;
+  if (wx >= nx) return; /* the whole warp */
+  const int y0 = blockIdx.y * SS_H;
+  thermal_sweep2_warp<true, SiblingRule<RULE>>(a, b, nx, ny, talus, 0.f, zmax, 0, wx, y0, min(ny, y0 + SS_H),
+                                               intensity);
+}
+
+/* thermal_olsen: radius-2 reads, a shared-memory tile per CTA */
 template <int RULE>
 __global__ void __launch_bounds__(SB_TX *SB_TY)
     k_sibling_step(const float *__restrict__ a,
@@ -103,10 +170,14 @@ __global__ void __launch_bounds__(SB_TX *SB_TY)
     float          self = zat(0, 0);
     const float    talus_ref = __ldg(talus + idx);
     const unsigned shift = hash21u((unsigned)i, (unsigned)j) & 7u;
+    /* HMAP_DI / HMAP_DJ + 1 packed two bits per direction, so a direction
+     * chosen at run time is decoded with shifts instead of an indexed
+     * local array */
+    constexpr unsigned DI1 = 0xA094u, DJ1 = 0x8849u;
     for (int k = 0; k < 8; ++k)
     {
       const int s = (k + (int)shift) & 7;
-      const int gx = di[s], gy = dj[s]; /* neighbour offset */
+      const int gx = (int)((DI1 >> (2 * s)) & 3u) - 1, gy = (int)((DJ1 >> (2 * s)) & 3u) - 1; /* neighbour offset */
       float     dsum = 0.f, dmax = 0.f, dz[8];
 #pragma unroll
       for (int p = 0; p < 8; ++p)
@@ -202,17 +273,23 @@ int sibling_core(int device, int rule, float *z, int nx, int ny, const float *ta
   const dim3   grid((nx + SB_TX - 1) / SB_TX, (ny + SB_TY - 1) / SB_TY), block(SB_TX, SB_TY);
   const float *src = z;
   float       *dst = tmp;
+  auto al8 = [](const void *p) { return ((uintptr_t)p & 7u) == 0; };
+  const bool pairs = nx % 2 == 0 && al8(z) && al8(tmp) && al8(talus) && (rule != HM_SCREE || al8(zmax));
+  const dim3 g2((nx + 2 * SS2_NT - 1) / (2 * SS2_NT), (ny + SS_H - 1) / SS_H);
+  const dim3 g1((nx + SS_NT - 1) / SS_NT, (ny + SS_H - 1) / SS_H);
   for (int it = 0; it < iterations; it++)
   {
+#define HM_SIB_SWEEP(R)                                                                                                \
+  if (pairs) k_sibling_sweep2<R><<<g2, SS2_NT, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity);                       \
+  else k_sibling_sweep<R><<<g1, SS_NT, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity);
     switch (rule)
     {
-    case HM_RIDGE: k_sibling_step<HM_RIDGE><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity); break;
-    case HM_SCREE: k_sibling_step<HM_SCREE><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity); break;
-    case HM_SCHOTT:
-      k_sibling_step<HM_SCHOTT><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity);
-      break;
+    case HM_RIDGE: HM_SIB_SWEEP(HM_RIDGE) break;
+    case HM_SCREE: HM_SIB_SWEEP(HM_SCREE) break;
+    case HM_SCHOTT: HM_SIB_SWEEP(HM_SCHOTT) break;
     default: k_sibling_step<HM_OLSEN><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity);
     }
+#undef HM_SIB_SWEEP
     HM_LAUNCH_CHECK("k_sibling_step");
     const float *t = src;
     src = dst;

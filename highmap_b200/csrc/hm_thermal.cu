@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(SW_NT)
   const int wx = (blockIdx.x * (SW_NT / 32) + (threadIdx.x >> 5)) * 32;
   if (wx >= nx) return; /* the whole warp: no CTA barrier in this kernel */
   const int y0 = blockIdx.y * SW_H;
-  thermal_sweep_warp<TMAP, BED>(a, b, nx, ny, talus, talus_value, bedrock, first, wx, y0, min(ny, y0 + SW_H));
+  thermal_sweep_warp<TMAP, TalusExchange<BED>>(a, b, nx, ny, talus, talus_value, bedrock, first, wx, y0, min(ny, y0 + SW_H));
 }
 
 /* One Jacobi step, a warp per 64 columns (two per lane) and SW_H rows
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(S2_NT)
   const int wx = (blockIdx.x * (S2_NT / 32) + (threadIdx.x >> 5)) * 64;
   if (wx >= nx) return; /* the whole warp: no CTA barrier in this kernel */
   const int y0 = blockIdx.y * SW_H;
-  thermal_sweep2_warp<TMAP, BED>(a, b, nx, ny, talus, talus_value, bedrock, first, wx, y0, min(ny, y0 + SW_H));
+  thermal_sweep2_warp<TMAP, TalusExchange<BED>>(a, b, nx, ny, talus, talus_value, bedrock, first, wx, y0, min(ny, y0 + SW_H));
 }
 
 /* ------------------------------------------------------------------ */

@@ -23,9 +23,25 @@ namespace hm
 
 constexpr int SW_P = 8; /* rows whose loads are issued together */
 
+/* Cell rules of the sweeps: R::cell(c, w, s, n, e, nw, sw, ne, se, talus,
+ * extra, first, param) is the new value of an interior cell from its 3 x 3
+ * neighbourhood (named by position: w = (i-1, j), s = (i, j+1), n =
+ * (i, j-1), ...), its talus, the value of the optional per-cell grid
+ * `extra` (R::EXTRA), the first-step flag and a scalar parameter. */
+template <int BED>
+struct TalusExchange
+{
+  static constexpr bool EXTRA = BED != BED_NONE;
+  __device__ static __forceinline__ float cell(float c, float w, float s, float n, float e, float nw, float sw,
+                                               float ne, float se, float t, float x, bool first, float)
+  {
+    return thermal_cell<BED>(c, w, s, n, e, nw, sw, ne, se, t, x, first);
+  }
+};
+
 /* Columns wx .. wx+31 (lane = column; columns past nx only feed the
  * shuffles), output rows y0 .. y1-1.  The whole warp must call it. */
-template <bool TMAP, int BED>
+template <bool TMAP, class R>
 __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
                                                    float *__restrict__ b,
                                                    int nx,
@@ -36,7 +52,8 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
                                                    int first,
                                                    int wx,
                                                    int y0,
-                                                   int y1)
+                                                   int y1,
+                                                   float param = 0.f)
 {
   const int  lane = threadIdx.x & 31;
   const int  gx = wx + lane;
@@ -71,7 +88,7 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
       vl[q + 2] = __ldg(r + hx); /* the halo value until the shuffles below */
       const size_t o = (size_t)min(j0 + q, ny - 1) * nx + gxc;
       tl[q] = TMAP ? __ldg(talus + o) : talus_value;
-      bd[q] = BED != BED_NONE ? __ldg(bedrock + o) : 0.f;
+      bd[q] = R::EXTRA ? __ldg(bedrock + o) : 0.f;
     }
 #pragma unroll
     for (int q = 2; q < SW_P + 2; q++)
@@ -92,8 +109,8 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
       else if (j == 0) out = vc[q + 2];
       else if (j == ny - 1) out = vc[q];
       else
-        out = thermal_cell<BED>(vc[q + 1], vl[q + 1], vc[q + 2], vc[q], vr[q + 1], vl[q], vl[q + 2], vr[q], vr[q + 2],
-                                tl[q], bd[q], first != 0);
+        out = R::cell(vc[q + 1], vl[q + 1], vc[q + 2], vc[q], vr[q + 1], vl[q], vl[q + 2], vr[q], vr[q + 2], tl[q],
+                      bd[q], first != 0, param);
       b[(size_t)j * nx + gx] = out;
     }
     vc[0] = vc[SW_P];
@@ -113,7 +130,7 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
  * grids; identical bits to thermal_sweep_warp. */
 constexpr int S2_P = 4; /* rows whose loads are issued together */
 
-template <bool TMAP, int BED>
+template <bool TMAP, class R>
 __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
                                                     float *__restrict__ b,
                                                     int nx,
@@ -124,7 +141,8 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
                                                     int first,
                                                     int wx,
                                                     int y0,
-                                                    int y1)
+                                                    int y1,
+                                                    float param = 0.f)
 {
   const int  lane = threadIdx.x & 31;
   const int  gx = wx + 2 * lane; /* first of the lane's two columns (nx is even) */
@@ -160,7 +178,7 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
       load(min(j0 + 1 + q, ny - 1), q + 2);
       const size_t o = (size_t)min(j0 + q, ny - 1) * nx + gxc;
       tl[q] = TMAP ? __ldg(reinterpret_cast<const float2 *>(talus + o)) : make_float2(talus_value, talus_value);
-      bd[q] = BED != BED_NONE ? __ldg(reinterpret_cast<const float2 *>(bedrock + o)) : make_float2(0.f, 0.f);
+      bd[q] = R::EXTRA ? __ldg(reinterpret_cast<const float2 *>(bedrock + o)) : make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int q = 2; q < S2_P + 2; q++) exchange(q);
@@ -175,14 +193,14 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
       else if (j == 0) out.x = vx[q + 2];
       else if (j == ny - 1) out.x = vx[q];
       else
-        out.x = thermal_cell<BED>(vx[q + 1], vw[q + 1], vx[q + 2], vx[q], vy[q + 1], vw[q], vw[q + 2], vy[q],
-                                  vy[q + 2], tl[q].x, bd[q].x, first != 0);
+        out.x = R::cell(vx[q + 1], vw[q + 1], vx[q + 2], vx[q], vy[q + 1], vw[q], vw[q + 2], vy[q], vy[q + 2],
+                        tl[q].x, bd[q].x, first != 0, param);
       if (gx + 1 == nx - 1) out.y = vx[q + 1];
       else if (j == 0) out.y = vy[q + 2];
       else if (j == ny - 1) out.y = vy[q];
       else
-        out.y = thermal_cell<BED>(vy[q + 1], vx[q + 1], vy[q + 2], vy[q], ve[q + 1], vx[q], vx[q + 2], ve[q],
-                                  ve[q + 2], tl[q].y, bd[q].y, first != 0);
+        out.y = R::cell(vy[q + 1], vx[q + 1], vy[q + 2], vy[q], ve[q + 1], vx[q], vx[q + 2], ve[q], ve[q + 2],
+                        tl[q].y, bd[q].y, first != 0, param);
       *reinterpret_cast<float2 *>(b + (size_t)j * nx + gx) = out;
     }
     vx[0] = vx[S2_P];
