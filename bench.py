@@ -646,6 +646,21 @@ def run_extras(a):
         rows[name] = {"iterations": iters, "cell_updates_per_s": rate, "bytes_per_cell_update": bpc,
                       "gb_per_s": rate * bpc / 1e9, "frac": rate * bpc / 1e9 / peak, "peak": peak,
                       "peak_kind": peak_kind}
+    # sediment_deposition: 20 layers of 25 thermal steps (talus map) each
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for rep in range(a.warmup + 1):
+        zt.copy_(zd)
+        torch.cuda.synchronize()
+        e0.record()
+        G.sediment_deposition_device(zt, td, None, 0.01, 20, 25, ctx=ctx)
+        e1.record()
+        torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3
+    rate = cells * 500 / t
+    rows["sediment_deposition"] = {"iterations": 500, "cell_updates_per_s": rate, "bytes_per_cell_update": 12.0,
+                                   "gb_per_s": rate * 12.0 / 1e9, "frac": rate * 12.0 / 1e9 / peak, "peak": peak,
+                                   "peak_kind": peak_kind, "layers": 20, "thermal_subiterations": 25}
     # sibling talus stencils, 200 iterations each
     zmax = (z + 0.25).astype(np.float32)
     zmd = torch.from_numpy(zmax).to(dev)
@@ -671,6 +686,7 @@ def run_extras(a):
             ("flow_simulation", lambda k: po.ref_flow_simulation(z, 0.01, depth_map, k))]
     for name, rule, _ in sib:
         refs.append((name, lambda k, rule=rule: po.ref_thermal_sibling(rule, z, talus, k, zmax=zmax)))
+    refs.append(("sediment_deposition", lambda k: po.ref_sediment_deposition(z, talus, 0.01, 1, k)))
     for name, fn in refs:
         fn(1)
         k = 4 if name in ("flow_simulation", "thermal_olsen") else 8

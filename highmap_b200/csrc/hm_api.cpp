@@ -189,6 +189,69 @@ int sibling_host(hm_context *ctx, int rule, float *z, int nx, int ny, const floa
 }
 } // namespace
 
+namespace
+{
+int deposition_check(hm_context *ctx, const float *z, int nx, int ny, const float *talus, int iterations,
+                     int thermal_subiterations)
+{
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "sediment_deposition: ctx is NULL");
+  if (!talus) return hm::fail(HM_ERR_INVALID_ARGUMENT, "sediment_deposition: talus is NULL");
+  if (iterations < 0 || thermal_subiterations < 0)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "sediment_deposition: negative iteration count");
+  return hm::thermal_check_args(z, nx, ny, thermal_subiterations, nullptr);
+}
+} // namespace
+
+int hm_sediment_deposition(hm_context *ctx, float *z, int nx, int ny, const float *talus, float max_deposition,
+                           int iterations, int thermal_subiterations, float *deposition_map, const float *mask)
+{
+  hm::clear_error();
+  int st = deposition_check(ctx, z, nx, ny, talus, iterations, thermal_subiterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const size_t n = (size_t)nx * ny;
+  const size_t nbytes = n * sizeof(float);
+  const size_t fields = 2 + (deposition_map ? 1 : 0) + (mask ? 1 : 0);
+  const size_t total = fields * align_up(nbytes, 256) + align_up(hm::deposition_scratch_floats(nx, ny) * 4, 256);
+  void        *ws = nullptr;
+  if ((st = hm::workspace(ctx, total, &ws))) return st;
+  Slab         sl{(char *)ws};
+  float       *dz = sl.take(n);
+  float       *dt = sl.take(n);
+  float       *dd = deposition_map ? sl.take(n) : nullptr;
+  float       *dm = mask ? sl.take(n) : nullptr;
+  float       *scr = sl.take(hm::deposition_scratch_floats(nx, ny));
+  cudaStream_t s = ctx->stream;
+  HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
+  HM_CUDA_TRY(cudaMemcpyAsync(dt, talus, nbytes, cudaMemcpyHostToDevice, s));
+  if (dm) HM_CUDA_TRY(cudaMemcpyAsync(dm, mask, nbytes, cudaMemcpyHostToDevice, s));
+  st = hm::deposition_core(ctx->device, dz, nx, ny, dt, max_deposition, iterations, thermal_subiterations, dd, dm,
+                           scr, s);
+  if (st)
+  {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  HM_CUDA_TRY(cudaMemcpyAsync(z, dz, nbytes, cudaMemcpyDeviceToHost, s));
+  if (dd) HM_CUDA_TRY(cudaMemcpyAsync(deposition_map, dd, nbytes, cudaMemcpyDeviceToHost, s));
+  HM_CUDA_TRY(cudaStreamSynchronize(s));
+  return HM_OK;
+}
+
+int hm_sediment_deposition_device(hm_context *ctx, float *z, int nx, int ny, const float *talus,
+                                  float max_deposition, int iterations, int thermal_subiterations,
+                                  float *deposition_map, const float *mask, void *stream)
+{
+  hm::clear_error();
+  int st = deposition_check(ctx, z, nx, ny, talus, iterations, thermal_subiterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::deposition_scratch_floats(nx, ny) * sizeof(float), &ws))) return st;
+  return hm::deposition_core(ctx->device, z, nx, ny, talus, max_deposition, iterations, thermal_subiterations,
+                             deposition_map, mask, (float *)ws, (cudaStream_t)stream);
+}
+
 int hm_thermal_ridge(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
                      float *deposition_map, const float *mask)
 {

@@ -8,6 +8,7 @@
  *   hydraulic_vpipes HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
  *   flow_simulation  HighMap/src/hydrology/flow_simulation.cpp:26-110
  *   thermal_olsen / _ridge / _schott / _scree  HighMap/src/erosion/thermal_gpu.cpp:221-396
+ *   sediment_deposition  HighMap/src/erosion/deposition.cpp:19-66
  *   init_opencl      HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134
  * The reference functions return void and report problems only through
  * their logger; here a failed call leaves z untouched, prints the status
@@ -211,6 +212,41 @@ void sibling_impl(int rule, const char *fn, Array &z, const Array *p_mask, const
   }
 }
 } // namespace
+
+void sediment_deposition(Array &z, Array *p_mask, const Array &talus, Array *p_deposition_map, float max_deposition,
+                         int iterations, int thermal_subiterations)
+{
+  const char *fn = "hmap::gpu::sediment_deposition";
+  if (!same_shape(&talus, z) || !same_shape(p_mask, z) || z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
+  {
+    report(HM_ERR_INVALID_ARGUMENT, fn);
+    g_err += "arrays of different shapes";
+    return;
+  }
+  hm_context *ctx = context();
+  if (!ctx)
+  {
+    report(HM_ERR_NO_DEVICE, fn);
+    return;
+  }
+  std::vector<float> zw(z.vector), depo(p_deposition_map ? z.vector.size() : 0);
+  int st = hm_sediment_deposition(ctx, zw.data(), z.shape.x, z.shape.y, talus.vector.data(), max_deposition,
+                                  iterations, thermal_subiterations, p_deposition_map ? depo.data() : nullptr,
+                                  p_mask ? p_mask->vector.data() : nullptr);
+  if (!report(st, fn)) return;
+  z.vector.swap(zw);
+  if (p_deposition_map)
+  {
+    shape_like(p_deposition_map, z);
+    p_deposition_map->vector.swap(depo);
+  }
+}
+
+void sediment_deposition(Array &z, const Array &talus, Array *p_deposition_map, float max_deposition,
+                         int iterations, int thermal_subiterations)
+{
+  sediment_deposition(z, nullptr, talus, p_deposition_map, max_deposition, iterations, thermal_subiterations);
+}
 
 void thermal_olsen(Array &z, const Array &talus, int iterations)
 {

@@ -19,6 +19,11 @@ int    thermal_core(int device, float *z, int nx, int ny, const float *talus, fl
 /* border extrapolation, deposition map and mask blend after the steps */
 int    thermal_finish(int device, float *z, int nx, int ny, const float *z0, float *depo, const float *mask,
                       cudaStream_t s, bool depo_abs = false);
+/* sediment_deposition (hm_deposition.cu): device pointers, ordered on s */
+size_t deposition_scratch_floats(int nx, int ny);
+int    deposition_core(int device, float *z, int nx, int ny, const float *talus, float max_deposition,
+                       int iterations, int thermal_subiterations, float *depo, const float *mask, float *scratch,
+                       cudaStream_t s);
 /* sibling talus stencils (hm_sibling.cu): rule HM_RIDGE .. HM_OLSEN; zmax
  * for scree, intensity for schott; scratch of thermal_scratch_floats(nx,
  * ny, true) floats */

@@ -161,6 +161,35 @@ def thermal_auto_bedrock(z: np.ndarray, talus, iterations: int = 10, deposition_
                                             _ptr(deposition_map), C.byref(opts)))
 
 
+def sediment_deposition(z: np.ndarray, talus: np.ndarray, deposition_map: np.ndarray | None = None,
+                        max_deposition: float = 0.01, iterations: int = 5, thermal_subiterations: int = 10,
+                        mask: np.ndarray | None = None, ctx: Context | None = None) -> None:
+    """hmap::gpu::sediment_deposition (deposition.cpp:19-66), in place."""
+    _grid(z, "z", writable=True)
+    ny, nx = z.shape
+    _grid(talus, "talus", z.shape)
+    if deposition_map is not None:
+        _grid(deposition_map, "deposition_map", z.shape, writable=True)
+    if mask is not None:
+        _grid(mask, "mask", z.shape)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_sediment_deposition(ctx.handle, _ptr(z), nx, ny, _ptr(talus), C.c_float(max_deposition),
+                                           int(iterations), int(thermal_subiterations), _ptr(deposition_map),
+                                           _ptr(mask)))
+
+
+def sediment_deposition_device(z, talus, deposition_map=None, max_deposition: float = 0.01, iterations: int = 5,
+                               thermal_subiterations: int = 10, mask=None, ctx: Context | None = None,
+                               stream=None) -> None:
+    ny, nx = z.shape
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_sediment_deposition_device(ctx.handle, _tptr(z, "z"), nx, ny, _tptr(talus, "talus", z.shape),
+                                                  C.c_float(max_deposition), int(iterations),
+                                                  int(thermal_subiterations),
+                                                  _tptr(deposition_map, "deposition_map", z.shape),
+                                                  _tptr(mask, "mask", z.shape), _stream(stream)))
+
+
 RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
 
 

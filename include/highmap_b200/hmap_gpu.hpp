@@ -66,6 +66,22 @@ void thermal_auto_bedrock(Array &z,
                           int    iterations = 10,
                           Array *p_deposition_map = nullptr);
 
+/* HighMap/include/highmap/erosion.hpp:1366-1379 */
+void sediment_deposition(Array       &z,
+                         Array       *p_mask,
+                         const Array &talus,
+                         Array       *p_deposition_map = nullptr,
+                         float        max_deposition = 0.01,
+                         int          iterations = 5,
+                         int          thermal_subiterations = 10);
+
+void sediment_deposition(Array       &z,
+                         const Array &talus,
+                         Array       *p_deposition_map = nullptr,
+                         float        max_deposition = 0.01,
+                         int          iterations = 5,
+                         int          thermal_subiterations = 10);
+
 /* sibling talus stencils, HighMap/include/highmap/erosion.hpp:1887-2028 */
 void thermal_olsen(Array &z, const Array &talus, int iterations);
 

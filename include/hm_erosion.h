@@ -205,6 +205,40 @@ int hm_thermal_auto_bedrock_device(hm_context               *ctx,
                                    const hm_thermal_options *opts,
                                    void                     *stream);
 
+/* ---- sediment deposition ------------------------------------------------- */
+
+/* Replaces hmap::gpu::sediment_deposition(Array &z, const Array &talus,
+ * Array *p_deposition_map, float max_deposition, int iterations,
+ * int thermal_subiterations) and the masked overload
+ * (HighMap/include/highmap/erosion.hpp:1366-1379,
+ *  HighMap/src/erosion/deposition.cpp:19-66): max_deposition laid down in
+ * `iterations` layers, each settled by thermal_subiterations thermal steps
+ * (talus map); z += sediment (blended with the input by mask when given);
+ * deposition_map receives the sediment.  mask and deposition_map nullable. */
+int hm_sediment_deposition(hm_context  *ctx,
+                           float       *z,
+                           int          nx,
+                           int          ny,
+                           const float *talus,
+                           float        max_deposition,
+                           int          iterations,
+                           int          thermal_subiterations,
+                           float       *deposition_map,
+                           const float *mask);
+
+/* The same on device buffers, ordered on `stream`. */
+int hm_sediment_deposition_device(hm_context  *ctx,
+                                  float       *z,
+                                  int          nx,
+                                  int          ny,
+                                  const float *talus,
+                                  float        max_deposition,
+                                  int          iterations,
+                                  int          thermal_subiterations,
+                                  float       *deposition_map,
+                                  const float *mask,
+                                  void        *stream);
+
 /* ---- sibling talus stencils ---------------------------------------------- */
 
 /* Rules of hm_thermal_stencil_device. */

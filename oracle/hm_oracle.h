@@ -122,6 +122,27 @@ int hmo_vpipes_f64(double                  *z,
                    double                  *vel_u,
                    double                  *vel_v);
 
+/* sediment_deposition (HighMap/src/erosion/deposition.cpp:19-66) and its
+ * masked overload; deposition_map and mask nullable. */
+int hmo_sediment_deposition_f32(float       *z,
+                                int          nx,
+                                int          ny,
+                                const float *talus,
+                                float        max_deposition,
+                                int          iterations,
+                                int          thermal_subiterations,
+                                float       *deposition_map,
+                                const float *mask);
+int hmo_sediment_deposition_f64(double       *z,
+                                int           nx,
+                                int           ny,
+                                const double *talus,
+                                double        max_deposition,
+                                int           iterations,
+                                int           thermal_subiterations,
+                                double       *deposition_map,
+                                const double *mask);
+
 /* Sibling talus stencils (thermal_gpu.cpp:221-396; kernels thermal_ridge.cl,
  * thermal_scree.cl, thermal_schott.cl, thermal_olsen.cl), Jacobi form.
  * zmax: scree only; intensity: schott only; deposition_map: |z - z0| for

@@ -146,6 +146,37 @@ def vpipes(z, params: VpipesParams, rain_map=None, dtype=np.float32):
     return (z, *outs)
 
 
+def sediment_deposition(z, talus, max_deposition=0.01, iterations=5, thermal_subiterations=10, mask=None,
+                        dtype=np.float32):
+    """Oracle sediment_deposition; returns (z, deposition map)."""
+    z = _grid(z, dtype).copy()
+    ny, nx = z.shape
+    talus = _grid(talus, dtype)
+    mask = None if mask is None else _grid(mask, dtype)
+    depo = np.empty_like(z)
+    fn = _lib().hmo_sediment_deposition_f32 if dtype == np.float32 else _lib().hmo_sediment_deposition_f64
+    S = C.c_float if dtype == np.float32 else C.c_double
+    rc = fn(_p(z), nx, ny, _p(talus), S(max_deposition), int(iterations), int(thermal_subiterations), _p(depo),
+            _p(mask))
+    if rc:
+        raise ValueError("oracle sediment_deposition rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
+def ref_sediment_deposition(z, talus, max_deposition=0.01, iterations=5, thermal_subiterations=10, mask=None):
+    """deposition.cpp:19-66 driven over the reference's thermal kernel text."""
+    z = _grid(z, np.float32).copy()
+    ny, nx = z.shape
+    talus = _grid(talus, np.float32)
+    mask = None if mask is None else _grid(mask, np.float32)
+    depo = np.empty_like(z)
+    rc = _ref().ref_sediment_deposition(_p(z), nx, ny, _p(talus), C.c_float(max_deposition), int(iterations),
+                                        int(thermal_subiterations), _p(depo), _p(mask))
+    if rc:
+        raise ValueError("ref sediment_deposition rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
 RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
 
 

@@ -13,6 +13,7 @@
  *   ref_vpipes     : HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
  *   ref_flow_simulation : HighMap/src/hydrology/flow_simulation.cpp:26-110
  *   ref_thermal_sibling : HighMap/src/erosion/thermal_gpu.cpp:221-396
+ *   ref_sediment_deposition : HighMap/src/erosion/deposition.cpp:19-66
  *
  * Work-items run as a host loop (OpenMP over rows).  The in-place thermal
  * kernels are given a private copy of the three rows around the work-item,
@@ -181,6 +182,38 @@ int ref_thermal_auto_bedrock(float       *z,
   if (deposition_map)
     for (size_t k = 0; k < n; k++) deposition_map[k] = std::max(a[k] - z0[k], 0.f);
   std::memcpy(z, a.data(), n * sizeof(float));
+  return 0;
+}
+
+/* deposition.cpp:19-66 over the reference's thermal kernel (ref_thermal) */
+int ref_sediment_deposition(float       *z,
+                            int          nx,
+                            int          ny,
+                            const float *talus,
+                            float        max_deposition,
+                            int          iterations,
+                            int          thermal_subiterations,
+                            float       *deposition_map,
+                            const float *mask)
+{
+  if (!z || !talus || nx < 3 || ny < 3 || iterations < 0 || thermal_subiterations < 0) return 1;
+  const size_t       n = (size_t)nx * ny;
+  const float        step = max_deposition / (int)iterations;
+  std::vector<float> smap(n, 0.f), ztot(n);
+  for (int it = 0; it < iterations; it++)
+  {
+    for (size_t k = 0; k < n; k++) smap[k] = smap[k] + step;
+    for (size_t k = 0; k < n; k++) ztot[k] = z[k] + smap[k];
+    int rc = ref_thermal(ztot.data(), nx, ny, talus, thermal_subiterations, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    for (size_t k = 0; k < n; k++) smap[k] = std::max(ztot[k] - z[k], 0.f);
+  }
+  for (size_t k = 0; k < n; k++)
+  {
+    const float zf = z[k] + smap[k];
+    z[k] = mask ? z[k] * (1.f - mask[k]) + zf * mask[k] : zf;
+    if (deposition_map) deposition_map[k] = smap[k];
+  }
   return 0;
 }
 

@@ -6,7 +6,7 @@
  * requested solver, writes the results as raw float32 for the test to
  * compare with the oracle.
  *
- * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen>
+ * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition>
  *        nx ny in.f32 out_prefix
  */
 #include <cstdio>
@@ -94,6 +94,13 @@ int main(int argc, char **argv)
     else hmap::gpu::thermal_olsen(z, &mask, talus, 20);
     write_raw(out + "_z.f32", z);
     if (mode != "olsen") write_raw(out + "_depo.f32", depo);
+  }
+  else if (mode == "deposition")
+  {
+    hmap::Array talus(shape, 0.5f / shape.x), depo;
+    hmap::gpu::sediment_deposition(z, talus, &depo, 0.02f, 4, 8);
+    write_raw(out + "_z.f32", z);
+    write_raw(out + "_depo.f32", depo);
   }
   else if (mode == "vpipes")
   {

@@ -8,7 +8,7 @@ thermal_ridge.cl, thermal_scree.cl, thermal_schott.cl, thermal_olsen.cl) compile
 for the CPU by oracle/build_oracle.py and driven by oracle/ref_harness.cpp
 (Jacobi form).  Run in a checkout where the reference tree is present:
 
-    python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation] [siblings]
+    python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation] [siblings] [deposition]
 
 Each .npz holds the inputs, the parameters and the outputs of one case.
 """
@@ -126,8 +126,17 @@ def sibling_cases():
         _save(name, **arrays)
 
 
+def deposition_cases():
+    nx, ny = 50, 42
+    z = fbm(nx, ny, seed=10)
+    talus = ((0.3 + fbm(nx, ny, seed=11)) / nx).astype(np.float32)
+    zo, depo = po.ref_sediment_deposition(z, talus, max_deposition=0.02, iterations=4, thermal_subiterations=8)
+    _save("sediment_deposition", z=z, talus=talus, params=np.array(json.dumps(
+        dict(max_deposition=0.02, iterations=4, thermal_subiterations=8))), out_z=zo, out_depo=depo)
+
+
 GROUPS = {"thermal": thermal_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases,
-          "siblings": sibling_cases}
+          "siblings": sibling_cases, "deposition": deposition_cases}
 
 if __name__ == "__main__":
     if not po.ref_available():

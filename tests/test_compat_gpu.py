@@ -104,6 +104,15 @@ def test_sibling_stencils(gpu, example, tmp_path, mode):
         assert np.array_equal(load("depo"), depo)
 
 
+def test_sediment_deposition(gpu, example, tmp_path):
+    z = fbm(80, 64, seed=12)
+    load = _run(example, "deposition", z, tmp_path)
+    talus = np.full_like(z, np.float32(0.5) / np.float32(80))
+    want, depo = po.sediment_deposition(z, talus, 0.02, 4, 8)
+    assert np.array_equal(load("z"), want)
+    assert np.array_equal(load("depo"), depo)
+
+
 def test_vpipes(gpu, example, tmp_path):
     z = fbm(96, 64, seed=2)
     load = _run(example, "vpipes", z, tmp_path)

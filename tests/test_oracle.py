@@ -100,6 +100,13 @@ def test_sibling_golden_bit_exact(name, rule):
         assert np.array_equal(depo, g["out_depo"])
 
 
+def test_sediment_deposition_golden_bit_exact():
+    g = _load("sediment_deposition")
+    kw = json.loads(str(g["params"]))
+    z, depo = po.sediment_deposition(g["z"], g["talus"], **kw)
+    assert np.array_equal(z, g["out_z"]) and np.array_equal(depo, g["out_depo"])
+
+
 def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))}
     assert {"thermal_uniform", "vpipes_defaults", "vpipes_rain_per_step"} <= names
@@ -153,6 +160,17 @@ def test_siblings_match_reference_text(rule):
         assert np.array_equal(a, b)
         if rule != po.OLSEN:
             assert np.array_equal(da, db)
+
+
+@ref_only
+def test_sediment_deposition_matches_reference_text():
+    z = fbm(47, 39, seed=27)
+    talus = ((0.3 + fbm(47, 39, seed=28)) / 47).astype(np.float32)
+    mask = fbm(47, 39, seed=29)
+    for m in (None, mask):
+        a, da = po.sediment_deposition(z, talus, 0.03, 3, 6, mask=m)
+        b, db = po.ref_sediment_deposition(z, talus, 0.03, 3, 6, mask=m)
+        assert np.array_equal(a, b) and np.array_equal(da, db)
 
 
 def test_flat_field_unchanged():
