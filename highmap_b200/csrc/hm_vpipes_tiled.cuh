@@ -49,6 +49,12 @@ constexpr int FWE_GENERIC = 8;   /* options read at run time            */
 constexpr int FWE_FLOWONLY = 16; /* flow and water passes only (flow_simulation): no
                                   * erosion, terrain fixed, writes depth and fluxes */
 
+/* Resident CTAs per SM the step kernels are compiled for: five (at most 48
+ * registers, 5 x 34 KB of shared memory) keeps 40 warps per SM issuing,
+ * which outruns four CTAs of the unconstrained 52-register code although
+ * the erosion forms then spill a few words. */
+constexpr int FWE_MIN_BLOCKS = 5;
+
 /* Shared-memory layout of the staged fields, one for both staging modes.
  * Every array row covers the 40 columns x0-4 .. x0+35 (a TMA box must start
  * on a 16-byte boundary, so the boxes start at x0-4), column c holding
@@ -391,7 +397,7 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
 }
 
 template <bool MAINTAIN, int F>
-__global__ void __launch_bounds__(FT_NT) k_vp_fwe(FweIo io, VpConst c, VpScalars *sc, double *partials)
+__global__ void __launch_bounds__(FT_NT, FWE_MIN_BLOCKS) k_vp_fwe(FweIo io, VpConst c, VpScalars *sc, double *partials)
 {
   __shared__ FweSmem sm;
   fwe_stage_cp_async(io, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm);
@@ -404,7 +410,7 @@ __global__ void __launch_bounds__(FT_NT) k_vp_fwe(FweIo io, VpConst c, VpScalars
  * top-up it still takes part in the grid-wide sum (adding zero) so the
  * last block's finish is not left waiting for it. */
 template <bool MAINTAIN, int F>
-__global__ void __launch_bounds__(FT_NT)
+__global__ void __launch_bounds__(FT_NT, FWE_MIN_BLOCKS)
     k_vp_fwe_tma(FweIo io, const __grid_constant__ FweMaps maps, VpConst c, VpScalars *sc, double *partials)
 {
   __shared__ FweSmem sm;
