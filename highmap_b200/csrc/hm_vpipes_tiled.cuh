@@ -49,11 +49,13 @@ constexpr int FWE_GENERIC = 8;   /* options read at run time            */
 constexpr int FWE_FLOWONLY = 16; /* flow and water passes only (flow_simulation): no
                                   * erosion, terrain fixed, writes depth and fluxes */
 
-/* Resident CTAs per SM the step kernels are compiled for: five (at most 48
- * registers, 5 x 34 KB of shared memory) keeps 40 warps per SM issuing,
- * which outruns four CTAs of the unconstrained 52-register code although
- * the erosion forms then spill a few words. */
-constexpr int FWE_MIN_BLOCKS = 5;
+/* Resident CTAs per SM the step kernels are compiled for.  The erosion
+ * forms take five (at most 48 registers, 5 x 34 KB of shared memory): 40
+ * warps per SM issuing outrun four CTAs of the unconstrained 52-register
+ * code although a few words then spill.  The flow-only form
+ * (flow_simulation) fits 40 registers, six CTAs per SM; a looser bound
+ * lets the compiler take 46 and costs the sixth CTA (5 % slower). */
+constexpr int fwe_min_blocks(int flags) { return (flags & FWE_FLOWONLY) ? 6 : 5; }
 
 /* Shared-memory layout of the staged fields, one for both staging modes.
  * Every array row covers the 40 columns x0-4 .. x0+35 (a TMA box must start
@@ -397,7 +399,7 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
 }
 
 template <bool MAINTAIN, int F>
-__global__ void __launch_bounds__(FT_NT, FWE_MIN_BLOCKS) k_vp_fwe(FweIo io, VpConst c, VpScalars *sc, double *partials)
+__global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F)) k_vp_fwe(FweIo io, VpConst c, VpScalars *sc, double *partials)
 {
   __shared__ FweSmem sm;
   fwe_stage_cp_async(io, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm);
@@ -410,7 +412,7 @@ __global__ void __launch_bounds__(FT_NT, FWE_MIN_BLOCKS) k_vp_fwe(FweIo io, VpCo
  * top-up it still takes part in the grid-wide sum (adding zero) so the
  * last block's finish is not left waiting for it. */
 template <bool MAINTAIN, int F>
-__global__ void __launch_bounds__(FT_NT, FWE_MIN_BLOCKS)
+__global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
     k_vp_fwe_tma(FweIo io, const __grid_constant__ FweMaps maps, VpConst c, VpScalars *sc, double *partials)
 {
   __shared__ FweSmem sm;
