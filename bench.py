@@ -596,9 +596,10 @@ FLOW_BYTES = 44.0          # z, depth and four fluxes in; depth and four fluxes 
 
 def run_extras(a):
     """thermal_auto_bedrock (talus map, 500 iterations), flow_simulation
-    (depth map, 1000 iterations, reference defaults) and the sibling talus
-    stencils ridge, scree (zmax = z + 0.25), schott and olsen (200
-    iterations each) on the 4096^2 inputs:
+    (depth map, 1000 iterations, reference defaults), sediment_deposition
+    (20 layers x 25 steps), sediment_layer and the snow post-filter (500
+    steps each) and the sibling talus stencils ridge, scree (zmax = z +
+    0.25), schott and olsen (200 iterations each) on the 4096^2 inputs:
     device-timed cell-updates/s against the HBM roofline, and the
     reference's kernel text on the host cores on a bounded sample (a few
     iterations on the full grid, scaled)."""
@@ -661,6 +662,31 @@ def run_extras(a):
     rows["sediment_deposition"] = {"iterations": 500, "cell_updates_per_s": rate, "bytes_per_cell_update": 12.0,
                                    "gb_per_s": rate * 12.0 / 1e9, "frac": rate * 12.0 / 1e9 / peak, "peak": peak,
                                    "peak_kind": peak_kind, "layers": 20, "thermal_subiterations": 25}
+    # sediment_layer (500 thermal steps, post-filter on) and the snow
+    # post-filter (500 masked thermal steps): thermal cell-updates/s at the
+    # 12 B of a talus-map step, the preparation and filter passes included
+    upper = ((3.0 + 2.0 * fbm(n, n, seed=5)) / n).astype(np.float32)
+    snow = (0.08 * fbm(n, n, seed=6)).astype(np.float32)
+    ud = torch.from_numpy(upper).to(dev)
+    sd = torch.from_numpy(snow).to(dev)
+    s_w = torch.empty_like(sd)
+    for name, run in (("sediment_layer", lambda: G.sediment_layer_device(zt, td, ud, 500, True, ctx=ctx)),
+                      ("snow_post_filter", lambda: G.snow_post_filter_device(zd, s_w, 0.05, 500, 0.2, ctx=ctx))):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for rep in range(a.warmup + 1):
+            zt.copy_(zd)
+            s_w.copy_(sd)
+            torch.cuda.synchronize()
+            e0.record()
+            run()
+            e1.record()
+            torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+        rate = cells * 500 / t
+        rows[name] = {"iterations": 500, "cell_updates_per_s": rate, "bytes_per_cell_update": 12.0,
+                      "gb_per_s": rate * 12.0 / 1e9, "frac": rate * 12.0 / 1e9 / peak, "peak": peak,
+                      "peak_kind": peak_kind}
     # sibling talus stencils, 200 iterations each
     zmax = (z + 0.25).astype(np.float32)
     zmd = torch.from_numpy(zmax).to(dev)
@@ -687,6 +713,8 @@ def run_extras(a):
     for name, rule, _ in sib:
         refs.append((name, lambda k, rule=rule: po.ref_thermal_sibling(rule, z, talus, k, zmax=zmax)))
     refs.append(("sediment_deposition", lambda k: po.ref_sediment_deposition(z, talus, 0.01, 1, k)))
+    refs.append(("sediment_layer", lambda k: po.ref_sediment_layer(z, talus, upper, k, True)))
+    refs.append(("snow_post_filter", lambda k: po.ref_snow_post_filter(z, snow, 0.05, k, 0.2)))
     for name, fn in refs:
         fn(1)
         k = 4 if name in ("flow_simulation", "thermal_olsen") else 8
@@ -696,7 +724,8 @@ def run_extras(a):
         rows[name]["cpu_baseline"] = {"value": cells * k / t, "unit": "cell-updates/s", "cores": po.num_threads(),
                                       "kind": "reference", "sample": "%d iterations on the full %dx%d inputs" %
                                       (k, n, n)}
-    out = {"metric": "cell-updates/s at %d^2, thermal_auto_bedrock, flow_simulation, sibling talus stencils" % n,
+    out = {"metric": "cell-updates/s at %d^2, thermal_auto_bedrock, flow_simulation, deposition callers, "
+                     "sibling talus stencils" % n,
            "value": rows["flow_simulation"]["cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": 1,
            "higher_is_better": True, "dtype": "f32", "data": "synthetic", "form": "extras",
            "config": {"workload": "auto-bedrock thermal (talus map) x500, flow simulation (depth map fBm seed 4, "

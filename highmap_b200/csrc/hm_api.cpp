@@ -252,6 +252,120 @@ int hm_sediment_deposition_device(hm_context *ctx, float *z, int nx, int ny, con
                              deposition_map, mask, (float *)ws, (cudaStream_t)stream);
 }
 
+namespace
+{
+int layer_check(hm_context *ctx, const float *z, int nx, int ny, const float *talus_layer,
+                const float *talus_upper_limit, int iterations)
+{
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "sediment_layer: ctx is NULL");
+  if (!talus_layer || !talus_upper_limit)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "sediment_layer: talus_layer or talus_upper_limit is NULL");
+  return hm::thermal_check_args(z, nx, ny, iterations, nullptr);
+}
+} // namespace
+
+int hm_sediment_layer(hm_context *ctx, float *z, int nx, int ny, const float *talus_layer,
+                      const float *talus_upper_limit, int iterations, int apply_post_filter, float *deposition_map)
+{
+  hm::clear_error();
+  int st = layer_check(ctx, z, nx, ny, talus_layer, talus_upper_limit, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const size_t n = (size_t)nx * ny;
+  const size_t nbytes = n * sizeof(float);
+  const size_t fields = 3 + (deposition_map ? 1 : 0);
+  const size_t total = fields * align_up(nbytes, 256) + align_up(hm::layer_scratch_floats(nx, ny) * 4, 256);
+  void        *ws = nullptr;
+  if ((st = hm::workspace(ctx, total, &ws))) return st;
+  Slab         sl{(char *)ws};
+  float       *dz = sl.take(n);
+  float       *dl = sl.take(n);
+  float       *du = sl.take(n);
+  float       *dd = deposition_map ? sl.take(n) : nullptr;
+  float       *scr = sl.take(hm::layer_scratch_floats(nx, ny));
+  cudaStream_t s = ctx->stream;
+  HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
+  HM_CUDA_TRY(cudaMemcpyAsync(dl, talus_layer, nbytes, cudaMemcpyHostToDevice, s));
+  HM_CUDA_TRY(cudaMemcpyAsync(du, talus_upper_limit, nbytes, cudaMemcpyHostToDevice, s));
+  st = hm::layer_core(ctx->device, dz, nx, ny, dl, du, iterations, apply_post_filter != 0, dd, scr, s);
+  if (st)
+  {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  HM_CUDA_TRY(cudaMemcpyAsync(z, dz, nbytes, cudaMemcpyDeviceToHost, s));
+  if (dd) HM_CUDA_TRY(cudaMemcpyAsync(deposition_map, dd, nbytes, cudaMemcpyDeviceToHost, s));
+  HM_CUDA_TRY(cudaStreamSynchronize(s));
+  return HM_OK;
+}
+
+int hm_sediment_layer_device(hm_context *ctx, float *z, int nx, int ny, const float *talus_layer,
+                             const float *talus_upper_limit, int iterations, int apply_post_filter,
+                             float *deposition_map, void *stream)
+{
+  hm::clear_error();
+  int st = layer_check(ctx, z, nx, ny, talus_layer, talus_upper_limit, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::layer_scratch_floats(nx, ny) * sizeof(float), &ws))) return st;
+  return hm::layer_core(ctx->device, z, nx, ny, talus_layer, talus_upper_limit, iterations, apply_post_filter != 0,
+                        deposition_map, (float *)ws, (cudaStream_t)stream);
+}
+
+namespace
+{
+int snow_check(hm_context *ctx, const float *z, const float *s, int nx, int ny, int iterations)
+{
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "snow_post_filter: ctx is NULL");
+  if (!s) return hm::fail(HM_ERR_INVALID_ARGUMENT, "snow_post_filter: s is NULL");
+  return hm::thermal_check_args(z, nx, ny, iterations, nullptr);
+}
+} // namespace
+
+int hm_snow_post_filter(hm_context *ctx, const float *z, float *s, int nx, int ny, float snow_depth, int iterations,
+                        float thermal_talus_ratio)
+{
+  hm::clear_error();
+  int st = snow_check(ctx, z, s, nx, ny, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const size_t n = (size_t)nx * ny;
+  const size_t nbytes = n * sizeof(float);
+  const size_t total = 2 * align_up(nbytes, 256) + align_up(hm::snow_scratch_floats(nx, ny) * 4, 256);
+  void        *ws = nullptr;
+  if ((st = hm::workspace(ctx, total, &ws))) return st;
+  Slab         sl{(char *)ws};
+  float       *dz = sl.take(n);
+  float       *ds = sl.take(n);
+  float       *scr = sl.take(hm::snow_scratch_floats(nx, ny));
+  cudaStream_t cs = ctx->stream;
+  HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, cs));
+  HM_CUDA_TRY(cudaMemcpyAsync(ds, s, nbytes, cudaMemcpyHostToDevice, cs));
+  st = hm::snow_post_filter_core(ctx->device, dz, ds, nx, ny, snow_depth, iterations, thermal_talus_ratio, scr, cs);
+  if (st)
+  {
+    cudaStreamSynchronize(cs);
+    return st;
+  }
+  HM_CUDA_TRY(cudaMemcpyAsync(s, ds, nbytes, cudaMemcpyDeviceToHost, cs));
+  HM_CUDA_TRY(cudaStreamSynchronize(cs));
+  return HM_OK;
+}
+
+int hm_snow_post_filter_device(hm_context *ctx, const float *z, float *s, int nx, int ny, float snow_depth,
+                               int iterations, float thermal_talus_ratio, void *stream)
+{
+  hm::clear_error();
+  int st = snow_check(ctx, z, s, nx, ny, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::snow_scratch_floats(nx, ny) * sizeof(float), &ws))) return st;
+  return hm::snow_post_filter_core(ctx->device, z, s, nx, ny, snow_depth, iterations, thermal_talus_ratio,
+                                   (float *)ws, (cudaStream_t)stream);
+}
+
 int hm_thermal_ridge(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
                      float *deposition_map, const float *mask)
 {

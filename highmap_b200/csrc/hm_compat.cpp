@@ -9,6 +9,7 @@
  *   flow_simulation  HighMap/src/hydrology/flow_simulation.cpp:26-110
  *   thermal_olsen / _ridge / _schott / _scree  HighMap/src/erosion/thermal_gpu.cpp:221-396
  *   sediment_deposition  HighMap/src/erosion/deposition.cpp:19-66
+ *   sediment_layer       HighMap/src/erosion/deposition.cpp:68-113
  *   init_opencl      HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134
  * The reference functions return void and report problems only through
  * their logger; here a failed call leaves z untouched, prints the status
@@ -246,6 +247,36 @@ void sediment_deposition(Array &z, const Array &talus, Array *p_deposition_map, 
                          int iterations, int thermal_subiterations)
 {
   sediment_deposition(z, nullptr, talus, p_deposition_map, max_deposition, iterations, thermal_subiterations);
+}
+
+void sediment_layer(Array &z, const Array &talus_layer, const Array &talus_upper_limit, int iterations,
+                    bool apply_post_filter, Array *p_deposition_map)
+{
+  const char *fn = "hmap::gpu::sediment_layer";
+  if (!same_shape(&talus_layer, z) || !same_shape(&talus_upper_limit, z) ||
+      z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
+  {
+    report(HM_ERR_INVALID_ARGUMENT, fn);
+    g_err += "arrays of different shapes";
+    return;
+  }
+  hm_context *ctx = context();
+  if (!ctx)
+  {
+    report(HM_ERR_NO_DEVICE, fn);
+    return;
+  }
+  std::vector<float> zw(z.vector), depo(p_deposition_map ? z.vector.size() : 0);
+  int st = hm_sediment_layer(ctx, zw.data(), z.shape.x, z.shape.y, talus_layer.vector.data(),
+                             talus_upper_limit.vector.data(), iterations, apply_post_filter ? 1 : 0,
+                             p_deposition_map ? depo.data() : nullptr);
+  if (!report(st, fn)) return;
+  z.vector.swap(zw);
+  if (p_deposition_map)
+  {
+    shape_like(p_deposition_map, z);
+    p_deposition_map->vector.swap(depo);
+  }
 }
 
 void thermal_olsen(Array &z, const Array &talus, int iterations)

@@ -24,6 +24,16 @@ size_t deposition_scratch_floats(int nx, int ny);
 int    deposition_core(int device, float *z, int nx, int ny, const float *talus, float max_deposition,
                        int iterations, int thermal_subiterations, float *depo, const float *mask, float *scratch,
                        cudaStream_t s);
+/* sediment_layer (hm_layer.cu): device pointers, ordered on s; depo
+ * nullable; scratch of layer_scratch_floats(nx, ny) floats */
+size_t layer_scratch_floats(int nx, int ny);
+int    layer_core(int device, float *z, int nx, int ny, const float *talus_layer, const float *talus_upper_limit,
+                  int iterations, bool post_filter, float *depo, float *scratch, cudaStream_t s);
+/* snow_simulation's post-filter (hm_snow.cu): device pointers, ordered on
+ * s; scratch of snow_scratch_floats(nx, ny) floats */
+size_t snow_scratch_floats(int nx, int ny);
+int    snow_post_filter_core(int device, const float *z, float *s, int nx, int ny, float snow_depth, int iterations,
+                             float ratio, float *scratch, cudaStream_t st);
 /* sibling talus stencils (hm_sibling.cu): rule HM_RIDGE .. HM_OLSEN; zmax
  * for scree, intensity for schott; scratch of thermal_scratch_floats(nx,
  * ny, true) floats */

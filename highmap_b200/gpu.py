@@ -190,6 +190,53 @@ def sediment_deposition_device(z, talus, deposition_map=None, max_deposition: fl
                                                   _tptr(mask, "mask", z.shape), _stream(stream)))
 
 
+def sediment_layer(z: np.ndarray, talus_layer: np.ndarray, talus_upper_limit: np.ndarray, iterations: int,
+                   apply_post_filter: bool = True, deposition_map: np.ndarray | None = None,
+                   ctx: Context | None = None) -> None:
+    """hmap::gpu::sediment_layer (deposition.cpp:68-113), in place."""
+    _grid(z, "z", writable=True)
+    ny, nx = z.shape
+    _grid(talus_layer, "talus_layer", z.shape)
+    _grid(talus_upper_limit, "talus_upper_limit", z.shape)
+    if deposition_map is not None:
+        _grid(deposition_map, "deposition_map", z.shape, writable=True)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_sediment_layer(ctx.handle, _ptr(z), nx, ny, _ptr(talus_layer), _ptr(talus_upper_limit),
+                                      int(iterations), 1 if apply_post_filter else 0, _ptr(deposition_map)))
+
+
+def sediment_layer_device(z, talus_layer, talus_upper_limit, iterations: int, apply_post_filter: bool = True,
+                          deposition_map=None, ctx: Context | None = None, stream=None) -> None:
+    ny, nx = z.shape
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_sediment_layer_device(ctx.handle, _tptr(z, "z"), nx, ny,
+                                             _tptr(talus_layer, "talus_layer", z.shape),
+                                             _tptr(talus_upper_limit, "talus_upper_limit", z.shape),
+                                             int(iterations), 1 if apply_post_filter else 0,
+                                             _tptr(deposition_map, "deposition_map", z.shape), _stream(stream)))
+
+
+def snow_post_filter(z: np.ndarray, s: np.ndarray, snow_depth: float, iterations: int,
+                     thermal_talus_ratio: float = 0.2, ctx: Context | None = None) -> None:
+    """Post-filter of hmap::gpu::snow_simulation (snow_simulation.cpp:140-152
+    and its clamp_min(s, 0)): updates the snow depth s over terrain z in place."""
+    _grid(z, "z")
+    _grid(s, "s", z.shape, writable=True)
+    ny, nx = z.shape
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_snow_post_filter(ctx.handle, _ptr(z), _ptr(s), nx, ny, C.c_float(snow_depth),
+                                        int(iterations), C.c_float(thermal_talus_ratio)))
+
+
+def snow_post_filter_device(z, s, snow_depth: float, iterations: int, thermal_talus_ratio: float = 0.2,
+                            ctx: Context | None = None, stream=None) -> None:
+    ny, nx = z.shape
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_snow_post_filter_device(ctx.handle, _tptr(z, "z"), _tptr(s, "s", z.shape), nx, ny,
+                                               C.c_float(snow_depth), int(iterations),
+                                               C.c_float(thermal_talus_ratio), _stream(stream)))
+
+
 RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
 
 

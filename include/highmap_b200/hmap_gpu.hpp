@@ -82,6 +82,14 @@ void sediment_deposition(Array       &z,
                          int          iterations = 5,
                          int          thermal_subiterations = 10);
 
+/* HighMap/include/highmap/erosion.hpp:1402-1407 */
+void sediment_layer(Array       &z,
+                    const Array &talus_layer,
+                    const Array &talus_upper_limit,
+                    int          iterations,
+                    bool         apply_post_filter = true,
+                    Array       *p_deposition_map = nullptr);
+
 /* sibling talus stencils, HighMap/include/highmap/erosion.hpp:1887-2028 */
 void thermal_olsen(Array &z, const Array &talus, int iterations);
 

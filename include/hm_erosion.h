@@ -239,6 +239,65 @@ int hm_sediment_deposition_device(hm_context  *ctx,
                                   const float *mask,
                                   void        *stream);
 
+/* Replaces hmap::gpu::sediment_layer(Array &z, const Array &talus_layer,
+ * const Array &talus_upper_limit, int iterations, bool apply_post_filter,
+ * Array *p_deposition_map) (HighMap/include/highmap/erosion.hpp:1402-1407,
+ *  HighMap/src/erosion/deposition.cpp:68-113): talus from the terrain's
+ * gradient_talus (gradient.cpp:217-243), steepened to
+ * 4 (g - limit) + limit where g exceeds talus_upper_limit; `iterations`
+ * thermal steps with that talus map; with apply_post_filter (non-zero),
+ * z = z_in + deposition, smoothed by hmap::laplace (sigma 0.125, 3 steps)
+ * where the smoothed mask of the unclamped cells allows.  deposition_map
+ * (nullable) receives max(z_thermal - z_in, 0). */
+int hm_sediment_layer(hm_context  *ctx,
+                      float       *z,
+                      int          nx,
+                      int          ny,
+                      const float *talus_layer,
+                      const float *talus_upper_limit,
+                      int          iterations,
+                      int          apply_post_filter,
+                      float       *deposition_map);
+
+/* The same on device buffers, ordered on `stream`. */
+int hm_sediment_layer_device(hm_context  *ctx,
+                             float       *z,
+                             int          nx,
+                             int          ny,
+                             const float *talus_layer,
+                             const float *talus_upper_limit,
+                             int          iterations,
+                             int          apply_post_filter,
+                             float       *deposition_map,
+                             void        *stream);
+
+/* Replaces the post-filter of hmap::gpu::snow_simulation
+ * (HighMap/src/hydrology/snow_simulation.cpp:140-152, with the
+ * clamp_min(s, 0) that follows it), for a caller that runs the snow
+ * kernel itself: on terrain z and snow depth s (updated in place),
+ * mask = clamp_max_smooth(s / snow_depth, 1), z_w = z + s, `iterations`
+ * thermal steps of z_w with talus thermal_talus_ratio * gradient_norm(z_w)
+ * blended in by the mask, then s = max(z_w - z, 0). */
+int hm_snow_post_filter(hm_context  *ctx,
+                        const float *z,
+                        float       *s,
+                        int          nx,
+                        int          ny,
+                        float        snow_depth,
+                        int          iterations,
+                        float        thermal_talus_ratio);
+
+/* The same on device buffers, ordered on `stream`. */
+int hm_snow_post_filter_device(hm_context  *ctx,
+                               const float *z,
+                               float       *s,
+                               int          nx,
+                               int          ny,
+                               float        snow_depth,
+                               int          iterations,
+                               float        thermal_talus_ratio,
+                               void        *stream);
+
 /* ---- sibling talus stencils ---------------------------------------------- */
 
 /* Rules of hm_thermal_stencil_device. */

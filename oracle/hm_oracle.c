@@ -24,6 +24,7 @@
 #define POW powf
 #define RINT rintf
 #define FABS fabsf
+#define SQRT sqrtf
 #define FLOOR floorf
 #define FMIN fminf
 #define FMAX fmaxf
@@ -35,6 +36,7 @@
 #undef POW
 #undef RINT
 #undef FABS
+#undef SQRT
 #undef FLOOR
 #undef FMIN
 #undef FMAX
@@ -47,6 +49,7 @@
 #define POW pow
 #define RINT rint
 #define FABS fabs
+#define SQRT sqrt
 #define FLOOR floor
 #define FMIN fmin
 #define FMAX fmax
@@ -58,6 +61,7 @@
 #undef POW
 #undef RINT
 #undef FABS
+#undef SQRT
 #undef FLOOR
 #undef FMIN
 #undef FMAX

@@ -143,6 +143,43 @@ int hmo_sediment_deposition_f64(double       *z,
                                 double       *deposition_map,
                                 const double *mask);
 
+/* sediment_layer (HighMap/src/erosion/deposition.cpp:68-113):
+ * apply_post_filter 0/1; deposition_map nullable. */
+int hmo_sediment_layer_f32(float       *z,
+                           int          nx,
+                           int          ny,
+                           const float *talus_layer,
+                           const float *talus_upper_limit,
+                           int          iterations,
+                           int          apply_post_filter,
+                           float       *deposition_map);
+int hmo_sediment_layer_f64(double       *z,
+                           int           nx,
+                           int           ny,
+                           const double *talus_layer,
+                           const double *talus_upper_limit,
+                           int           iterations,
+                           int           apply_post_filter,
+                           double       *deposition_map);
+
+/* snow_simulation's post-filter (HighMap/src/hydrology/snow_simulation.cpp:
+ * 140-152, then its clamp_min(s, 0)): z the terrain, s the snow depth,
+ * updated in place. */
+int hmo_snow_post_filter_f32(const float *z,
+                             float       *s,
+                             int          nx,
+                             int          ny,
+                             float        snow_depth,
+                             int          iterations,
+                             float        thermal_talus_ratio);
+int hmo_snow_post_filter_f64(const double *z,
+                             double       *s,
+                             int           nx,
+                             int           ny,
+                             double        snow_depth,
+                             int           iterations,
+                             double        thermal_talus_ratio);
+
 /* Sibling talus stencils (thermal_gpu.cpp:221-396; kernels thermal_ridge.cl,
  * thermal_scree.cl, thermal_schott.cl, thermal_olsen.cl), Jacobi form.
  * zmax: scree only; intensity: schott only; deposition_map: |z - z0| for

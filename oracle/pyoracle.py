@@ -177,6 +177,60 @@ def ref_sediment_deposition(z, talus, max_deposition=0.01, iterations=5, thermal
     return z, depo
 
 
+def sediment_layer(z, talus_layer, talus_upper_limit, iterations, apply_post_filter=True, dtype=np.float32):
+    """Oracle sediment_layer (deposition.cpp:68-113); returns (z, deposition map)."""
+    z = _grid(z, dtype).copy()
+    ny, nx = z.shape
+    tl = _grid(talus_layer, dtype)
+    tu = _grid(talus_upper_limit, dtype)
+    depo = np.empty_like(z)
+    fn = _lib().hmo_sediment_layer_f32 if dtype == np.float32 else _lib().hmo_sediment_layer_f64
+    rc = fn(_p(z), nx, ny, _p(tl), _p(tu), int(iterations), 1 if apply_post_filter else 0, _p(depo))
+    if rc:
+        raise ValueError("oracle sediment_layer rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
+def ref_sediment_layer(z, talus_layer, talus_upper_limit, iterations, apply_post_filter=True):
+    """deposition.cpp:68-113 driven over the reference's thermal kernel text."""
+    z = _grid(z, np.float32).copy()
+    ny, nx = z.shape
+    tl = _grid(talus_layer, np.float32)
+    tu = _grid(talus_upper_limit, np.float32)
+    depo = np.empty_like(z)
+    rc = _ref().ref_sediment_layer(_p(z), nx, ny, _p(tl), _p(tu), int(iterations), 1 if apply_post_filter else 0,
+                                   _p(depo))
+    if rc:
+        raise ValueError("ref sediment_layer rejected its arguments (status %d)" % rc)
+    return z, depo
+
+
+def snow_post_filter(z, s, snow_depth, iterations, thermal_talus_ratio, dtype=np.float32):
+    """Oracle snow_simulation post-filter (snow_simulation.cpp:140-152 and
+    its clamp_min(s, 0)); returns the new snow depth."""
+    z = _grid(z, dtype)
+    s = _grid(s, dtype).copy()
+    ny, nx = z.shape
+    fn = _lib().hmo_snow_post_filter_f32 if dtype == np.float32 else _lib().hmo_snow_post_filter_f64
+    S = C.c_float if dtype == np.float32 else C.c_double
+    rc = fn(_p(z), _p(s), nx, ny, S(snow_depth), int(iterations), S(thermal_talus_ratio))
+    if rc:
+        raise ValueError("oracle snow_post_filter rejected its arguments (status %d)" % rc)
+    return s
+
+
+def ref_snow_post_filter(z, s, snow_depth, iterations, thermal_talus_ratio):
+    """snow_simulation.cpp:140-152 driven over the reference's thermal kernel text."""
+    z = _grid(z, np.float32)
+    s = _grid(s, np.float32).copy()
+    ny, nx = z.shape
+    rc = _ref().ref_snow_post_filter(_p(z), _p(s), nx, ny, C.c_float(snow_depth), int(iterations),
+                                     C.c_float(thermal_talus_ratio))
+    if rc:
+        raise ValueError("ref snow_post_filter rejected its arguments (status %d)" % rc)
+    return s
+
+
 RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
 
 

@@ -14,6 +14,9 @@
  *   ref_flow_simulation : HighMap/src/hydrology/flow_simulation.cpp:26-110
  *   ref_thermal_sibling : HighMap/src/erosion/thermal_gpu.cpp:221-396
  *   ref_sediment_deposition : HighMap/src/erosion/deposition.cpp:19-66
+ *   ref_sediment_layer : HighMap/src/erosion/deposition.cpp:68-113 (with
+ *                        gradient.cpp:217-243 and filters.cpp:290-324)
+ *   ref_snow_post_filter : HighMap/src/hydrology/snow_simulation.cpp:140-152
  *
  * Work-items run as a host loop (OpenMP over rows).  The in-place thermal
  * kernels are given a private copy of the three rows around the work-item,
@@ -213,6 +216,125 @@ int ref_sediment_deposition(float       *z,
     const float zf = z[k] + smap[k];
     z[k] = mask ? z[k] * (1.f - mask[k]) + zf * mask[k] : zf;
     if (deposition_map) deposition_map[k] = smap[k];
+  }
+  return 0;
+}
+
+/* deposition.cpp:68-113 over the reference's thermal kernel: the talus
+ * preparation from gradient_talus (gradient.cpp:217-243, in-place pair
+ * sweeps from zero), ref_thermal with a deposition map, and the post
+ * filter (z = input + deposition; hmap::laplace with its defaults sigma
+ * 0.125 and 3 steps, filters.cpp:290-324, on the mask, then on a copy of z
+ * blended in by that mask) */
+int ref_sediment_layer(float       *z,
+                       int          nx,
+                       int          ny,
+                       const float *talus_layer,
+                       const float *talus_upper_limit,
+                       int          iterations,
+                       int          apply_post_filter,
+                       float       *deposition_map)
+{
+  if (!z || !talus_layer || !talus_upper_limit || nx < 3 || ny < 3 || iterations < 0) return 1;
+  const size_t       n = (size_t)nx * ny;
+  auto               at = [nx](int i, int j) { return (size_t)j * nx + i; };
+  std::vector<float> zb(z, z + n), g(n, 0.f), tr(talus_layer, talus_layer + n), fm(n, 1.f), map(n);
+  for (int j = 0; j < ny; j++)
+    for (int i = 1; i < nx - 1; i += 2)
+    {
+      const float d = std::abs(z[at(i, j)] - z[at(i + 1, j)]);
+      g[at(i, j)] = std::max(g[at(i, j)], d);
+      g[at(i - 1, j)] = std::max(g[at(i - 1, j)], g[at(i, j)]);
+      g[at(i + 1, j)] = d;
+    }
+  for (int j = 1; j < ny - 1; j += 2)
+    for (int i = 0; i < nx; i++)
+    {
+      const float d = std::abs(z[at(i, j)] - z[at(i, j + 1)]);
+      g[at(i, j)] = std::max(g[at(i, j)], d);
+      g[at(i, j - 1)] = std::max(g[at(i, j - 1)], g[at(i, j)]);
+      g[at(i, j + 1)] = d;
+    }
+  for (size_t k = 0; k < n; k++)
+    if (g[k] > talus_upper_limit[k])
+    {
+      fm[k] = 0.f;
+      tr[k] = 4.f * (g[k] - talus_upper_limit[k]) + talus_upper_limit[k];
+    }
+  int rc = ref_thermal(z, nx, ny, tr.data(), iterations, nullptr, map.data(), nullptr);
+  if (rc) return rc;
+  if (apply_post_filter)
+  {
+    auto laplace = [&](std::vector<float> &a) {
+      std::vector<float> delta(n);
+      for (int it = 0; it < 3; it++)
+      {
+        for (int j = 0; j < ny; j++)
+          for (int i = 0; i < nx; i++)
+          {
+            float sum = 0.f;
+            for (int dj = -1; dj <= 1; dj++)
+              for (int di = -1; di <= 1; di++)
+                if (di != 0 || dj != 0) sum += a[at(std::clamp(i + di, 0, nx - 1), std::clamp(j + dj, 0, ny - 1))];
+            delta[at(i, j)] = sum - 8.f * a[at(i, j)];
+          }
+        for (size_t k = 0; k < n; k++) a[k] += 0.125f * delta[k];
+      }
+    };
+    for (size_t k = 0; k < n; k++) z[k] = zb[k] + map[k];
+    laplace(fm);
+    std::vector<float> zs(z, z + n);
+    laplace(zs);
+    for (size_t k = 0; k < n; k++) z[k] = z[k] * (1.f - fm[k]) + zs[k] * fm[k];
+  }
+  if (deposition_map) std::memcpy(deposition_map, map.data(), n * sizeof(float));
+  return 0;
+}
+
+/* snow_simulation.cpp:140-152 and its clamp_min(s, 0) over the
+ * reference's thermal kernel: mask = clamp_max_smooth(s / snow_depth, 1)
+ * (range.cpp:98-110, k = 0.2), z_w = z + s, talus = ratio *
+ * gradient_norm(z_w) (gradient.cpp:124-135, 182-215; math.cpp:142-151),
+ * masked thermal on z_w, s = max(z_w - z, 0) */
+int ref_snow_post_filter(const float *z,
+                         float       *s,
+                         int          nx,
+                         int          ny,
+                         float        snow_depth,
+                         int          iterations,
+                         float        thermal_talus_ratio)
+{
+  if (!z || !s || nx < 3 || ny < 3 || iterations < 0) return 1;
+  const size_t       n = (size_t)nx * ny;
+  auto               at = [nx](int i, int j) { return (size_t)j * nx + i; };
+  std::vector<float> mask(n), zw(n), dx(n), dy(n), talus(n);
+  for (size_t k = 0; k < n; k++)
+  {
+    const float x = s[k] / snow_depth, kk = 0.2f, vmax = 1.f;
+    const float h = std::max(kk - std::abs(x - vmax), 0.f) / kk;
+    mask[k] = std::min(x, vmax) - h * h * h * kk / 6.f;
+    zw[k] = z[k] + s[k];
+  }
+  for (int j = 0; j < ny; j++)
+  {
+    for (int i = 1; i < nx - 1; i++) dx[at(i, j)] = 0.5f * (zw[at(i + 1, j)] - zw[at(i - 1, j)]);
+    dx[at(0, j)] = zw[at(1, j)] - zw[at(0, j)];
+    dx[at(nx - 1, j)] = zw[at(nx - 1, j)] - zw[at(nx - 2, j)];
+  }
+  for (int j = 1; j < ny - 1; j++)
+    for (int i = 0; i < nx; i++) dy[at(i, j)] = 0.5f * (zw[at(i, j + 1)] - zw[at(i, j - 1)]);
+  for (int i = 0; i < nx; i++)
+  {
+    dy[at(i, 0)] = zw[at(i, 1)] - zw[at(i, 0)];
+    dy[at(i, ny - 1)] = zw[at(i, ny - 1)] - zw[at(i, ny - 2)];
+  }
+  for (size_t k = 0; k < n; k++) talus[k] = thermal_talus_ratio * std::sqrt(dx[k] * dx[k] + dy[k] * dy[k]);
+  int rc = ref_thermal(zw.data(), nx, ny, talus.data(), iterations, nullptr, nullptr, mask.data());
+  if (rc) return rc;
+  for (size_t k = 0; k < n; k++)
+  {
+    const float d = zw[k] - z[k];
+    s[k] = d > 0.f ? d : 0.f;
   }
   return 0;
 }

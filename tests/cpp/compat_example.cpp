@@ -6,7 +6,7 @@
  * requested solver, writes the results as raw float32 for the test to
  * compare with the oracle.
  *
- * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition>
+ * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition|layer>
  *        nx ny in.f32 out_prefix
  */
 #include <cstdio>
@@ -99,6 +99,13 @@ int main(int argc, char **argv)
   {
     hmap::Array talus(shape, 0.5f / shape.x), depo;
     hmap::gpu::sediment_deposition(z, talus, &depo, 0.02f, 4, 8);
+    write_raw(out + "_z.f32", z);
+    write_raw(out + "_depo.f32", depo);
+  }
+  else if (mode == "layer")
+  {
+    hmap::Array tl(shape, 0.5f / shape.x), tu(shape, 4.f / shape.x), depo;
+    hmap::gpu::sediment_layer(z, tl, tu, 20, true, &depo);
     write_raw(out + "_z.f32", z);
     write_raw(out + "_depo.f32", depo);
   }

@@ -9,6 +9,7 @@ for the CPU by oracle/build_oracle.py and driven by oracle/ref_harness.cpp
 (Jacobi form).  Run in a checkout where the reference tree is present:
 
     python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation] [siblings] [deposition]
+                                     [layer] [snow]
 
 Each .npz holds the inputs, the parameters and the outputs of one case.
 """
@@ -135,8 +136,30 @@ def deposition_cases():
         dict(max_deposition=0.02, iterations=4, thermal_subiterations=8))), out_z=zo, out_depo=depo)
 
 
+def layer_cases():
+    # sediment_layer: about half of the cells steeper than the upper limit
+    for (nx, ny, seed, iters, post) in ((50, 42, 30, 25, True), (37, 29, 33, 15, False)):
+        z = fbm(nx, ny, seed=seed)
+        tl = ((0.5 + fbm(nx, ny, seed=seed + 1)) / nx).astype(np.float32)
+        tu = ((3.0 + 2.0 * fbm(nx, ny, seed=seed + 2)) / nx).astype(np.float32)
+        zo, depo = po.ref_sediment_layer(z, tl, tu, iters, post)
+        _save("sediment_layer_%s" % ("post" if post else "nopost"), z=z, talus_layer=tl, talus_upper_limit=tu,
+              iterations=np.int32(iters), apply_post_filter=np.int32(post), out_z=zo, out_depo=depo)
+
+
+def snow_cases():
+    # snow_simulation's post-filter on a snow cover of about a tenth of the relief
+    nx, ny = 56, 44
+    z = fbm(nx, ny, seed=40)
+    s = (0.08 * fbm(nx, ny, seed=41)).astype(np.float32)
+    so = po.ref_snow_post_filter(z, s, 0.05, 30, 0.2)
+    _save("snow_post_filter", z=z, s=s, snow_depth=np.float32(0.05), iterations=np.int32(30),
+          thermal_talus_ratio=np.float32(0.2), out_s=so)
+
+
 GROUPS = {"thermal": thermal_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases,
-          "siblings": sibling_cases, "deposition": deposition_cases}
+          "siblings": sibling_cases, "deposition": deposition_cases,
+          "layer": layer_cases, "snow": snow_cases}
 
 if __name__ == "__main__":
     if not po.ref_available():

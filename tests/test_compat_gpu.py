@@ -113,6 +113,16 @@ def test_sediment_deposition(gpu, example, tmp_path):
     assert np.array_equal(load("depo"), depo)
 
 
+def test_sediment_layer(gpu, example, tmp_path):
+    z = fbm(80, 64, seed=13)
+    load = _run(example, "layer", z, tmp_path)
+    tl = np.full_like(z, np.float32(0.5) / np.float32(80))
+    tu = np.full_like(z, np.float32(4.0) / np.float32(80))
+    want, depo = po.sediment_layer(z, tl, tu, 20, True)
+    assert np.array_equal(load("z"), want)
+    assert np.array_equal(load("depo"), depo)
+
+
 def test_vpipes(gpu, example, tmp_path):
     z = fbm(96, 64, seed=2)
     load = _run(example, "vpipes", z, tmp_path)

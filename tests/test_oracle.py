@@ -107,6 +107,24 @@ def test_sediment_deposition_golden_bit_exact():
     assert np.array_equal(z, g["out_z"]) and np.array_equal(depo, g["out_depo"])
 
 
+@pytest.mark.parametrize("case", ["sediment_layer_post", "sediment_layer_nopost"])
+def test_sediment_layer_golden_bit_exact(case):
+    g = _load(case)
+    z, depo = po.sediment_layer(g["z"], g["talus_layer"], g["talus_upper_limit"], int(g["iterations"]),
+                                bool(g["apply_post_filter"]))
+    assert np.array_equal(z, g["out_z"]) and np.array_equal(depo, g["out_depo"])
+    # the solve moved material in a good share of the cells
+    assert 0.1 < float((depo != 0).mean()) <= 1.0
+
+
+def test_snow_post_filter_golden_bit_exact():
+    g = _load("snow_post_filter")
+    out = po.snow_post_filter(g["z"], g["s"], float(g["snow_depth"]), int(g["iterations"]),
+                              float(g["thermal_talus_ratio"]))
+    assert np.array_equal(out, g["out_s"])
+    assert (out >= 0).all() and not np.array_equal(out, g["s"])
+
+
 def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))}
     assert {"thermal_uniform", "vpipes_defaults", "vpipes_rain_per_step"} <= names
@@ -253,3 +271,29 @@ def test_fast_water_case_exceeds_staged_radius():
     out = po.vpipes(z0, po.VpipesParams.make(**fast))
     reach = fast["dt"] * np.maximum(np.abs(out[3]), np.abs(out[4]))
     assert float(reach.max()) > 3.5
+
+
+@ref_only
+@pytest.mark.parametrize("shape", [(41, 53), (40, 52), (3, 3), (4, 6), (7, 5)])
+def test_sediment_layer_matches_reference_text(shape):
+    ny, nx = shape
+    z = fbm(nx, ny, seed=31) if min(shape) > 8 else np.random.RandomState(31).rand(ny, nx).astype(np.float32)
+    tl = np.full_like(z, 0.5 / nx)
+    tu = ((3.0 + 2.0 * fbm(nx, ny, seed=32)) / nx).astype(np.float32)
+    for post in (True, False):
+        a, da = po.sediment_layer(z, tl, tu, 12, post)
+        b, db = po.ref_sediment_layer(z, tl, tu, 12, post)
+        assert np.array_equal(a, b) and np.array_equal(da, db)
+
+
+@ref_only
+@pytest.mark.parametrize("shape", [(41, 53), (3, 3), (4, 6)])
+def test_snow_post_filter_matches_reference_text(shape):
+    ny, nx = shape
+    rs = np.random.RandomState(35)
+    z = fbm(nx, ny, seed=35) if min(shape) > 8 else rs.rand(ny, nx).astype(np.float32)
+    s = (0.1 * rs.rand(ny, nx)).astype(np.float32)
+    for ratio in (0.2, 1.0):
+        a = po.snow_post_filter(z, s, 0.05, 15, ratio)
+        b = po.ref_snow_post_filter(z, s, 0.05, 15, ratio)
+        assert np.array_equal(a, b)
