@@ -598,8 +598,9 @@ def run_extras(a):
     """thermal_auto_bedrock (talus map, 500 iterations), flow_simulation
     (depth map, 1000 iterations, reference defaults), sediment_deposition
     (20 layers x 25 steps), sediment_layer and the snow post-filter (500
-    steps each) and the sibling talus stencils ridge, scree (zmax = z +
-    0.25), schott and olsen (200 iterations each) on the 4096^2 inputs:
+    steps each), the sibling talus stencils ridge, scree (zmax = z +
+    0.25), schott and olsen and the relatives flatten, inflate and rib (200
+    iterations each) on the 4096^2 inputs:
     device-timed cell-updates/s against the HBM roofline, and the
     reference's kernel text on the host cores on a bounded sample (a few
     iterations on the full grid, scaled)."""
@@ -707,6 +708,24 @@ def run_extras(a):
         rows[name] = {"iterations": 200, "cell_updates_per_s": rate, "bytes_per_cell_update": bpc,
                       "gb_per_s": rate * bpc / 1e9, "frac": rate * bpc / 1e9 / peak, "peak": peak,
                       "peak_kind": peak_kind}
+    # thermal_flatten (sigma_inf 0.5, sigma_sup 0.2), thermal_inflate and
+    # thermal_rib, 200 iterations each (rib: no talus read)
+    rel = (("thermal_flatten", G.FLATTEN, 12.0), ("thermal_inflate", G.INFLATE, 12.0), ("thermal_rib", G.RIB, 8.0))
+    for name, rule, bpc in rel:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for rep in range(a.warmup + 1):
+            zt.copy_(zd)
+            torch.cuda.synchronize()
+            e0.record()
+            G.thermal_relief_device(rule, zt, td if rule != G.RIB else None, 200, 0.5, 0.2, ctx=ctx)
+            e1.record()
+            torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+        rate = cells * 200 / t
+        rows[name] = {"iterations": 200, "cell_updates_per_s": rate, "bytes_per_cell_update": bpc,
+                      "gb_per_s": rate * bpc / 1e9, "frac": rate * bpc / 1e9 / peak, "peak": peak,
+                      "peak_kind": peak_kind}
     # the reference's kernel text on the host cores, a few iterations
     refs = [("thermal_auto_bedrock", lambda k: po.ref_thermal_auto_bedrock(z, talus, k)),
             ("flow_simulation", lambda k: po.ref_flow_simulation(z, 0.01, depth_map, k))]
@@ -715,9 +734,11 @@ def run_extras(a):
     refs.append(("sediment_deposition", lambda k: po.ref_sediment_deposition(z, talus, 0.01, 1, k)))
     refs.append(("sediment_layer", lambda k: po.ref_sediment_layer(z, talus, upper, k, True)))
     refs.append(("snow_post_filter", lambda k: po.ref_snow_post_filter(z, snow, 0.05, k, 0.2)))
+    for name, rule, _ in rel:
+        refs.append((name, lambda k, rule=rule: po.ref_thermal_relief(rule, z, talus, k, 0.5, 0.2)))
     for name, fn in refs:
         fn(1)
-        k = 4 if name in ("flow_simulation", "thermal_olsen") else 8
+        k = 4 if name in ("flow_simulation", "thermal_olsen", "thermal_flatten") else 8
         t0 = time.perf_counter()
         fn(k)
         t = time.perf_counter() - t0

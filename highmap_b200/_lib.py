@@ -33,6 +33,7 @@ EXPORTED = (
     "hm_thermal_ridge", "hm_thermal_scree", "hm_thermal_schott", "hm_thermal_olsen", "hm_thermal_stencil_device",
     "hm_sediment_deposition", "hm_sediment_deposition_device", "hm_sediment_layer", "hm_sediment_layer_device",
     "hm_snow_post_filter", "hm_snow_post_filter_device",
+    "hm_thermal_flatten", "hm_thermal_inflate", "hm_thermal_rib", "hm_thermal_relief_device",
     "hm_vpipes_default_params", "hm_vpipes", "hm_vpipes_device",
     "hm_launch_count", "hm_launch_count_reset",
     "hm_thermal_device_noalloc", "hm_vpipes_set_launch", "hm_thermal_set_launch",
@@ -132,6 +133,10 @@ def _declare(lib):
     lib.hm_sediment_layer_device.argtypes = [vp, vp, i, i, vp, vp, i, i, vp, vp]
     lib.hm_snow_post_filter.argtypes = [vp, vp, vp, i, i, f, i, f]
     lib.hm_snow_post_filter_device.argtypes = [vp, vp, vp, i, i, f, i, f, vp]
+    lib.hm_thermal_flatten.argtypes = [vp, vp, i, i, vp, i, f, f, vp]
+    lib.hm_thermal_inflate.argtypes = [vp, vp, i, i, vp, i, vp]
+    lib.hm_thermal_rib.argtypes = [vp, vp, i, i, i, vp]
+    lib.hm_thermal_relief_device.argtypes = [vp, i, vp, i, i, vp, f, f, i, vp, vp]
     lib.hm_thermal_scree.argtypes = [vp, vp, i, i, vp, vp, i, vp, vp]
     lib.hm_thermal_schott.argtypes = [vp, vp, i, i, vp, i, f, vp, vp]
     lib.hm_thermal_olsen.argtypes = [vp, vp, i, i, vp, i, vp]

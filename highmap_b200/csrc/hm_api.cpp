@@ -151,7 +151,7 @@ int hm_thermal_auto_bedrock_device(hm_context *ctx, float *z, int nx, int ny, co
 namespace
 {
 int sibling_host(hm_context *ctx, int rule, float *z, int nx, int ny, const float *talus, const float *zmax,
-                 float intensity, int iterations, float *depo, const float *mask)
+                 float intensity, int iterations, float *depo, const float *mask, float p1 = 0.f)
 {
   hm::clear_error();
   if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: ctx is NULL");
@@ -160,23 +160,23 @@ int sibling_host(hm_context *ctx, int rule, float *z, int nx, int ny, const floa
   if ((st = hm::use_device(ctx->device))) return st;
   const size_t n = (size_t)nx * ny;
   const size_t nbytes = n * sizeof(float);
-  size_t       fields = 2 + (zmax ? 1 : 0) + (depo ? 1 : 0) + (mask ? 1 : 0);
+  size_t       fields = 1 + (talus ? 1 : 0) + (zmax ? 1 : 0) + (depo ? 1 : 0) + (mask ? 1 : 0);
   size_t total = fields * align_up(nbytes, 256) + align_up(hm::thermal_scratch_floats(nx, ny, true) * 4, 256);
   void  *ws = nullptr;
   if ((st = hm::workspace(ctx, total, &ws))) return st;
   Slab         sl{(char *)ws};
   float       *dz = sl.take(n);
-  float       *dt = sl.take(n);
+  float       *dt = talus ? sl.take(n) : nullptr;
   float       *dzm = zmax ? sl.take(n) : nullptr;
   float       *dd = depo ? sl.take(n) : nullptr;
   float       *dm = mask ? sl.take(n) : nullptr;
   float       *scr = sl.take(hm::thermal_scratch_floats(nx, ny, true));
   cudaStream_t s = ctx->stream;
   HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
-  HM_CUDA_TRY(cudaMemcpyAsync(dt, talus, nbytes, cudaMemcpyHostToDevice, s));
+  if (dt) HM_CUDA_TRY(cudaMemcpyAsync(dt, talus, nbytes, cudaMemcpyHostToDevice, s));
   if (dzm) HM_CUDA_TRY(cudaMemcpyAsync(dzm, zmax, nbytes, cudaMemcpyHostToDevice, s));
   if (dm) HM_CUDA_TRY(cudaMemcpyAsync(dm, mask, nbytes, cudaMemcpyHostToDevice, s));
-  st = hm::sibling_core(ctx->device, rule, dz, nx, ny, dt, dzm, intensity, iterations, dd, dm, scr, s);
+  st = hm::sibling_core(ctx->device, rule, dz, nx, ny, dt, dzm, intensity, iterations, dd, dm, scr, s, p1);
   if (st)
   {
     cudaStreamSynchronize(s);
@@ -396,6 +396,9 @@ int hm_thermal_stencil_device(hm_context *ctx, int rule, float *z, int nx, int n
 {
   hm::clear_error();
   if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_stencil_device: ctx is NULL");
+  if (rule > HM_OLSEN)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_stencil_device: rules above HM_OLSEN go through "
+                                             "hm_thermal_relief_device");
   int st = hm::sibling_check_args(rule, z, nx, ny, talus, zmax, iterations);
   if (st) return st;
   if ((st = hm::use_device(ctx->device))) return st;
@@ -521,6 +524,41 @@ int hm_vpipes_device(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_
   void *ws = nullptr;
   if ((st = hm::workspace(ctx, hm::vpipes_scratch_bytes(nx, ny), &ws))) return st;
   return hm::vpipes_core(z, nx, ny, p, rain_map, water_depth, sediment, vel_u, vel_v, ws, (cudaStream_t)stream);
+}
+
+
+int hm_thermal_flatten(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
+                       float sigma_inf, float sigma_sup, const float *mask)
+{
+  return sibling_host(ctx, HM_FLATTEN, z, nx, ny, talus, nullptr, sigma_inf, iterations, nullptr, mask, sigma_sup);
+}
+
+int hm_thermal_inflate(hm_context *ctx, float *z, int nx, int ny, const float *talus, int iterations,
+                       const float *mask)
+{
+  return sibling_host(ctx, HM_INFLATE, z, nx, ny, talus, nullptr, 0.f, iterations, nullptr, mask);
+}
+
+int hm_thermal_rib(hm_context *ctx, float *z, int nx, int ny, int iterations, const float *mask)
+{
+  return sibling_host(ctx, HM_RIB, z, nx, ny, nullptr, nullptr, 0.f, iterations, nullptr, mask);
+}
+
+int hm_thermal_relief_device(hm_context *ctx, int rule, float *z, int nx, int ny, const float *talus, float sigma_inf,
+                             float sigma_sup, int iterations, const float *mask, void *stream)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_relief_device: ctx is NULL");
+  if (rule < HM_FLATTEN || rule > HM_RIB)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_thermal_relief_device: rule must be HM_FLATTEN .. HM_RIB");
+  const float *t = rule == HM_RIB ? nullptr : talus;
+  int          st = hm::sibling_check_args(rule, z, nx, ny, t, nullptr, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::thermal_scratch_floats(nx, ny, true) * sizeof(float), &ws))) return st;
+  return hm::sibling_core(ctx->device, rule, z, nx, ny, t, nullptr, sigma_inf, iterations, nullptr, mask,
+                          (float *)ws, (cudaStream_t)stream, sigma_sup);
 }
 
 } // extern "C"

@@ -10,6 +10,7 @@
  *   thermal_olsen / _ridge / _schott / _scree  HighMap/src/erosion/thermal_gpu.cpp:221-396
  *   sediment_deposition  HighMap/src/erosion/deposition.cpp:19-66
  *   sediment_layer       HighMap/src/erosion/deposition.cpp:68-113
+ *   thermal_flatten, thermal_inflate, thermal_rib  thermal_gpu.cpp:154-219,249-272
  *   init_opencl      HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134
  * The reference functions return void and report problems only through
  * their logger; here a failed call leaves z untouched, prints the status
@@ -277,6 +278,68 @@ void sediment_layer(Array &z, const Array &talus_layer, const Array &talus_upper
     shape_like(p_deposition_map, z);
     p_deposition_map->vector.swap(depo);
   }
+}
+
+/* thermal_flatten / thermal_inflate / thermal_rib (thermal_gpu.cpp:154-219,
+ * 249-272): talus NULL for rib */
+void relief_impl(int rule, const char *fn, Array &z, const Array *p_mask, const Array *talus, float sigma_inf,
+                 float sigma_sup, int iterations)
+{
+  if (!same_shape(talus, z) || !same_shape(p_mask, z) || z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
+  {
+    report(HM_ERR_INVALID_ARGUMENT, fn);
+    g_err += "arrays of different shapes";
+    return;
+  }
+  hm_context *ctx = context();
+  if (!ctx)
+  {
+    report(HM_ERR_NO_DEVICE, fn);
+    return;
+  }
+  std::vector<float> zw(z.vector);
+  const float       *mp = p_mask ? p_mask->vector.data() : nullptr;
+  int                st;
+  if (rule == HM_FLATTEN)
+    st = hm_thermal_flatten(ctx, zw.data(), z.shape.x, z.shape.y, talus->vector.data(), iterations, sigma_inf,
+                            sigma_sup, mp);
+  else if (rule == HM_INFLATE)
+    st = hm_thermal_inflate(ctx, zw.data(), z.shape.x, z.shape.y, talus->vector.data(), iterations, mp);
+  else
+    st = hm_thermal_rib(ctx, zw.data(), z.shape.x, z.shape.y, iterations, mp);
+  if (!report(st, fn)) return;
+  z.vector.swap(zw);
+}
+
+void thermal_flatten(Array &z, const Array &talus, int iterations, float sigma_inf, float sigma_sup)
+{
+  relief_impl(HM_FLATTEN, "hmap::gpu::thermal_flatten", z, nullptr, &talus, sigma_inf, sigma_sup, iterations);
+}
+
+void thermal_flatten(Array &z, const Array *p_mask, const Array &talus, int iterations, float sigma_inf,
+                     float sigma_sup)
+{
+  relief_impl(HM_FLATTEN, "hmap::gpu::thermal_flatten", z, p_mask, &talus, sigma_inf, sigma_sup, iterations);
+}
+
+void thermal_inflate(Array &z, const Array &talus, int iterations)
+{
+  relief_impl(HM_INFLATE, "hmap::gpu::thermal_inflate", z, nullptr, &talus, 0.f, 0.f, iterations);
+}
+
+void thermal_inflate(Array &z, const Array *p_mask, const Array &talus, int iterations)
+{
+  relief_impl(HM_INFLATE, "hmap::gpu::thermal_inflate", z, p_mask, &talus, 0.f, 0.f, iterations);
+}
+
+void thermal_rib(Array &z, int iterations)
+{
+  relief_impl(HM_RIB, "hmap::gpu::thermal_rib", z, nullptr, nullptr, 0.f, 0.f, iterations);
+}
+
+void thermal_rib(Array &z, const Array *p_mask, int iterations)
+{
+  relief_impl(HM_RIB, "hmap::gpu::thermal_rib", z, p_mask, nullptr, 0.f, 0.f, iterations);
 }
 
 void thermal_olsen(Array &z, const Array &talus, int iterations)

@@ -1,18 +1,22 @@
 /*
  * hm_sibling.cu - the sibling talus stencils of thermal erosion on sm_100a:
- * thermal_ridge, thermal_scree, thermal_schott and thermal_olsen.
+ * thermal_ridge, thermal_scree, thermal_schott, thermal_olsen,
+ * thermal_flatten, thermal_inflate and thermal_rib.
  *
- * Replaces the drivers of HighMap/src/erosion/thermal_gpu.cpp:221-396 and
+ * Replaces the drivers of HighMap/src/erosion/thermal_gpu.cpp:154-396 and
  * the in-place OpenCL kernels thermal_ridge.cl, thermal_scree.cl,
- * thermal_schott.cl and thermal_olsen.cl (Jacobi form: every read sees
+ * thermal_schott.cl, thermal_olsen.cl, thermal_flatten.cl,
+ * thermal_inflate.cl and thermal_rib.cl (Jacobi form: every read sees
  * step t, except a work-item's reads of its own cell, which see its own
  * earlier writes).  After the steps, the thermal finish pass: border
- * extrapolation, the deposition map (|z - z0| for ridge and schott,
- * max(z - z0, 0) for scree, none for olsen) and the mask blend.
+ * extrapolation (3 cells deep for rib), the deposition map (|z - z0| for
+ * ridge and schott, max(z - z0, 0) for scree, none for the others) and
+ * the mask blend.
  *
- * Kernel: k_sibling_step, a 32 x 8 tile per CTA with a 2-cell halo of z in
- * shared memory (olsen reads the neighbours of its neighbours), one cell
- * per thread.  Arithmetic is explicitly rounded, one rounding per
+ * Kernels: the 3 x 3 rules (ridge, scree, schott, inflate, rib) run as
+ * cell rules of the thermal warp sweeps; olsen and flatten, which read the
+ * neighbours of their neighbours, on k_sibling_step, a 32 x 8 tile per CTA
+ * with a 2-cell halo of z in shared memory, one cell per thread.  Arithmetic is explicitly rounded, one rounding per
  * operation as the reference's fp32 text; division by the diagonal
  * distance 1.414f is the exact Markstein form of hm_thermal_math.cuh.
  */
@@ -87,6 +91,16 @@ struct SiblingRule
       }
       return __fadd_rn(c, __fmul_rn(__fmul_rn(intensity, t), (float)(up - down)));
     }
+    if (RULE == HM_RIB)
+    {
+      /* thermal_rib.cl: z -= the least |slope| to a neighbour */
+      float delta_min = FLT_MAX;
+#pragma unroll
+      for (int k = 0; k < 8; k++) delta_min = fminf(delta_min, fabsf(slope(c, z8[k], k >= 4)));
+      return __fsub_rn(c, delta_min);
+    }
+    /* ridge sums the slopes down to the neighbours, scree and inflate the
+     * slopes up */
     float sum = 0.f, slope_max = 0.f;
 #pragma unroll
     for (int k = 0; k < 8; k++)
@@ -111,8 +125,8 @@ __global__ void __launch_bounds__(SS_NT)
   const int wx = (blockIdx.x * (SS_NT / 32) + (threadIdx.x >> 5)) * 32;
   if (wx >= nx) return; /* the whole warp */
   const int y0 = blockIdx.y * SS_H;
-  thermal_sweep_warp<true, SiblingRule<RULE>>(a, b, nx, ny, talus, 0.f, zmax, 0, wx, y0, min(ny, y0 + SS_H),
-                                              intensity);
+  thermal_sweep_warp<RULE != HM_RIB, SiblingRule<RULE>>(a, b, nx, ny, talus, 0.f, zmax, 0, wx, y0,
+                                                         min(ny, y0 + SS_H), intensity);
 }
 
 template <int RULE>
@@ -123,11 +137,12 @@ __global__ void __launch_bounds__(SS2_NT)
   const int wx = (blockIdx.x * (SS2_NT / 32) + (threadIdx.x >> 5)) * 64;
   if (wx >= nx) return; /* the whole warp */
   const int y0 = blockIdx.y * SS_H;
-  thermal_sweep2_warp<true, SiblingRule<RULE>>(a, b, nx, ny, talus, 0.f, zmax, 0, wx, y0, min(ny, y0 + SS_H),
-                                               intensity);
+  thermal_sweep2_warp<RULE != HM_RIB, SiblingRule<RULE>>(a, b, nx, ny, talus, 0.f, zmax, 0, wx, y0,
+                                                          min(ny, y0 + SS_H), intensity);
 }
 
-/* thermal_olsen: radius-2 reads, a shared-memory tile per CTA */
+/* thermal_olsen and thermal_flatten: radius-2 reads, a shared-memory tile
+ * per CTA (intensity: flatten's sigma_inf, p1 its sigma_sup) */
 template <int RULE>
 __global__ void __launch_bounds__(SB_TX *SB_TY)
     k_sibling_step(const float *__restrict__ a,
@@ -136,7 +151,8 @@ __global__ void __launch_bounds__(SB_TX *SB_TY)
                    int ny,
                    const float *__restrict__ talus,
                    const float *__restrict__ zmax,
-                   float intensity)
+                   float intensity,
+                   float p1)
 {
   __shared__ float t[SB_TY + 2 * SB_H][SB_TX + 2 * SB_H];
   const int x0 = blockIdx.x * SB_TX, y0 = blockIdx.y * SB_TY;
@@ -208,6 +224,64 @@ __global__ void __launch_bounds__(SB_TX *SB_TY)
     return;
   }
 
+  if (RULE == HM_FLATTEN)
+  {
+    /* apply_boundaries_buffer(z, i, j, nx, ny, 2), _common_index.cl:134-152 */
+    const int bw = 2;
+    if (!(i >= bw && i < nx - bw && j >= bw && j < ny - bw))
+    {
+      const int ci = min(max(i, bw), nx - bw - 1), cj = min(max(j, bw), ny - bw - 1);
+      b[idx] = __ldg(a + (size_t)cj * nx + ci);
+      return;
+    }
+    /* thermal_flatten.cl: neighbours visited from a rotating start
+     * (i + j) % 8, the first strict maximum kept; the cell loses sigma_inf
+     * (below its talus) or sigma_sup (above) times its steepest descent and
+     * gains half of each neighbour's steepest descent that points at it
+     * and lies below that neighbour's talus */
+    /* HMAP_DI / HMAP_DJ + 1 packed two bits per direction: the rotated
+     * directions are decoded with shifts instead of an indexed local array */
+    constexpr unsigned DI1 = 0xA094u, DJ1 = 0x8849u;
+    auto        ddi = [](int k) { return (int)((DI1 >> (2 * k)) & 3u) - 1; };
+    auto        ddj = [](int k) { return (int)((DJ1 >> (2 * k)) & 3u) - 1; };
+    const int   rot = (i + j) % 8;
+    const float zc = zat(0, 0);
+    const float tc = __ldg(talus + idx);
+    const float slope_min = __fdiv_rn(0.f, (float)nx);
+    float       delta = 0.f, dmax = 0.f;
+    for (int n = 0; n < 8; ++n)
+    {
+      const int   k = (n + rot) & 7;
+      const float dz = slope(zc, zat(ddi(k), ddj(k)), k >= 4);
+      if (dz > dmax) dmax = dz;
+    }
+    const float excess = fmaxf(__fsub_rn(dmax, slope_min), 0.f);
+    if (dmax < tc) delta = __fsub_rn(delta, __fmul_rn(intensity, excess));
+    if (dmax > tc) delta = __fsub_rn(delta, __fmul_rn(p1, excess));
+    for (int n = 0; n < 8; ++n)
+    {
+      const int   k = (n + rot) & 7;
+      const int   px = -ddi(k), py = -ddj(k);
+      const float zp = zat(px, py);
+      float       dm = 0.f;
+      int         ka = -1;
+      for (int m = 0; m < 8; ++m)
+      {
+        const int   kk = (m + rot) & 7;
+        const float dz = slope(zp, zat(px + ddi(kk), py + ddj(kk)), kk >= 4);
+        if (dz > dm)
+        {
+          dm = dz;
+          ka = kk;
+        }
+      }
+      if (ka == k && dm > 0.f && dm < __ldg(talus + (size_t)(j + py) * nx + (i + px)))
+        delta = __fadd_rn(delta, __fmul_rn(0.5f, dm));
+    }
+    b[idx] = __fadd_rn(zc, delta);
+    return;
+  }
+
   /* apply_boundaries, _common_index.cl:106-132: x edges first, then y */
   if (i == 0) { b[idx] = zat(1, 0); return; }
   if (i == nx - 1) { b[idx] = zat(-1, 0); return; }
@@ -248,13 +322,16 @@ __global__ void __launch_bounds__(SB_TX *SB_TY)
 
 int sibling_check_args(int rule, const float *z, int nx, int ny, const float *talus, const float *zmax, int iterations)
 {
-  if (rule < HM_RIDGE || rule > HM_OLSEN) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: unknown rule");
-  if (!z || !talus) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: z or talus is NULL");
+  if (rule < HM_RIDGE || rule > HM_RIB) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: unknown rule");
+  if (!z) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: z is NULL");
+  if (!talus && rule != HM_RIB) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: talus is NULL");
   if (rule == HM_SCREE && !zmax) return fail(HM_ERR_INVALID_ARGUMENT, "thermal_scree: zmax is NULL");
-  const int nmin = rule == HM_OLSEN ? 7 : 3;
+  /* olsen's border is 3 cells wide; flatten's 2; rib extrapolates 3 deep */
+  const int nmin = rule == HM_OLSEN ? 7 : (rule == HM_FLATTEN || rule == HM_RIB ? 5 : 3);
   if (nx < nmin || ny < nmin)
-    return fail(HM_ERR_INVALID_ARGUMENT, rule == HM_OLSEN ? "thermal_olsen: nx and ny must be >= 7"
-                                                          : "thermal stencil: nx and ny must be >= 3");
+    return fail(HM_ERR_INVALID_ARGUMENT, rule == HM_OLSEN   ? "thermal_olsen: nx and ny must be >= 7"
+                                         : nmin == 5        ? "thermal_flatten / thermal_rib: nx and ny must be >= 5"
+                                                            : "thermal stencil: nx and ny must be >= 3");
   if ((long long)nx * (long long)ny > (1ll << 34))
     return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: grid larger than 2^34 cells");
   if (iterations < 0) return fail(HM_ERR_INVALID_ARGUMENT, "thermal stencil: iterations < 0");
@@ -263,12 +340,12 @@ int sibling_check_args(int rule, const float *z, int nx, int ny, const float *ta
 
 int sibling_core(int device, int rule, float *z, int nx, int ny, const float *talus, const float *zmax,
                  float intensity, int iterations, float *depo, const float *mask, float *scratch_buf,
-                 cudaStream_t s)
+                 cudaStream_t s, float p1)
 {
   const size_t n = (size_t)nx * ny;
   float       *tmp = scratch_buf;
   float       *z0 = scratch_buf + align_up(n, 64);
-  const bool   want_depo = depo && rule != HM_OLSEN;
+  const bool   want_depo = depo && rule <= HM_SCHOTT;
   if (want_depo || mask) HM_CUDA_TRY(cudaMemcpyAsync(z0, z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
   const dim3   grid((nx + SB_TX - 1) / SB_TX, (ny + SB_TY - 1) / SB_TY), block(SB_TX, SB_TY);
   const float *src = z;
@@ -287,7 +364,10 @@ int sibling_core(int device, int rule, float *z, int nx, int ny, const float *ta
     case HM_RIDGE: HM_SIB_SWEEP(HM_RIDGE) break;
     case HM_SCREE: HM_SIB_SWEEP(HM_SCREE) break;
     case HM_SCHOTT: HM_SIB_SWEEP(HM_SCHOTT) break;
-    default: k_sibling_step<HM_OLSEN><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity);
+    case HM_INFLATE: HM_SIB_SWEEP(HM_INFLATE) break;
+    case HM_RIB: HM_SIB_SWEEP(HM_RIB) break;
+    case HM_FLATTEN: k_sibling_step<HM_FLATTEN><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity, p1); break;
+    default: k_sibling_step<HM_OLSEN><<<grid, block, 0, s>>>(src, dst, nx, ny, talus, zmax, intensity, p1);
     }
 #undef HM_SIB_SWEEP
     HM_LAUNCH_CHECK("k_sibling_step");
@@ -296,7 +376,8 @@ int sibling_core(int device, int rule, float *z, int nx, int ny, const float *ta
     dst = const_cast<float *>(t);
   }
   if (src != z) HM_CUDA_TRY(cudaMemcpyAsync(z, src, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-  return thermal_finish(device, z, nx, ny, z0, want_depo ? depo : nullptr, mask, s, rule != HM_SCREE);
+  return thermal_finish(device, z, nx, ny, z0, want_depo ? depo : nullptr, mask, s, rule != HM_SCREE,
+                        rule == HM_RIB ? 3 : 1);
 }
 
 } // namespace hm

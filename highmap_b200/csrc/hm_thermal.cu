@@ -221,6 +221,32 @@ __global__ void __launch_bounds__(1024) k_extrapolate(float *z, int nx, int ny)
   }
 }
 
+/* extrapolate_borders(z, nb, 0) for nb > 1 (boundary.cpp:19-41): per row,
+ * for k = nb-1 .. 0, column k from columns k+1, k+2, then column nx-1-k
+ * from its two inward neighbours; then the same per column over the rows.
+ * One thread walks one row (then one column) in the reference's order, so
+ * rows narrower than 2 nb + 2, where the two sides meet, match too. */
+__global__ void __launch_bounds__(1024) k_extrapolate_n(float *z, int nx, int ny, int nb)
+{
+  for (int j = threadIdx.x; j < ny; j += blockDim.x)
+  {
+    float *r = z + (size_t)j * nx;
+    for (int k = nb - 1; k > -1; k--)
+    {
+      r[k] = __fsub_rn(__fmul_rn(2.f, r[k + 1]), r[k + 2]);
+      r[nx - 1 - k] = __fsub_rn(__fmul_rn(2.f, r[nx - 2 - k]), r[nx - 3 - k]);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nx; i += blockDim.x)
+    for (int k = nb - 1; k > -1; k--)
+    {
+      z[(size_t)k * nx + i] = __fsub_rn(__fmul_rn(2.f, z[(size_t)(k + 1) * nx + i]), z[(size_t)(k + 2) * nx + i]);
+      z[(size_t)(ny - 1 - k) * nx + i] =
+          __fsub_rn(__fmul_rn(2.f, z[(size_t)(ny - 2 - k) * nx + i]), z[(size_t)(ny - 3 - k) * nx + i]);
+    }
+}
+
 __global__ void k_thermal_final(float *__restrict__ z,
                                 const float *__restrict__ z0,
                                 float *__restrict__ depo,
@@ -305,14 +331,22 @@ static void step_dispatch(const float *a, float *b, int nx, int ny, const float 
 }
 
 /* post-processing of a finished thermal solve (z holds the last step):
- * border extrapolation, then the deposition map (max(z - z0, 0), or
+ * border extrapolation (nbuffer cells deep), then the deposition map (max(z - z0, 0), or
  * |z - z0| with depo_abs) and the mask blend when asked (z0 = the input
  * heights) */
 int thermal_finish(int device, float *z, int nx, int ny, const float *z0, float *depo, const float *mask,
-                   cudaStream_t s, bool depo_abs)
+                   cudaStream_t s, bool depo_abs, int nbuffer)
 {
-  k_extrapolate<<<1, 1024, 0, s>>>(z, nx, ny);
-  HM_LAUNCH_CHECK("k_extrapolate");
+  if (nbuffer > 1)
+  {
+    k_extrapolate_n<<<1, 1024, 0, s>>>(z, nx, ny, nbuffer);
+    HM_LAUNCH_CHECK("k_extrapolate_n");
+  }
+  else
+  {
+    k_extrapolate<<<1, 1024, 0, s>>>(z, nx, ny);
+    HM_LAUNCH_CHECK("k_extrapolate");
+  }
   if (depo || mask)
   {
     k_thermal_final<<<num_sms(device) * 8, 256, 0, s>>>(z, z0, depo, mask, (size_t)nx * ny, depo_abs ? 1 : 0);

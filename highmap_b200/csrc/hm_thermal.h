@@ -18,7 +18,7 @@ int    thermal_core(int device, float *z, int nx, int ny, const float *talus, fl
                     float *scratch_buf, cudaStream_t s, bool auto_bed = false);
 /* border extrapolation, deposition map and mask blend after the steps */
 int    thermal_finish(int device, float *z, int nx, int ny, const float *z0, float *depo, const float *mask,
-                      cudaStream_t s, bool depo_abs = false);
+                      cudaStream_t s, bool depo_abs = false, int nbuffer = 1);
 /* sediment_deposition (hm_deposition.cu): device pointers, ordered on s */
 size_t deposition_scratch_floats(int nx, int ny);
 int    deposition_core(int device, float *z, int nx, int ny, const float *talus, float max_deposition,
@@ -34,14 +34,15 @@ int    layer_core(int device, float *z, int nx, int ny, const float *talus_layer
 size_t snow_scratch_floats(int nx, int ny);
 int    snow_post_filter_core(int device, const float *z, float *s, int nx, int ny, float snow_depth, int iterations,
                              float ratio, float *scratch, cudaStream_t st);
-/* sibling talus stencils (hm_sibling.cu): rule HM_RIDGE .. HM_OLSEN; zmax
- * for scree, intensity for schott; scratch of thermal_scratch_floats(nx,
+/* sibling talus stencils (hm_sibling.cu): rule HM_RIDGE .. HM_RIB; zmax
+ * for scree, intensity for schott, intensity and p1 (sigma_inf, sigma_sup)
+ * for flatten; talus NULL for rib; scratch of thermal_scratch_floats(nx,
  * ny, true) floats */
 int    sibling_check_args(int rule, const float *z, int nx, int ny, const float *talus, const float *zmax,
                           int iterations);
 int    sibling_core(int device, int rule, float *z, int nx, int ny, const float *talus, const float *zmax,
                     float intensity, int iterations, float *depo, const float *mask, float *scratch_buf,
-                    cudaStream_t s);
+                    cudaStream_t s, float p1 = 0.f);
 } // namespace hm
 
 #endif

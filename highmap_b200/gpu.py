@@ -238,6 +238,7 @@ def snow_post_filter_device(z, s, snow_depth: float, iterations: int, thermal_ta
 
 
 RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
+FLATTEN, INFLATE, RIB = 4, 5, 6
 
 
 def _sibling_host(z, talus, deposition_map, mask):
@@ -299,6 +300,43 @@ def thermal_stencil_device(rule: int, z, talus, iterations: int = 10, zmax=None,
                                               C.c_float(intensity), int(iterations),
                                               _tptr(deposition_map, "deposition_map", z.shape),
                                               _tptr(mask, "mask", z.shape), _stream(stream)))
+
+
+def thermal_flatten(z: np.ndarray, talus: np.ndarray, iterations: int, sigma_inf: float = 0.5,
+                    sigma_sup: float = 0.0, mask: np.ndarray | None = None, ctx: Context | None = None) -> None:
+    """hmap::gpu::thermal_flatten (thermal_gpu.cpp:154-190), in place."""
+    nx, ny = _sibling_host(z, talus, None, mask)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_flatten(ctx.handle, _ptr(z), nx, ny, _ptr(talus), int(iterations),
+                                       C.c_float(sigma_inf), C.c_float(sigma_sup), _ptr(mask)))
+
+
+def thermal_inflate(z: np.ndarray, talus: np.ndarray, iterations: int = 10, mask: np.ndarray | None = None,
+                    ctx: Context | None = None) -> None:
+    """hmap::gpu::thermal_inflate (thermal_gpu.cpp:192-219), in place."""
+    nx, ny = _sibling_host(z, talus, None, mask)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_inflate(ctx.handle, _ptr(z), nx, ny, _ptr(talus), int(iterations), _ptr(mask)))
+
+
+def thermal_rib(z: np.ndarray, iterations: int, mask: np.ndarray | None = None, ctx: Context | None = None) -> None:
+    """hmap::gpu::thermal_rib (thermal_gpu.cpp:249-272), in place."""
+    _grid(z, "z", writable=True)
+    ny, nx = z.shape
+    if mask is not None:
+        _grid(mask, "mask", z.shape)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_rib(ctx.handle, _ptr(z), nx, ny, int(iterations), _ptr(mask)))
+
+
+def thermal_relief_device(rule: int, z, talus=None, iterations: int = 10, sigma_inf: float = 0.5,
+                          sigma_sup: float = 0.0, mask=None, ctx: Context | None = None, stream=None) -> None:
+    ny, nx = z.shape
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_thermal_relief_device(ctx.handle, int(rule), _tptr(z, "z"), nx, ny,
+                                             _tptr(talus, "talus", z.shape), C.c_float(sigma_inf),
+                                             C.c_float(sigma_sup), int(iterations), _tptr(mask, "mask", z.shape),
+                                             _stream(stream)))
 
 
 def flow_simulation(z: np.ndarray, water_height: float, depth_map: np.ndarray, iterations: int, dt: float = 0.5,

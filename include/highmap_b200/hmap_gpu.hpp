@@ -90,6 +90,23 @@ void sediment_layer(Array       &z,
                     bool         apply_post_filter = true,
                     Array       *p_deposition_map = nullptr);
 
+/* HighMap/include/highmap/erosion.hpp:1855-1866, 1911-1916, 1930-1932 */
+void thermal_flatten(Array       &z,
+                     const Array &talus,
+                     int          iterations,
+                     float        sigma_inf = 0.5f,
+                     float        sigma_sup = 0.f);
+void thermal_flatten(Array       &z,
+                     const Array *p_mask,
+                     const Array &talus,
+                     int          iterations,
+                     float        sigma_inf = 0.5f,
+                     float        sigma_sup = 0.f);
+void thermal_inflate(Array &z, const Array &talus, int iterations = 10);
+void thermal_inflate(Array &z, const Array *p_mask, const Array &talus, int iterations = 10);
+void thermal_rib(Array &z, int iterations);
+void thermal_rib(Array &z, const Array *p_mask, int iterations);
+
 /* sibling talus stencils, HighMap/include/highmap/erosion.hpp:1887-2028 */
 void thermal_olsen(Array &z, const Array &talus, int iterations);
 

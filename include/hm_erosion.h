@@ -300,11 +300,15 @@ int hm_snow_post_filter_device(hm_context  *ctx,
 
 /* ---- sibling talus stencils ---------------------------------------------- */
 
-/* Rules of hm_thermal_stencil_device. */
+/* Rules of hm_thermal_stencil_device (ridge .. olsen) and
+ * hm_thermal_relief_device (flatten .. rib). */
 #define HM_RIDGE 0
 #define HM_SCREE 1
 #define HM_SCHOTT 2
 #define HM_OLSEN 3
+#define HM_FLATTEN 4
+#define HM_INFLATE 5
+#define HM_RIB 6
 
 /* Replaces hmap::gpu::thermal_ridge(Array &z, const Array &talus,
  * int iterations, Array *p_deposition_map) and its masked overload
@@ -375,6 +379,60 @@ int hm_thermal_stencil_device(hm_context  *ctx,
                               float       *deposition_map,
                               const float *mask,
                               void        *stream);
+
+/* Replaces hmap::gpu::thermal_flatten(Array &z, const Array &talus,
+ * int iterations, float sigma_inf, float sigma_sup) and its masked overload
+ * (HighMap/include/highmap/erosion.hpp:1855-1866,
+ *  HighMap/src/erosion/thermal_gpu.cpp:154-190, kernel thermal_flatten.cl):
+ * a cell loses sigma_inf (slope below its talus) or sigma_sup (above)
+ * times its steepest descent and gains half of each neighbour's steepest
+ * descent that points at it; border cells within 2 of the edge copy the
+ * nearest interior cell; then extrapolate_borders; with a mask
+ * z = lerp(z, result, mask).  nx, ny >= 5; mask nullable.  The reference's
+ * defaults are sigma_inf 0.5, sigma_sup 0. */
+int hm_thermal_flatten(hm_context  *ctx,
+                       float       *z,
+                       int          nx,
+                       int          ny,
+                       const float *talus,
+                       int          iterations,
+                       float        sigma_inf,
+                       float        sigma_sup,
+                       const float *mask);
+
+/* Replaces hmap::gpu::thermal_inflate(Array &z, const Array &talus,
+ * int iterations) and its masked overload (erosion.hpp:1911-1916,
+ * thermal_gpu.cpp:192-219, kernel thermal_inflate.cl), then
+ * extrapolate_borders and the mask blend.  mask nullable. */
+int hm_thermal_inflate(hm_context  *ctx,
+                       float       *z,
+                       int          nx,
+                       int          ny,
+                       const float *talus,
+                       int          iterations,
+                       const float *mask);
+
+/* Replaces hmap::gpu::thermal_rib(Array &z, int iterations) and its masked
+ * overload (erosion.hpp:1930-1932, thermal_gpu.cpp:249-272, kernel
+ * thermal_rib.cl): each cell drops by its least |slope| to a neighbour;
+ * then extrapolate_borders(z, 3) and the mask blend.  nx, ny >= 5; mask
+ * nullable. */
+int hm_thermal_rib(hm_context *ctx, float *z, int nx, int ny, int iterations, const float *mask);
+
+/* The three on device buffers, ordered on `stream`: rule HM_FLATTEN,
+ * HM_INFLATE or HM_RIB; talus unused (may be NULL) for rib; sigma_inf and
+ * sigma_sup used by flatten only; mask nullable. */
+int hm_thermal_relief_device(hm_context  *ctx,
+                             int          rule,
+                             float       *z,
+                             int          nx,
+                             int          ny,
+                             const float *talus,
+                             float        sigma_inf,
+                             float        sigma_sup,
+                             int          iterations,
+                             const float *mask,
+                             void        *stream);
 
 /* ---- flow simulation ---------------------------------------------------- */
 

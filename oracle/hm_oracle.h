@@ -162,6 +162,30 @@ int hmo_sediment_layer_f64(double       *z,
                            int           apply_post_filter,
                            double       *deposition_map);
 
+/* thermal_flatten (rule 4; sigma_inf, sigma_sup), thermal_inflate (rule 5)
+ * and thermal_rib (rule 6; talus unused, may be NULL),
+ * HighMap/src/erosion/thermal_gpu.cpp:154-219,249-272, Jacobi form; mask:
+ * apply_with_mask blend, nullable.  No deposition maps (the reference
+ * functions have none). */
+int hmo_thermal_relief_f32(int          rule,
+                           float       *z,
+                           int          nx,
+                           int          ny,
+                           const float *talus,
+                           float        sigma_inf,
+                           float        sigma_sup,
+                           int          iterations,
+                           const float *mask);
+int hmo_thermal_relief_f64(int           rule,
+                           double       *z,
+                           int           nx,
+                           int           ny,
+                           const double *talus,
+                           double        sigma_inf,
+                           double        sigma_sup,
+                           int           iterations,
+                           const double *mask);
+
 /* snow_simulation's post-filter (HighMap/src/hydrology/snow_simulation.cpp:
  * 140-152, then its clamp_min(s, 0)): z the terrain, s the snow depth,
  * updated in place. */

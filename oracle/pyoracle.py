@@ -231,6 +231,37 @@ def ref_snow_post_filter(z, s, snow_depth, iterations, thermal_talus_ratio):
     return s
 
 
+FLATTEN, INFLATE, RIB = 4, 5, 6
+
+
+def thermal_relief(rule, z, talus=None, iterations=10, sigma_inf=0.5, sigma_sup=0.0, mask=None, dtype=np.float32):
+    """Oracle thermal_flatten (rule 4) / thermal_inflate (5) / thermal_rib (6)
+    (thermal_gpu.cpp:154-219,249-272); returns z."""
+    z = _grid(z, dtype).copy()
+    ny, nx = z.shape
+    talus = None if talus is None else _grid(talus, dtype)
+    mask = None if mask is None else _grid(mask, dtype)
+    fn = _lib().hmo_thermal_relief_f32 if dtype == np.float32 else _lib().hmo_thermal_relief_f64
+    S = C.c_float if dtype == np.float32 else C.c_double
+    rc = fn(int(rule), _p(z), nx, ny, _p(talus), S(sigma_inf), S(sigma_sup), int(iterations), _p(mask))
+    if rc:
+        raise ValueError("oracle thermal_relief rejected its arguments (status %d)" % rc)
+    return z
+
+
+def ref_thermal_relief(rule, z, talus=None, iterations=10, sigma_inf=0.5, sigma_sup=0.0, mask=None):
+    """thermal_flatten / _inflate / _rib driven over the reference's kernel text."""
+    z = _grid(z, np.float32).copy()
+    ny, nx = z.shape
+    talus = None if talus is None else _grid(talus, np.float32)
+    mask = None if mask is None else _grid(mask, np.float32)
+    rc = _ref().ref_thermal_relief(int(rule), _p(z), nx, ny, _p(talus), C.c_float(sigma_inf), C.c_float(sigma_sup),
+                                   int(iterations), _p(mask))
+    if rc:
+        raise ValueError("ref thermal_relief rejected its arguments (status %d)" % rc)
+    return z
+
+
 RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
 
 

@@ -17,6 +17,7 @@
  *   ref_sediment_layer : HighMap/src/erosion/deposition.cpp:68-113 (with
  *                        gradient.cpp:217-243 and filters.cpp:290-324)
  *   ref_snow_post_filter : HighMap/src/hydrology/snow_simulation.cpp:140-152
+ *   ref_thermal_relief : HighMap/src/erosion/thermal_gpu.cpp:154-219,249-272
  *
  * Work-items run as a host loop (OpenMP over rows).  The in-place thermal
  * kernels are given a private copy of the three rows around the work-item,
@@ -60,6 +61,14 @@ void thermal_ridge(float *z, const float *talus, const int nx, const int ny);
 void thermal_scree(float *z, const float *talus, const float *zmax, const int nx, const int ny);
 void thermal_schott(float *z, const float *talus, const int nx, const int ny, const float intensity);
 void thermal_olsen(float *z, const float *talus, const int nx, const int ny);
+void thermal_flatten(float       *z,
+                     const float *talus,
+                     const int    nx,
+                     const int    ny,
+                     const float  sigma_inf,
+                     const float  sigma_sup);
+void thermal_inflate(float *z, const float *talus, const int nx, const int ny);
+void thermal_rib(float *z, const int nx, const int ny);
 void hydraulic_vpipes_flow_pass(image2d_t, image2d_t, image2d_t, image2d_t, image2d_t, image2d_t,
                                 image2d_t, image2d_t, image2d_t, image2d_t, const int, const int,
                                 const float, const int, const float);
@@ -90,6 +99,24 @@ void extrapolate_borders(float *z, int ni, int nj)
     at(i, 0) = 2.f * at(i, 1) - at(i, 2);
     at(i, nj - 1) = 2.f * at(i, nj - 2) - at(i, nj - 3);
   }
+}
+
+/* extrapolate_borders(z, nbuffer, sigma = 0), boundary.cpp:19-41 */
+void extrapolate_borders_n(float *z, int ni, int nj, int nb)
+{
+  auto at = [&](int i, int j) -> float & { return z[(long)j * ni + i]; };
+  for (int j = 0; j < nj; j++)
+    for (int k = nb - 1; k > -1; k--)
+    {
+      at(k, j) = 2.f * at(k + 1, j) - at(k + 2, j);
+      at(ni - 1 - k, j) = 2.f * at(ni - 2 - k, j) - at(ni - 3 - k, j);
+    }
+  for (int i = 0; i < ni; i++)
+    for (int k = nb - 1; k > -1; k--)
+    {
+      at(i, k) = 2.f * at(i, k + 1) - at(i, k + 2);
+      at(i, nj - 1 - k) = 2.f * at(i, nj - 2 - k) - at(i, nj - 3 - k);
+    }
 }
 
 /* One launch of an in-place thermal kernel over the nx x ny NDRange,
@@ -562,6 +589,40 @@ int ref_flow_simulation(const float *z,
     }
   }
   std::memcpy(water_depth, d.data(), n * sizeof(float));
+  return 0;
+}
+
+/* thermal_gpu.cpp:154-219,249-272: thermal_flatten (rule 4), thermal_inflate
+ * (rule 5), thermal_rib (rule 6), as hmo_thermal_relief; the masked
+ * overloads via apply_with_mask */
+int ref_thermal_relief(int          rule,
+                       float       *z,
+                       int          nx,
+                       int          ny,
+                       const float *talus,
+                       float        sigma_inf,
+                       float        sigma_sup,
+                       int          iterations,
+                       const float *mask)
+{
+  if (!z || rule < 4 || rule > 6 || iterations < 0 || (rule != 6 && !talus)) return 1;
+  const int nmin = rule == 5 ? 3 : 5;
+  if (nx < nmin || ny < nmin) return 1;
+  const size_t       n = (size_t)nx * ny;
+  std::vector<float> a(z, z + n), b(n);
+  for (int it = 0; it < iterations; it++)
+  {
+    if (rule == 4)
+      run_inplace(a.data(), b.data(), nullptr, nx, ny,
+                  [&](float *zw) { hmref::thermal_flatten(zw, talus, nx, ny, sigma_inf, sigma_sup); }, 2);
+    else if (rule == 5)
+      run_inplace(a.data(), b.data(), nullptr, nx, ny, [&](float *zw) { hmref::thermal_inflate(zw, talus, nx, ny); });
+    else
+      run_inplace(a.data(), b.data(), nullptr, nx, ny, [&](float *zw) { hmref::thermal_rib(zw, nx, ny); });
+    std::swap(a, b);
+  }
+  extrapolate_borders_n(a.data(), nx, ny, rule == 6 ? 3 : 1);
+  for (size_t k = 0; k < n; k++) z[k] = mask ? z[k] * (1.f - mask[k]) + a[k] * mask[k] : a[k];
   return 0;
 }
 

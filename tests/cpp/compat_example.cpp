@@ -6,7 +6,7 @@
  * requested solver, writes the results as raw float32 for the test to
  * compare with the oracle.
  *
- * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition|layer>
+ * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition|layer|flatten|inflate|rib>
  *        nx ny in.f32 out_prefix
  */
 #include <cstdio>
@@ -101,6 +101,14 @@ int main(int argc, char **argv)
     hmap::gpu::sediment_deposition(z, talus, &depo, 0.02f, 4, 8);
     write_raw(out + "_z.f32", z);
     write_raw(out + "_depo.f32", depo);
+  }
+  else if (mode == "flatten" || mode == "inflate" || mode == "rib")
+  {
+    hmap::Array talus(shape, 0.6f / shape.x), mask(shape, 0.5f);
+    if (mode == "flatten") hmap::gpu::thermal_flatten(z, talus, 12, 0.5f, 0.2f);
+    else if (mode == "inflate") hmap::gpu::thermal_inflate(z, &mask, talus, 12);
+    else hmap::gpu::thermal_rib(z, 6);
+    write_raw(out + "_z.f32", z);
   }
   else if (mode == "layer")
   {

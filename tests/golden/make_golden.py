@@ -9,7 +9,7 @@ for the CPU by oracle/build_oracle.py and driven by oracle/ref_harness.cpp
 (Jacobi form).  Run in a checkout where the reference tree is present:
 
     python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation] [siblings] [deposition]
-                                     [layer] [snow]
+                                     [layer] [snow] [relief]
 
 Each .npz holds the inputs, the parameters and the outputs of one case.
 """
@@ -157,9 +157,28 @@ def snow_cases():
           thermal_talus_ratio=np.float32(0.2), out_s=so)
 
 
+def relief_cases():
+    # thermal_flatten (sigma_inf 0.5, sigma_sup 0.2), thermal_inflate, thermal_rib; rib and flatten also masked
+    nx, ny = 52, 38
+    z = fbm(nx, ny, seed=50)
+    talus = ((0.5 + fbm(nx, ny, seed=51)) / nx).astype(np.float32)
+    mask = fbm(nx, ny, seed=52)
+    for name, rule, kw in (("thermal_flatten", po.FLATTEN, dict(sigma_inf=0.5, sigma_sup=0.2)),
+                           ("thermal_inflate", po.INFLATE, {}), ("thermal_rib", po.RIB, {})):
+        for m in (None, mask):
+            if m is not None and rule == po.INFLATE:
+                continue
+            zo = po.ref_thermal_relief(rule, z, talus, 15, mask=m, **kw)
+            arrays = dict(z=z, talus=talus, iterations=np.int32(15), rule=np.int32(rule), out_z=zo,
+                          sigma_inf=np.float32(kw.get("sigma_inf", 0.5)), sigma_sup=np.float32(kw.get("sigma_sup", 0.0)))
+            if m is not None:
+                arrays["mask"] = m
+            _save(name + ("_masked" if m is not None else ""), **arrays)
+
+
 GROUPS = {"thermal": thermal_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases,
           "siblings": sibling_cases, "deposition": deposition_cases,
-          "layer": layer_cases, "snow": snow_cases}
+          "layer": layer_cases, "snow": snow_cases, "relief": relief_cases}
 
 if __name__ == "__main__":
     if not po.ref_available():

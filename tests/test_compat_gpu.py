@@ -123,6 +123,20 @@ def test_sediment_layer(gpu, example, tmp_path):
     assert np.array_equal(load("depo"), depo)
 
 
+@pytest.mark.parametrize("mode", ["flatten", "inflate", "rib"])
+def test_thermal_relief(gpu, example, tmp_path, mode):
+    z = fbm(72, 56, seed=14)
+    load = _run(example, mode, z, tmp_path)
+    talus = np.full_like(z, np.float32(0.6) / np.float32(72))
+    if mode == "flatten":
+        want = po.thermal_relief(po.FLATTEN, z, talus, 12, 0.5, 0.2)
+    elif mode == "inflate":
+        want = po.thermal_relief(po.INFLATE, z, talus, 12, mask=np.full_like(z, 0.5))
+    else:
+        want = po.thermal_relief(po.RIB, z, None, 6)
+    assert np.array_equal(load("z"), want)
+
+
 def test_vpipes(gpu, example, tmp_path):
     z = fbm(96, 64, seed=2)
     load = _run(example, "vpipes", z, tmp_path)

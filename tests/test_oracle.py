@@ -125,6 +125,15 @@ def test_snow_post_filter_golden_bit_exact():
     assert (out >= 0).all() and not np.array_equal(out, g["s"])
 
 
+@pytest.mark.parametrize("case", ["thermal_flatten", "thermal_flatten_masked", "thermal_inflate", "thermal_rib",
+                                  "thermal_rib_masked"])
+def test_thermal_relief_golden_bit_exact(case):
+    g = _load(case)
+    z = po.thermal_relief(int(g["rule"]), g["z"], g["talus"], int(g["iterations"]), float(g["sigma_inf"]),
+                          float(g["sigma_sup"]), mask=g.get("mask"))
+    assert np.array_equal(z, g["out_z"])
+
+
 def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))}
     assert {"thermal_uniform", "vpipes_defaults", "vpipes_rain_per_step"} <= names
@@ -297,3 +306,18 @@ def test_snow_post_filter_matches_reference_text(shape):
         a = po.snow_post_filter(z, s, 0.05, 15, ratio)
         b = po.ref_snow_post_filter(z, s, 0.05, 15, ratio)
         assert np.array_equal(a, b)
+
+
+@ref_only
+@pytest.mark.parametrize("rule", [4, 5, 6])
+@pytest.mark.parametrize("shape", [(41, 53), (5, 5), (6, 9)])
+def test_thermal_relief_matches_reference_text(rule, shape):
+    ny, nx = shape
+    rs = np.random.RandomState(40 + rule)
+    z = fbm(nx, ny, seed=41) if min(shape) > 8 else rs.rand(ny, nx).astype(np.float32)
+    talus = np.full_like(z, 0.6 / nx)
+    mask = rs.rand(ny, nx).astype(np.float32)
+    for m in (None, mask):
+        a = po.thermal_relief(rule, z, talus, 9, 0.5, 0.3, mask=m)
+        b = po.ref_thermal_relief(rule, z, talus, 9, 0.5, 0.3, mask=m)
+        assert np.array_equal(a, b, equal_nan=True)
