@@ -600,7 +600,8 @@ def run_extras(a):
     (20 layers x 25 steps), sediment_layer and the snow post-filter (500
     steps each), the sibling talus stencils ridge, scree (zmax = z +
     0.25), schott and olsen and the relatives flatten, inflate and rib (200
-    iterations each) on the 4096^2 inputs:
+    iterations each) and flow_simulation_viscous (1000 steps) on the 4096^2
+    inputs:
     device-timed cell-updates/s against the HBM roofline, and the
     reference's kernel text on the host cores on a bounded sample (a few
     iterations on the full grid, scaled)."""
@@ -726,6 +727,22 @@ def run_extras(a):
         rows[name] = {"iterations": 200, "cell_updates_per_s": rate, "bytes_per_cell_update": bpc,
                       "gb_per_s": rate * bpc / 1e9, "frac": rate * bpc / 1e9 / peak, "peak": peak,
                       "peak_kind": peak_kind}
+    # flow_simulation_viscous, 1000 steps (depth map, water height 0.01):
+    # 12 B per step (z and the depth read, the depth written; neighbours in
+    # cache), the adaptive time step and the dry-out included
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for rep in range(a.warmup + 1):
+        torch.cuda.synchronize()
+        e0.record()
+        G.flow_simulation_viscous_device(zd, 0.01, dm, 1000, w, 0.5, 0.0, 1.0, 2.5, ctx=ctx)
+        e1.record()
+        torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3
+    rate = cells * 1000 / t
+    rows["flow_simulation_viscous"] = {"iterations": 1000, "cell_updates_per_s": rate, "bytes_per_cell_update": 12.0,
+                                       "gb_per_s": rate * 12.0 / 1e9, "frac": rate * 12.0 / 1e9 / peak, "peak": peak,
+                                       "peak_kind": peak_kind}
     # the reference's kernel text on the host cores, a few iterations
     refs = [("thermal_auto_bedrock", lambda k: po.ref_thermal_auto_bedrock(z, talus, k)),
             ("flow_simulation", lambda k: po.ref_flow_simulation(z, 0.01, depth_map, k))]
@@ -736,9 +753,10 @@ def run_extras(a):
     refs.append(("snow_post_filter", lambda k: po.ref_snow_post_filter(z, snow, 0.05, k, 0.2)))
     for name, rule, _ in rel:
         refs.append((name, lambda k, rule=rule: po.ref_thermal_relief(rule, z, talus, k, 0.5, 0.2)))
+    refs.append(("flow_simulation_viscous", lambda k: po.ref_flow_simulation_viscous(z, 0.01, depth_map, k)))
     for name, fn in refs:
         fn(1)
-        k = 4 if name in ("flow_simulation", "thermal_olsen", "thermal_flatten") else 8
+        k = 4 if name in ("flow_simulation", "thermal_olsen", "thermal_flatten", "flow_simulation_viscous") else 8
         t0 = time.perf_counter()
         fn(k)
         t = time.perf_counter() - t0

@@ -34,6 +34,7 @@ EXPORTED = (
     "hm_sediment_deposition", "hm_sediment_deposition_device", "hm_sediment_layer", "hm_sediment_layer_device",
     "hm_snow_post_filter", "hm_snow_post_filter_device",
     "hm_thermal_flatten", "hm_thermal_inflate", "hm_thermal_rib", "hm_thermal_relief_device",
+    "hm_flow_simulation_viscous", "hm_flow_simulation_viscous_device",
     "hm_vpipes_default_params", "hm_vpipes", "hm_vpipes_device",
     "hm_launch_count", "hm_launch_count_reset",
     "hm_thermal_device_noalloc", "hm_vpipes_set_launch", "hm_thermal_set_launch",
@@ -137,6 +138,8 @@ def _declare(lib):
     lib.hm_thermal_inflate.argtypes = [vp, vp, i, i, vp, i, vp]
     lib.hm_thermal_rib.argtypes = [vp, vp, i, i, i, vp]
     lib.hm_thermal_relief_device.argtypes = [vp, i, vp, i, i, vp, f, f, i, vp, vp]
+    lib.hm_flow_simulation_viscous.argtypes = [vp, vp, i, i, f, vp, i, f, f, f, f, vp]
+    lib.hm_flow_simulation_viscous_device.argtypes = [vp, vp, i, i, f, vp, i, f, f, f, f, vp, vp]
     lib.hm_thermal_scree.argtypes = [vp, vp, i, i, vp, vp, i, vp, vp]
     lib.hm_thermal_schott.argtypes = [vp, vp, i, i, vp, i, f, vp, vp]
     lib.hm_thermal_olsen.argtypes = [vp, vp, i, i, vp, i, vp]

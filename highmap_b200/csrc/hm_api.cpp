@@ -461,6 +461,54 @@ int hm_flow_simulation_device(hm_context *ctx, const float *z, int nx, int ny, f
                                   flux_diffusion_strength, dry_out_ratio, water_depth, ws, (cudaStream_t)stream);
 }
 
+int hm_flow_simulation_viscous(hm_context *ctx, const float *z, int nx, int ny, float water_height,
+                               const float *depth_map, int iterations, float dt, float dry_out_ratio,
+                               float viscosity, float power, float *water_depth)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_flow_simulation_viscous: ctx is NULL");
+  int st = hm::vflow_check_args(z, depth_map, water_depth, nx, ny, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  const size_t n = (size_t)nx * ny;
+  const size_t nbytes = n * sizeof(float);
+  const size_t total = 3 * align_up(nbytes, 256) + align_up(hm::vflow_scratch_bytes(nx, ny), 256);
+  void        *ws = nullptr;
+  if ((st = hm::workspace(ctx, total, &ws))) return st;
+  Slab         sl{(char *)ws};
+  float       *dz = sl.take(n);
+  float       *ddm = sl.take(n);
+  float       *dout = sl.take(n);
+  void        *scr = sl.take_bytes(hm::vflow_scratch_bytes(nx, ny));
+  cudaStream_t s = ctx->stream;
+  HM_CUDA_TRY(cudaMemcpyAsync(dz, z, nbytes, cudaMemcpyHostToDevice, s));
+  HM_CUDA_TRY(cudaMemcpyAsync(ddm, depth_map, nbytes, cudaMemcpyHostToDevice, s));
+  st = hm::vflow_core(dz, nx, ny, water_height, ddm, iterations, dt, dry_out_ratio, viscosity, power, dout, scr, s);
+  if (st)
+  {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  HM_CUDA_TRY(cudaMemcpyAsync(water_depth, dout, nbytes, cudaMemcpyDeviceToHost, s));
+  HM_CUDA_TRY(cudaStreamSynchronize(s));
+  return HM_OK;
+}
+
+int hm_flow_simulation_viscous_device(hm_context *ctx, const float *z, int nx, int ny, float water_height,
+                                      const float *depth_map, int iterations, float dt, float dry_out_ratio,
+                                      float viscosity, float power, float *water_depth, void *stream)
+{
+  hm::clear_error();
+  if (!ctx) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_flow_simulation_viscous_device: ctx is NULL");
+  int st = hm::vflow_check_args(z, depth_map, water_depth, nx, ny, iterations);
+  if (st) return st;
+  if ((st = hm::use_device(ctx->device))) return st;
+  void *ws = nullptr;
+  if ((st = hm::workspace(ctx, hm::vflow_scratch_bytes(nx, ny), &ws))) return st;
+  return hm::vflow_core(z, nx, ny, water_height, depth_map, iterations, dt, dry_out_ratio, viscosity, power,
+                        water_depth, ws, (cudaStream_t)stream);
+}
+
 int hm_vpipes(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_params *params, const float *rain_map,
               float *water_depth, float *sediment, float *vel_u, float *vel_v)
 {

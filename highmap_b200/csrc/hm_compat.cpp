@@ -11,6 +11,7 @@
  *   sediment_deposition  HighMap/src/erosion/deposition.cpp:19-66
  *   sediment_layer       HighMap/src/erosion/deposition.cpp:68-113
  *   thermal_flatten, thermal_inflate, thermal_rib  thermal_gpu.cpp:154-219,249-272
+ *   flow_simulation_viscous  HighMap/src/hydrology/flow_simulation.cpp:112-157
  *   init_opencl      HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134
  * The reference functions return void and report problems only through
  * their logger; here a failed call leaves z untouched, prints the status
@@ -409,6 +410,33 @@ Array flow_simulation(const Array &z, float water_height, const Array &depth_map
   int st = hm_flow_simulation(ctx, z.vector.data(), z.shape.x, z.shape.y, water_height, depth_map.vector.data(),
                               iterations, dt, flux_diffusion ? 1 : 0, flux_diffusion_strength, dry_out_ratio,
                               d.data());
+  if (report(st, fn)) out.vector.swap(d);
+  return out;
+}
+
+Array flow_simulation_viscous(const Array &z, float water_depth, const Array &depth_map, int iterations, float dt,
+                              float dry_out_ratio, float viscosity, float power)
+{
+  const char *fn = "hmap::gpu::flow_simulation_viscous";
+  Array       out;
+  shape_like(&out, z);
+  std::fill(out.vector.begin(), out.vector.end(), 0.f);
+  if (!same_shape(&depth_map, z) || z.vector.size() != (size_t)z.shape.x * (size_t)z.shape.y)
+  {
+    report(HM_ERR_INVALID_ARGUMENT, fn);
+    g_err += "arrays of different shapes";
+    return out;
+  }
+  hm_context *ctx = context();
+  if (!ctx)
+  {
+    report(HM_ERR_NO_DEVICE, fn);
+    return out;
+  }
+  std::vector<float> d(z.vector.size());
+  int st = hm_flow_simulation_viscous(ctx, z.vector.data(), z.shape.x, z.shape.y, water_depth,
+                                      depth_map.vector.data(), iterations, dt, dry_out_ratio, viscosity, power,
+                                      d.data());
   if (report(st, fn)) out.vector.swap(d);
   return out;
 }

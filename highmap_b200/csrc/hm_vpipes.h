@@ -32,6 +32,14 @@ int             flow_simulation_core(const float *z, int nx, int ny, float water
                                      int iterations, float dt, int flux_diffusion, float flux_diffusion_strength,
                                      float dry_out_ratio, float *water_depth, void *scratch, cudaStream_t s);
 const unsigned *flow_error_word(const void *scratch, int nx, int ny);
+/* flow_simulation_viscous (hm_vflow.cu): device pointers, ordered on s;
+ * scratch of vflow_scratch_bytes; water_depth receives the final depth */
+int             vflow_check_args(const float *z, const float *depth_map, const float *out, int nx, int ny,
+                                 int iterations);
+size_t          vflow_scratch_bytes(int nx, int ny);
+int             vflow_core(const float *z, int nx, int ny, float water_height, const float *depth_map, int iterations,
+                           float dt, float dry_out_ratio, float viscosity, float power, float *water_depth,
+                           void *scratch, cudaStream_t s);
 /* fp64 partial-sum slots vpipes_init needs */
 size_t  vpipes_init_partials();
 /* water-depth output: stored depth plus the top-up of the last step */

@@ -302,6 +302,33 @@ def thermal_stencil_device(rule: int, z, talus, iterations: int = 10, zmax=None,
                                               _tptr(mask, "mask", z.shape), _stream(stream)))
 
 
+def flow_simulation_viscous(z: np.ndarray, water_height: float, depth_map: np.ndarray, iterations: int,
+                            dt: float = 0.5, dry_out_ratio: float = 0.0, viscosity: float = 1.0, power: float = 2.5,
+                            ctx: Context | None = None) -> np.ndarray:
+    """hmap::gpu::flow_simulation_viscous (flow_simulation.cpp:112-157): the water depth."""
+    _grid(z, "z")
+    _grid(depth_map, "depth_map", z.shape)
+    ny, nx = z.shape
+    out = np.empty_like(z)
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_flow_simulation_viscous(ctx.handle, _ptr(z), nx, ny, C.c_float(water_height), _ptr(depth_map),
+                                               int(iterations), C.c_float(dt), C.c_float(dry_out_ratio),
+                                               C.c_float(viscosity), C.c_float(power), _ptr(out)))
+    return out
+
+
+def flow_simulation_viscous_device(z, water_height: float, depth_map, iterations: int, water_depth, dt: float = 0.5,
+                                   dry_out_ratio: float = 0.0, viscosity: float = 1.0, power: float = 2.5,
+                                   ctx: Context | None = None, stream=None) -> None:
+    ny, nx = z.shape
+    ctx = ctx or default_context()
+    L.check(L.lib().hm_flow_simulation_viscous_device(ctx.handle, _tptr(z, "z"), nx, ny, C.c_float(water_height),
+                                                      _tptr(depth_map, "depth_map", z.shape), int(iterations),
+                                                      C.c_float(dt), C.c_float(dry_out_ratio), C.c_float(viscosity),
+                                                      C.c_float(power), _tptr(water_depth, "water_depth", z.shape),
+                                                      _stream(stream)))
+
+
 def thermal_flatten(z: np.ndarray, talus: np.ndarray, iterations: int, sigma_inf: float = 0.5,
                     sigma_sup: float = 0.0, mask: np.ndarray | None = None, ctx: Context | None = None) -> None:
     """hmap::gpu::thermal_flatten (thermal_gpu.cpp:154-190), in place."""

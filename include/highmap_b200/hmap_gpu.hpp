@@ -160,6 +160,16 @@ Array flow_simulation(const Array &z,
                       float        flux_diffusion_strength = 0.01f,
                       float        dry_out_ratio = 0.f);
 
+/* HighMap/include/highmap/hydrology/hydrology.hpp:884-891 */
+Array flow_simulation_viscous(const Array &z,
+                              float        water_depth,
+                              const Array &depth_map,
+                              int          iterations,
+                              float        dt = 0.5f,
+                              float        dry_out_ratio = 0.f,
+                              float        viscosity = 1.f,
+                              float        power = 2.5f);
+
 void hydraulic_vpipes(Array &z,
                       float  water_height = 1e-2f,
                       bool   maintain_water_volume = true,

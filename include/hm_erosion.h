@@ -475,6 +475,45 @@ int hm_flow_simulation_device(hm_context  *ctx,
                               float       *water_depth,
                               void        *stream);
 
+/* Replaces hmap::gpu::flow_simulation_viscous(const Array &z,
+ * float water_depth, const Array &depth_map, int iterations, float dt,
+ * float dry_out_ratio, float viscosity, float power)
+ * (HighMap/include/highmap/hydrology/hydrology.hpp:884-891,
+ *  HighMap/src/hydrology/flow_simulation.cpp:112-157, kernel
+ *  shallow_viscous_flow.cl): water_height * depth_map spread as a viscous
+ * film over the fixed terrain z for `iterations` steps, the time step
+ * re-derived from the deepest water every 10 steps (so `dt` matters only
+ * for iterations == 0), then the dry-out.  water_depth receives the depth.
+ * The reference's defaults: dt 0.5, dry_out_ratio 0, viscosity 1, power
+ * 2.5. */
+int hm_flow_simulation_viscous(hm_context  *ctx,
+                               const float *z,
+                               int          nx,
+                               int          ny,
+                               float        water_height,
+                               const float *depth_map,
+                               int          iterations,
+                               float        dt,
+                               float        dry_out_ratio,
+                               float        viscosity,
+                               float        power,
+                               float       *water_depth);
+
+/* The same on device buffers, ordered on `stream`. */
+int hm_flow_simulation_viscous_device(hm_context  *ctx,
+                                      const float *z,
+                                      int          nx,
+                                      int          ny,
+                                      float        water_height,
+                                      const float *depth_map,
+                                      int          iterations,
+                                      float        dt,
+                                      float        dry_out_ratio,
+                                      float        viscosity,
+                                      float        power,
+                                      float       *water_depth,
+                                      void        *stream);
+
 /* No counterpart in the reference (which allocates its OpenCL buffers on
  * every call).  Thermal erosion on device buffers for callers that cannot
  * allocate device memory when they run it (an application whose own pool

@@ -6,7 +6,7 @@
   (HighMap/src/gpu_opencl/kernels/_common_index.cl, thermal.cl,
   hydraulic_vpipes.cl, thermal_ridge.cl, thermal_scree.cl, thermal_schott.cl,
   thermal_olsen.cl, thermal_flatten.cl, thermal_inflate.cl, thermal_rib.cl,
-  and the helper functions they call from
+  shallow_viscous_flow.cl, and the helper functions they call from
   _common_math.cl and _common_rand.cl) compiled for the CPU behind
   ``ref_shim.h``, linked
   with the host-driver restatement ``ref_harness.cpp``.  Built only where
@@ -29,7 +29,8 @@ REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(HERE, "libhm_oracle.so")
 REF_SO = os.path.join(REF_DIR, "libhm_ref.so")
 KERNEL_FILES = ("_common_index.cl", "thermal.cl", "hydraulic_vpipes.cl", "thermal_ridge.cl", "thermal_scree.cl",
-                "thermal_schott.cl", "thermal_olsen.cl", "thermal_flatten.cl", "thermal_inflate.cl", "thermal_rib.cl")
+                "thermal_schott.cl", "thermal_olsen.cl", "thermal_flatten.cl", "thermal_inflate.cl", "thermal_rib.cl",
+                "shallow_viscous_flow.cl")
 # helpers the sibling talus kernels call, taken function by function from
 # the shared kernel files (the rest of those files is not needed)
 HELPER_FUNCTIONS = (("_common_math.cl", ("almost_unit_identity", "smoothstep3")), ("_common_rand.cl", ("hash21u",)))

@@ -186,6 +186,31 @@ int hmo_thermal_relief_f64(int           rule,
                            int           iterations,
                            const double *mask);
 
+/* flow_simulation_viscous (HighMap/src/hydrology/flow_simulation.cpp:112-157,
+ * kernel shallow_viscous_flow.cl): returns the water depth in water_depth. */
+int hmo_flow_simulation_viscous_f32(const float *z,
+                                    int          nx,
+                                    int          ny,
+                                    float        water_height,
+                                    const float *depth_map,
+                                    int          iterations,
+                                    float        dt,
+                                    float        dry_out_ratio,
+                                    float        viscosity,
+                                    float        power,
+                                    float       *water_depth);
+int hmo_flow_simulation_viscous_f64(const double *z,
+                                    int           nx,
+                                    int           ny,
+                                    double        water_height,
+                                    const double *depth_map,
+                                    int           iterations,
+                                    double        dt,
+                                    double        dry_out_ratio,
+                                    double        viscosity,
+                                    double        power,
+                                    double       *water_depth);
+
 /* snow_simulation's post-filter (HighMap/src/hydrology/snow_simulation.cpp:
  * 140-152, then its clamp_min(s, 0)): z the terrain, s the snow depth,
  * updated in place. */

@@ -262,6 +262,37 @@ def ref_thermal_relief(rule, z, talus=None, iterations=10, sigma_inf=0.5, sigma_
     return z
 
 
+def flow_simulation_viscous(z, water_height, depth_map, iterations, dt=0.5, dry_out_ratio=0.0, viscosity=1.0,
+                            power=2.5, dtype=np.float32):
+    """Oracle flow_simulation_viscous (flow_simulation.cpp:112-157); returns the water depth."""
+    z = _grid(z, dtype)
+    ny, nx = z.shape
+    dm = _grid(depth_map, dtype)
+    out = np.empty_like(z)
+    fn = _lib().hmo_flow_simulation_viscous_f32 if dtype == np.float32 else _lib().hmo_flow_simulation_viscous_f64
+    S = C.c_float if dtype == np.float32 else C.c_double
+    rc = fn(_p(z), nx, ny, S(water_height), _p(dm), int(iterations), S(dt), S(dry_out_ratio), S(viscosity), S(power),
+            _p(out))
+    if rc:
+        raise ValueError("oracle flow_simulation_viscous rejected its arguments (status %d)" % rc)
+    return out
+
+
+def ref_flow_simulation_viscous(z, water_height, depth_map, iterations, dt=0.5, dry_out_ratio=0.0, viscosity=1.0,
+                                power=2.5):
+    """flow_simulation.cpp:112-157 driven over the reference's shallow_viscous_flow.cl."""
+    z = _grid(z, np.float32)
+    ny, nx = z.shape
+    dm = _grid(depth_map, np.float32)
+    out = np.empty_like(z)
+    rc = _ref().ref_flow_simulation_viscous(_p(z), nx, ny, C.c_float(water_height), _p(dm), int(iterations),
+                                            C.c_float(dt), C.c_float(dry_out_ratio), C.c_float(viscosity),
+                                            C.c_float(power), _p(out))
+    if rc:
+        raise ValueError("ref flow_simulation_viscous rejected its arguments (status %d)" % rc)
+    return out
+
+
 RIDGE, SCREE, SCHOTT, OLSEN = 0, 1, 2, 3
 
 

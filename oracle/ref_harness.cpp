@@ -18,6 +18,7 @@
  *                        gradient.cpp:217-243 and filters.cpp:290-324)
  *   ref_snow_post_filter : HighMap/src/hydrology/snow_simulation.cpp:140-152
  *   ref_thermal_relief : HighMap/src/erosion/thermal_gpu.cpp:154-219,249-272
+ *   ref_flow_simulation_viscous : HighMap/src/hydrology/flow_simulation.cpp:112-157
  *
  * Work-items run as a host loop (OpenMP over rows).  The in-place thermal
  * kernels are given a private copy of the three rows around the work-item,
@@ -69,6 +70,7 @@ void thermal_flatten(float       *z,
                      const float  sigma_sup);
 void thermal_inflate(float *z, const float *talus, const int nx, const int ny);
 void thermal_rib(float *z, const int nx, const int ny);
+void shallow_viscous_flow(image2d_t, image2d_t, image2d_t, int, int, float, float, float);
 void hydraulic_vpipes_flow_pass(image2d_t, image2d_t, image2d_t, image2d_t, image2d_t, image2d_t,
                                 image2d_t, image2d_t, image2d_t, image2d_t, const int, const int,
                                 const float, const int, const float);
@@ -623,6 +625,59 @@ int ref_thermal_relief(int          rule,
   }
   extrapolate_borders_n(a.data(), nx, ny, rule == 6 ? 3 : 1);
   for (size_t k = 0; k < n; k++) z[k] = mask ? z[k] * (1.f - mask[k]) + a[k] * mask[k] : a[k];
+  return 0;
+}
+
+/* flow_simulation.cpp:112-157 over shallow_viscous_flow.cl: the adaptive
+ * dt of helper_vflow_compute_adaptive_dt (:16-24) every 10 steps, h_in ->
+ * h_out per step, then water_depth_dry_out (water_depth.cpp:40-66) */
+int ref_flow_simulation_viscous(const float *z,
+                                int          nx,
+                                int          ny,
+                                float        water_height,
+                                const float *depth_map,
+                                int          iterations,
+                                float        dt,
+                                float        dry_out_ratio,
+                                float        viscosity,
+                                float        power,
+                                float       *water_depth)
+{
+  if (!z || !depth_map || !water_depth || nx < 1 || ny < 1 || iterations < 0) return 1;
+  const size_t       n = (size_t)nx * ny;
+  std::vector<float> zz(z, z + n), d(n), d_o(n);
+  for (size_t k = 0; k < n; k++) d[k] = water_height * depth_map[k];
+  for (int it = 0; it < iterations; ++it)
+  {
+    if (it % 10 == 0)
+    {
+      const float hmax = *std::max_element(d.begin(), d.end());
+      const float mobility = std::pow(hmax, power) / viscosity;
+      dt = 0.2f / std::fmax(mobility, 1e-6f);
+    }
+    hmref::hm_image iz{zz.data(), nx, ny}, i_d{d.data(), nx, ny}, o_d{d_o.data(), nx, ny};
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < ny; j++)
+    {
+      hmref::g_gid1 = j;
+      for (int i = 0; i < nx; i++)
+      {
+        hmref::g_gid0 = i;
+        hmref::shallow_viscous_flow(&iz, &i_d, &o_d, nx, ny, dt, viscosity, power);
+      }
+    }
+    d.swap(d_o);
+  }
+  if (dry_out_ratio != 0.f)
+  {
+    const float dmax = *std::max_element(d.begin(), d.end());
+    for (size_t k = 0; k < n; k++)
+    {
+      d[k] -= dry_out_ratio * dmax;
+      d[k] = std::max(0.f, d[k]);
+    }
+  }
+  std::memcpy(water_depth, d.data(), n * sizeof(float));
   return 0;
 }
 

@@ -6,7 +6,7 @@
  * requested solver, writes the results as raw float32 for the test to
  * compare with the oracle.
  *
- * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition|layer|flatten|inflate|rib>
+ * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition|layer|flatten|inflate|rib|viscous>
  *        nx ny in.f32 out_prefix
  */
 #include <cstdio>
@@ -109,6 +109,12 @@ int main(int argc, char **argv)
     else if (mode == "inflate") hmap::gpu::thermal_inflate(z, &mask, talus, 12);
     else hmap::gpu::thermal_rib(z, 6);
     write_raw(out + "_z.f32", z);
+  }
+  else if (mode == "viscous")
+  {
+    hmap::Array dm(shape, 1.f);
+    hmap::Array d = hmap::gpu::flow_simulation_viscous(z, 0.05f, dm, 40);
+    write_raw(out + "_d.f32", d);
   }
   else if (mode == "layer")
   {

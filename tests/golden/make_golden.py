@@ -9,7 +9,7 @@ for the CPU by oracle/build_oracle.py and driven by oracle/ref_harness.cpp
 (Jacobi form).  Run in a checkout where the reference tree is present:
 
     python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation] [siblings] [deposition]
-                                     [layer] [snow] [relief]
+                                     [layer] [snow] [relief] [viscous]
 
 Each .npz holds the inputs, the parameters and the outputs of one case.
 """
@@ -176,9 +176,22 @@ def relief_cases():
             _save(name + ("_masked" if m is not None else ""), **arrays)
 
 
+def viscous_cases():
+    # flow_simulation_viscous on inputs where the film stays stable (water conserved), with and without dry-out
+    nx, ny = 128, 96
+    z = fbm(nx, ny, seed=11)
+    dm = fbm(nx, ny, seed=12)
+    for dry in (0.0, 0.1):
+        out = po.ref_flow_simulation_viscous(z, 0.05, dm, 60, 0.5, dry, 1.0, 2.5)
+        _save("flow_simulation_viscous%s" % ("_dry" if dry else ""), z=z, depth_map=dm, water_height=np.float32(0.05),
+              iterations=np.int32(60), dry_out_ratio=np.float32(dry), viscosity=np.float32(1.0),
+              power=np.float32(2.5), out_d=out)
+
+
 GROUPS = {"thermal": thermal_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases,
           "siblings": sibling_cases, "deposition": deposition_cases,
-          "layer": layer_cases, "snow": snow_cases, "relief": relief_cases}
+          "layer": layer_cases, "snow": snow_cases, "relief": relief_cases,
+          "viscous": viscous_cases}
 
 if __name__ == "__main__":
     if not po.ref_available():

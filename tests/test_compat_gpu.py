@@ -137,6 +137,14 @@ def test_thermal_relief(gpu, example, tmp_path, mode):
     assert np.array_equal(load("z"), want)
 
 
+def test_flow_simulation_viscous(gpu, example, tmp_path):
+    z = fbm(128, 96, seed=15)
+    load = _run(example, "viscous", z, tmp_path)
+    want = po.flow_simulation_viscous(z, 0.05, np.ones_like(z), 40)
+    got = load("d")
+    assert np.abs(got - want).max() <= 1e-3 * float(want.max())
+
+
 def test_vpipes(gpu, example, tmp_path):
     z = fbm(96, 64, seed=2)
     load = _run(example, "vpipes", z, tmp_path)

@@ -134,6 +134,14 @@ def test_thermal_relief_golden_bit_exact(case):
     assert np.array_equal(z, g["out_z"])
 
 
+@pytest.mark.parametrize("case", ["flow_simulation_viscous", "flow_simulation_viscous_dry"])
+def test_flow_simulation_viscous_golden_bit_exact(case):
+    g = _load(case)
+    out = po.flow_simulation_viscous(g["z"], float(g["water_height"]), g["depth_map"], int(g["iterations"]), 0.5,
+                                     float(g["dry_out_ratio"]), float(g["viscosity"]), float(g["power"]))
+    assert np.array_equal(out, g["out_d"])
+
+
 def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))}
     assert {"thermal_uniform", "vpipes_defaults", "vpipes_rain_per_step"} <= names
@@ -320,4 +328,17 @@ def test_thermal_relief_matches_reference_text(rule, shape):
     for m in (None, mask):
         a = po.thermal_relief(rule, z, talus, 9, 0.5, 0.3, mask=m)
         b = po.ref_thermal_relief(rule, z, talus, 9, 0.5, 0.3, mask=m)
+        assert np.array_equal(a, b, equal_nan=True)
+
+
+@ref_only
+@pytest.mark.parametrize("shape", [(41, 53), (1, 7), (6, 1), (64, 96)])
+def test_flow_simulation_viscous_matches_reference_text(shape):
+    ny, nx = shape
+    rs = np.random.RandomState(61)
+    z = fbm(nx, ny, seed=61) if min(shape) > 8 else rs.rand(ny, nx).astype(np.float32)
+    dm = fbm(nx, ny, seed=62) if min(shape) > 8 else rs.rand(ny, nx).astype(np.float32)
+    for dry, power in ((0.0, 2.5), (0.2, 1.5)):
+        a = po.flow_simulation_viscous(z, 0.04, dm, 25, 0.5, dry, 1.3, power)
+        b = po.ref_flow_simulation_viscous(z, 0.04, dm, 25, 0.5, dry, 1.3, power)
         assert np.array_equal(a, b, equal_nan=True)
