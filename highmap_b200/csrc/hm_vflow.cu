@@ -94,30 +94,49 @@ __device__ __forceinline__ float face_mobility(float h, float hn, float viscosit
   return fdiv(powr(fmul(0.5f, fadd(h, hn)), power), viscosity);
 }
 
-__global__ void __launch_bounds__(VF_NT) k_vflow_step(const float *__restrict__ z, const float *__restrict__ hin,
-                                                      float *__restrict__ hout, int nx, int ny,
-                                                      const float *__restrict__ dtp, float viscosity, float power)
+/* One step over a 32 x 8 tile.  Each face mobility is evaluated once, by
+ * the thread of the cell west / south of it (plus the tile's west and
+ * south edges), into shared memory; a face is the same value for the two
+ * cells it separates (fadd is commutative), so this equals evaluating it
+ * from both sides, at about half the pow calls.  Faces on the grid's edge
+ * pair a cell with itself, as the clamped reads do. */
+constexpr int VT_X = 32, VT_Y = 8;
+
+__global__ void __launch_bounds__(VT_X *VT_Y) k_vflow_step(const float *__restrict__ z, const float *__restrict__ hin,
+                                                          float *__restrict__ hout, int nx, int ny,
+                                                          const float *__restrict__ dtp, float viscosity, float power)
 {
-  const float  dt = *dtp;
-  const size_t n = (size_t)nx * ny;
-  for (size_t k = blockIdx.x * (size_t)VF_NT + threadIdx.x; k < n; k += (size_t)gridDim.x * VF_NT)
+  __shared__ float me[VT_Y][VT_X + 1]; /* me[ty][tx + 1]: east face of (tx, ty); [ty][0]: west edge  */
+  __shared__ float mn[VT_Y + 1][VT_X]; /* mn[ty + 1][tx]: north face of (tx, ty); [0][tx]: south edge */
+  const int  tx = threadIdx.x, ty = threadIdx.y;
+  const int  i = blockIdx.x * VT_X + tx, j = blockIdx.y * VT_Y + ty;
+  const bool in = i < nx && j < ny;
+  const int  ic = in ? i : 0, jc = in ? j : 0;
+  const size_t k = (size_t)jc * nx + ic;
+  const size_t ke = ic < nx - 1 ? k + 1 : k, kw = ic > 0 ? k - 1 : k;
+  const size_t kn = jc < ny - 1 ? k + nx : k, ks = jc > 0 ? k - nx : k; /* j + 1, j - 1 */
+  const float  h = hin[k];
+  const float  hxp = hin[ke], hxm = hin[kw], hyp = hin[kn], hym = hin[ks];
+  if (in)
   {
-    const int    j = (int)(k / (size_t)nx), i = (int)(k - (size_t)j * nx);
-    const size_t ke = i < nx - 1 ? k + 1 : k, kw = i > 0 ? k - 1 : k;
-    const size_t kn = j < ny - 1 ? k + nx : k, ks = j > 0 ? k - nx : k; /* j + 1, j - 1 */
-    const float  h = hin[k], zc = z[k];
-    const float  hxp = hin[ke], hxm = hin[kw], hyp = hin[kn], hym = hin[ks];
-    const float  Hc = fadd(h, zc);
-    const float  Hxp = fadd(hxp, z[ke]), Hxm = fadd(hxm, z[kw]), Hyp = fadd(hyp, z[kn]), Hym = fadd(hym, z[ks]);
-    const float  Mp = face_mobility(h, hxp, viscosity, power), Mm = face_mobility(h, hxm, viscosity, power);
-    const float  Myp = face_mobility(h, hyp, viscosity, power), Mym = face_mobility(h, hym, viscosity, power);
-    const float  qxp = fmul(-Mp, fsub(Hxp, Hc));
-    const float  qxm = fmul(-Mm, fsub(Hc, Hxm));
-    const float  qyp = fmul(-Myp, fsub(Hyp, Hc));
-    const float  qym = fmul(-Mym, fsub(Hc, Hym));
-    const float  dhdt = -fsub(fadd(fsub(qxp, qxm), qyp), qym);
-    hout[k] = fmaxf(0.f, fadd(h, fmul(dt, dhdt)));
+    me[ty][tx + 1] = face_mobility(h, hxp, viscosity, power);
+    mn[ty + 1][tx] = face_mobility(h, hyp, viscosity, power);
+    if (tx == 0) me[ty][0] = face_mobility(h, hxm, viscosity, power);
+    if (ty == 0) mn[0][tx] = face_mobility(h, hym, viscosity, power);
   }
+  __syncthreads();
+  if (!in) return;
+  const float dt = *dtp;
+  const float zc = z[k];
+  const float Hc = fadd(h, zc);
+  const float Hxp = fadd(hxp, z[ke]), Hxm = fadd(hxm, z[kw]), Hyp = fadd(hyp, z[kn]), Hym = fadd(hym, z[ks]);
+  const float Mp = me[ty][tx + 1], Mm = me[ty][tx], Myp = mn[ty + 1][tx], Mym = mn[ty][tx];
+  const float qxp = fmul(-Mp, fsub(Hxp, Hc));
+  const float qxm = fmul(-Mm, fsub(Hc, Hxm));
+  const float qyp = fmul(-Myp, fsub(Hyp, Hc));
+  const float qym = fmul(-Mym, fsub(Hc, Hym));
+  const float dhdt = -fsub(fadd(fsub(qxp, qxm), qyp), qym);
+  hout[k] = fmaxf(0.f, fadd(h, fmul(dt, dhdt)));
 }
 
 /* water_depth_dry_out: h -= ratio * hmax, then max(0, h) */
@@ -147,6 +166,8 @@ int vflow_check_args(const float *z, const float *depth_map, const float *out, i
   if ((long long)nx * (long long)ny > (1ll << 34))
     return fail(HM_ERR_INVALID_ARGUMENT, "flow_simulation_viscous: grid larger than 2^34 cells");
   if (iterations < 0) return fail(HM_ERR_INVALID_ARGUMENT, "flow_simulation_viscous: iterations < 0");
+  if ((ny + VT_Y - 1) / VT_Y > 65535)
+    return fail(HM_ERR_INVALID_ARGUMENT, "flow_simulation_viscous: ny larger than 524280 rows");
   return HM_OK;
 }
 
@@ -163,7 +184,8 @@ int vflow_core(const float *z, int nx, int ny, float water_height, const float *
   HM_LAUNCH_CHECK("k_vflow_reset");
   k_vflow_init<<<VF_GRID, VF_NT, 0, s>>>(hA, depth_map, water_height, n);
   HM_LAUNCH_CHECK("k_vflow_init");
-  float *cur = hA, *nxt = hB;
+  const dim3 tiles((nx + VT_X - 1) / VT_X, (ny + VT_Y - 1) / VT_Y);
+  float     *cur = hA, *nxt = hB;
   for (int it = 0; it < iterations; ++it)
   {
     if (it % 10 == 0)
@@ -173,7 +195,7 @@ int vflow_core(const float *z, int nx, int ny, float water_height, const float *
       k_vflow_dt<<<1, 1, 0, s>>>(slot, viscosity, power, dtp);
       HM_LAUNCH_CHECK("k_vflow_dt");
     }
-    k_vflow_step<<<VF_GRID, VF_NT, 0, s>>>(z, cur, nxt, nx, ny, dtp, viscosity, power);
+    k_vflow_step<<<tiles, dim3(VT_X, VT_Y), 0, s>>>(z, cur, nxt, nx, ny, dtp, viscosity, power);
     HM_LAUNCH_CHECK("k_vflow_step");
     float *t = cur;
     cur = nxt;
