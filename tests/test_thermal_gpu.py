@@ -3,7 +3,7 @@
 The GPU kernels evaluate the reference's fp32 arithmetic one rounding per
 operation, so the bar here is bit-exact equality with the oracle (which is
 itself bit-exact with the reference's kernel text, tests/test_oracle.py);
-the north-star tolerance (max abs error <= 1e-4 of the height range) is
+the thermal tolerance (max abs error <= 1e-4 of the height range) is
 checked as well so a failure reports its size.
 """
 import json

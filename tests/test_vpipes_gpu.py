@@ -4,7 +4,7 @@ Bit-exact where both sides evaluate the same fp32 operations (every case
 without the water-volume top-up and with discharge exponent 1: the GPU
 reproduces the reference's one-rounding-per-operation arithmetic, fp64
 hypot included).  Two cases differ by construction and are held to the
-north-star tolerance (max abs error <= 1e-3 of the height range) on z and
+vpipes tolerance (max abs error <= 1e-3 of the height range) on z and
 sediment instead: maintain_water_volume, whose grid-wide fp64 sum is
 reduced in a different order on the two sides, and exponents other than 1,
 where the C library's powf (not correctly rounded) and the GPU's fp64 pow
