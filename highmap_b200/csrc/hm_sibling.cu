@@ -59,6 +59,13 @@ __device__ __forceinline__ unsigned hash21u(unsigned x, unsigned y)
   return h;
 }
 
+/* HMAP_DI / HMAP_DJ (erosion.hpp:21-22) + 1, packed two bits per direction:
+ * a direction chosen at run time is decoded with shifts instead of an
+ * indexed local array */
+constexpr unsigned DI1 = 0xA094u, DJ1 = 0x8849u;
+__host__ __device__ constexpr int di8(int k) { return (int)((DI1 >> (2 * k)) & 3u) - 1; }
+__host__ __device__ constexpr int dj8(int k) { return (int)((DJ1 >> (2 * k)) & 3u) - 1; }
+
 /* (val - other) / c for c = 1 or 1.414 */
 __device__ __forceinline__ float slope(float val, float other, bool diag)
 {
@@ -164,6 +171,32 @@ __global__ void __launch_bounds__(SB_TX *SB_TY)
     t[ly][lx] = __ldg(a + (size_t)gy * nx + gx);
   }
   __syncthreads();
+  /* flatten: the steepest descent of every cell of the tile and its 1-cell
+   * ring, once per cell (see below) */
+  __shared__ float    fm[RULE == HM_FLATTEN ? SB_TY + 2 : 1][SB_TX + 2];
+  __shared__ unsigned fk[RULE == HM_FLATTEN ? SB_TY + 2 : 1][SB_TX + 2];
+  if (RULE == HM_FLATTEN)
+  {
+    for (int e = tid; e < (SB_TY + 2) * (SB_TX + 2); e += SB_TX * SB_TY)
+    {
+      const int   ly = e / (SB_TX + 2), lx = e - ly * (SB_TX + 2);
+      const float zp = t[ly + 1][lx + 1];
+      float       dz[8], m = 0.f;
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+      {
+        dz[k] = slope(zp, t[ly + 1 + dj8(k)][lx + 1 + di8(k)], k >= 4);
+        if (dz[k] > m) m = dz[k];
+      }
+      unsigned mask = 0u;
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+        if (m > 0.f && dz[k] == m) mask |= 1u << k;
+      fm[ly][lx] = m;
+      fk[ly][lx] = mask;
+    }
+    __syncthreads();
+  }
   const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
   if (i >= nx || j >= ny) return;
   const size_t idx = (size_t)j * nx + i;
@@ -186,14 +219,10 @@ __global__ void __launch_bounds__(SB_TX *SB_TY)
     float          self = zat(0, 0);
     const float    talus_ref = __ldg(talus + idx);
     const unsigned shift = hash21u((unsigned)i, (unsigned)j) & 7u;
-    /* HMAP_DI / HMAP_DJ + 1 packed two bits per direction, so a direction
-     * chosen at run time is decoded with shifts instead of an indexed
-     * local array */
-    constexpr unsigned DI1 = 0xA094u, DJ1 = 0x8849u;
     for (int k = 0; k < 8; ++k)
     {
       const int s = (k + (int)shift) & 7;
-      const int gx = (int)((DI1 >> (2 * s)) & 3u) - 1, gy = (int)((DJ1 >> (2 * s)) & 3u) - 1; /* neighbour offset */
+      const int gx = di8(s), gy = dj8(s); /* neighbour offset */
       float     dsum = 0.f, dmax = 0.f, dz[8];
 #pragma unroll
       for (int p = 0; p < 8; ++p)
@@ -234,49 +263,37 @@ __global__ void __launch_bounds__(SB_TX *SB_TY)
       b[idx] = __ldg(a + (size_t)cj * nx + ci);
       return;
     }
-    /* thermal_flatten.cl: neighbours visited from a rotating start
-     * (i + j) % 8, the first strict maximum kept; the cell loses sigma_inf
-     * (below its talus) or sigma_sup (above) times its steepest descent and
-     * gains half of each neighbour's steepest descent that points at it
-     * and lies below that neighbour's talus */
-    /* HMAP_DI / HMAP_DJ + 1 packed two bits per direction: the rotated
-     * directions are decoded with shifts instead of an indexed local array */
-    constexpr unsigned DI1 = 0xA094u, DJ1 = 0x8849u;
-    auto        ddi = [](int k) { return (int)((DI1 >> (2 * k)) & 3u) - 1; };
-    auto        ddj = [](int k) { return (int)((DJ1 >> (2 * k)) & 3u) - 1; };
+    /* thermal_flatten.cl visits the neighbours from a rotating start
+     * (i + j) % 8 and keeps the first strict maximum.  The cell loses
+     * sigma_inf (below its talus) or sigma_sup (above) times its steepest
+     * descent, and gains half of each neighbour's steepest descent that
+     * points at it and lies below that neighbour's talus.  A steepest
+     * descent's value does not depend on the visiting order; its direction
+     * does, through ties only: the first of the tied directions in this
+     * cell's rotated order.  So each cell's maximum and the mask of
+     * directions reaching it come from the table above, and the rotation is
+     * applied to the mask here (the kernel text evaluates the 64 slopes for
+     * every cell). */
     const int   rot = (i + j) % 8;
+    const int   ty = threadIdx.y + 1, tx = threadIdx.x + 1; /* this cell in the table */
     const float zc = zat(0, 0);
     const float tc = __ldg(talus + idx);
     const float slope_min = __fdiv_rn(0.f, (float)nx);
-    float       delta = 0.f, dmax = 0.f;
-    for (int n = 0; n < 8; ++n)
-    {
-      const int   k = (n + rot) & 7;
-      const float dz = slope(zc, zat(ddi(k), ddj(k)), k >= 4);
-      if (dz > dmax) dmax = dz;
-    }
+    const float dmax = fm[ty][tx];
+    float       delta = 0.f;
     const float excess = fmaxf(__fsub_rn(dmax, slope_min), 0.f);
     if (dmax < tc) delta = __fsub_rn(delta, __fmul_rn(intensity, excess));
     if (dmax > tc) delta = __fsub_rn(delta, __fmul_rn(p1, excess));
     for (int n = 0; n < 8; ++n)
     {
-      const int   k = (n + rot) & 7;
-      const int   px = -ddi(k), py = -ddj(k);
-      const float zp = zat(px, py);
-      float       dm = 0.f;
-      int         ka = -1;
-      for (int m = 0; m < 8; ++m)
-      {
-        const int   kk = (m + rot) & 7;
-        const float dz = slope(zp, zat(px + ddi(kk), py + ddj(kk)), kk >= 4);
-        if (dz > dm)
-        {
-          dm = dz;
-          ka = kk;
-        }
-      }
-      if (ka == k && dm > 0.f && dm < __ldg(talus + (size_t)(j + py) * nx + (i + px)))
-        delta = __fadd_rn(delta, __fmul_rn(0.5f, dm));
+      const int      k = (n + rot) & 7;
+      const int      px = -di8(k), py = -dj8(k);
+      const unsigned mask = fk[ty + py][tx + px];
+      if (!mask) continue; /* no descent: the kernel text's ka = -1 */
+      const unsigned r = ((mask >> rot) | (mask << (8 - rot))) & 0xffu;
+      const int      ka = (__ffs(r) - 1 + rot) & 7;
+      const float    dm = fm[ty + py][tx + px];
+      if (ka == k && dm < __ldg(talus + (size_t)(j + py) * nx + (i + px))) delta = __fadd_rn(delta, __fmul_rn(0.5f, dm));
     }
     b[idx] = __fadd_rn(zc, delta);
     return;
