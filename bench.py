@@ -378,13 +378,10 @@ def run_ours(a):
     elapsed_ms = t_start.elapsed_time(t_end)
     th_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
     vp_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
-    if world > 1:
-        t = torch.tensor([elapsed_ms, th_ms, vp_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms, th_ms, vp_ms = [float(x) for x in t.tolist()]
+    from highmap_b200.replicas import job_rate, max_over_ranks
+    elapsed_ms, th_ms, vp_ms = max_over_ranks([elapsed_ms, th_ms, vp_ms], dist if world > 1 else None, dev)
 
-    total_updates = world * a.steps * cells * (THERMAL_ITERS + VPIPES_ITERS)
-    value = total_updates / (elapsed_ms * 1e-3)
+    value = job_rate(world, a.steps, cells * (THERMAL_ITERS + VPIPES_ITERS), elapsed_ms)
     ms_per_step = elapsed_ms / a.steps
 
     peak, peak_kind = _peaks()
@@ -420,11 +417,9 @@ def run_ours(a):
         if world > 1:
             dist.barrier()
         tot = sum(e2e_step() for _ in range(a.steps))
-        if world > 1:
-            t = torch.tensor([tot], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot = float(t.item())
-        e2e = {"value": world * a.steps * cells * (THERMAL_ITERS + VPIPES_ITERS) / tot, "unit": "cell-updates/s",
+        tot = max_over_ranks([tot], dist if world > 1 else None, dev)[0]
+        e2e = {"value": job_rate(world, a.steps, cells * (THERMAL_ITERS + VPIPES_ITERS), 1e3 * tot),
+               "unit": "cell-updates/s",
                "h2d_bytes_per_step": int(4 * cells * 4), "d2h_bytes_per_step": int(2 * cells * 4),
                "ms_per_step": 1e3 * tot / a.steps}
 
