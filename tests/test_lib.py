@@ -77,3 +77,19 @@ def test_no_cpu_fallback_when_library_missing(monkeypatch, tmp_path):
     monkeypatch.setattr(L, "LIB_PATH", str(tmp_path / "missing.so"))
     with pytest.raises(RuntimeError, match="not built"):
         L.lib()
+
+
+@pytest.mark.parametrize("source", ["compat_example.cpp", "overloads.cpp"])
+def test_cpp_dropin_links(built_lib, tmp_path, source):
+    """Callers written against HighMap's hmap::gpu API compile against
+    include/highmap_b200/hmap_gpu.hpp and link to the library: the example
+    program of the GPU tests, and a file that takes the address of every
+    declared overload with its exact signature (so each one is defined)."""
+    import subprocess
+    libdir = os.path.dirname(built_lib)
+    exe = str(tmp_path / source[:-4])
+    r = subprocess.run(["g++", "-std=c++17", "-O0", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", source), "-L", libdir, "-lhm_erosion",
+                        "-Wl,-rpath," + libdir, "-Wl,--no-undefined", "-o", exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert os.path.exists(exe)
