@@ -167,82 +167,133 @@ def _bytes_plain(r):
     return n * (2 if r["kind"] == "thermal" else 17)
 
 
-def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=64, large_cells=1024 * 1024):
+class CudaLanes:
+    """The device side of the served loop: an open batch (hm_batch_*) on a
+    high-priority stream, and the large lane, plain device calls on a
+    low-priority stream.  Jobs are windows of the field pool."""
+
+    def __init__(self, pool):
+        import torch
+        self._torch = torch
+        dev = torch.cuda.current_device()
+        self.pool = pool
+        self.batch = B.Batch(G.Context(dev))
+        self.big_ctx = G.Context(dev)
+        self.big_stream = torch.cuda.Stream(priority=0)  # lowest priority
+
+    def start_large(self, r):
+        """Launch request r on the large lane; returns a handle."""
+        z = self.pool.take(r["id"], r["nx"], r["ny"])
+        self._torch.cuda.current_stream().synchronize()
+        _plain(r, z, self.big_ctx, self.big_stream.cuda_stream)
+        ev = self._torch.cuda.Event()
+        ev.record(self.big_stream)
+        return (z, ev)
+
+    def large_done(self, handle):
+        return handle[1].query()
+
+    def large_bytes(self, r):
+        return _bytes_plain(r)
+
+    def make_job(self, r):
+        z = self.pool.take(r["id"], r["nx"], r["ny"])
+        return (z, _job(r, z))
+
+    def job_bytes(self, job):
+        return B.job_bytes(job[1])
+
+    def add(self, job):
+        # the window copy runs on torch's stream, the batch on its own
+        self._torch.cuda.current_stream().synchronize()
+        return self.batch.add(job[1])
+
+    def bytes_in_use(self):
+        return self.batch.bytes_in_use()
+
+    def step(self, rounds):
+        self.batch.step(rounds)
+        self.batch.synchronize()
+
+    def status(self, jid):
+        return self.batch.status(jid)
+
+    def release(self, jid):
+        self.batch.release(jid)
+
+    def close(self):
+        self.batch.close()
+        self.big_ctx.close()
+
+
+def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=64, large_cells=1024 * 1024, lanes=None,
+          clock=time.perf_counter, sleep=time.sleep):
     """Size-aware continuous batching: returns per-request latencies (s) and
     totals.
 
     Requests of at least `large_cells` cells fill the GPU on their own:
     they go, first come first served, through the plain device path on a
     low-priority stream (one at a time; their state stays in the solver's
-    workspace).  Smaller requests are admitted into an open batch while
-    their device state fits the HBM budget, advance together a few rounds
-    per tick on the batch's high-priority stream, which runs beside the
-    large solve, and retire when done.  A tick runs until the next batched
-    job completes, at most `rounds_per_tick` rounds (which bounds how long
-    an arrival waits for admission)."""
-    import torch
-    dev = torch.cuda.current_device()
-    b = B.Batch(G.Context(dev))
-    big_ctx = G.Context(dev)
-    big_stream = torch.cuda.Stream(priority=0)  # lowest priority
+    workspace).  Smaller requests are admitted into an open batch, in
+    arrival order, while their device state and the large lane's fit the
+    HBM budget (the first into an empty batch always), advance together a
+    few rounds per tick on the batch's high-priority stream, which runs
+    beside the large solve, and retire when done.  A tick runs until the
+    next batched job completes, at most `rounds_per_tick` rounds (which
+    bounds how long an arrival waits for admission).  `lanes` is the device
+    side (CudaLanes over `pool` by default); `clock` and `sleep` the time
+    source."""
+    own = lanes is None
+    if own:
+        lanes = CudaLanes(pool)
     pending = list(reqs)
     waiting = []     # arrived small requests, not admitted (FIFO)
     big_queue = []   # arrived large requests (FIFO)
-    big = None       # (request, z, done event) of the running large solve
-    active = {}      # job id -> (request, tensor, job)
+    big = None       # (request, handle) of the running large solve
+    active = {}      # job id -> (request, job)
     lat = {}
-    t0 = time.perf_counter()
+    t0 = clock()
     cells = 0
     while pending or waiting or active or big_queue or big:
-        now = time.perf_counter() - t0
+        now = clock() - t0
         while pending and pending[0]["arrival"] <= now:
             r = pending.pop(0)
             (big_queue if r["nx"] * r["ny"] >= large_cells else waiting).append(r)
         # the large lane: start the next large solve when the lane is free
-        if big is not None and big[2].query():
+        if big is not None and lanes.large_done(big[1]):
             r = big[0]
-            lat[r["id"]] = time.perf_counter() - t0 - r["arrival"]
+            lat[r["id"]] = clock() - t0 - r["arrival"]
             cells += r["nx"] * r["ny"] * r["iterations"]
             big = None
         if big is None and big_queue:
             r = big_queue.pop(0)
-            z = pool.take(r["id"], r["nx"], r["ny"])
-            torch.cuda.current_stream().synchronize()
-            _plain(r, z, big_ctx, big_stream.cuda_stream)
-            ev = torch.cuda.Event()
-            ev.record(big_stream)
-            big = (r, z, ev)
-        big_bytes = _bytes_plain(big[0]) if big is not None else 0
+            big = (r, lanes.start_large(r))
+        big_bytes = lanes.large_bytes(big[0]) if big is not None else 0
         while waiting:
             r = waiting[0]
-            z = pool.take(r["id"], r["nx"], r["ny"])
-            job = _job(r, z)
-            if active and b.bytes_in_use() + B.job_bytes(job) + big_bytes > budget_bytes:
+            job = lanes.make_job(r)
+            if active and lanes.bytes_in_use() + lanes.job_bytes(job) + big_bytes > budget_bytes:
                 break
             waiting.pop(0)
-            # the window copy runs on torch's stream, the batch on its own
-            torch.cuda.current_stream().synchronize()
-            jid = b.add(job)
-            active[jid] = (r, z, job)
+            active[lanes.add(job)] = (r, job)
         if not active:
             if big is not None:
-                time.sleep(0.0002)
+                sleep(0.0002)
             elif pending:
-                time.sleep(max(0.0, min(0.01, pending[0]["arrival"] - now)))
+                sleep(max(0.0, min(0.01, pending[0]["arrival"] - now)))
             continue
-        nearest = min(r["iterations"] - b.status(jid)[0] for jid, (r, _, _) in active.items())
-        b.step(max(1, min(nearest, rounds_per_tick)))
-        b.synchronize()
-        done_t = time.perf_counter() - t0
+        nearest = min(r["iterations"] - lanes.status(jid)[0] for jid, (r, _) in active.items())
+        lanes.step(max(1, min(nearest, rounds_per_tick)))
+        done_t = clock() - t0
         for jid in list(active):
-            if b.status(jid)[1]:
-                r, z, job = active.pop(jid)
+            if lanes.status(jid)[1]:
+                r, _ = active.pop(jid)
                 lat[r["id"]] = done_t - r["arrival"]
                 cells += r["nx"] * r["ny"] * r["iterations"]
-                b.release(jid)
-    total = time.perf_counter() - t0
-    b.close()
-    big_ctx.close()
+                lanes.release(jid)
+    total = clock() - t0
+    if own:
+        lanes.close()
     return lat, cells, total
 
 

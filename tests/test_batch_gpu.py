@@ -169,3 +169,18 @@ def test_job_bytes_accounts_state(gpu):
     jv = B.vpipes_job(z, 10)
     assert B.job_bytes(jt) >= 120 * 100 * 4
     assert B.job_bytes(jv) >= 13 * 120 * 100 * 4
+
+
+def test_served_loop_completes_every_request(gpu):
+    """The served form's loop on the device: a short Poisson stream, the
+    larger requests through the plain lane beside the batch; every request
+    completes once and the work is counted once."""
+    from highmap_b200 import forms as F
+    reqs = F.serve_requests(12, 200.0, seed=5, lo=64, hi=1024, it_lo=5, it_hi=60)
+    pool = F.FieldPool(count=2, side=1024)
+    lat, cells, total = F.serve(reqs, pool, large_cells=512 * 512, rounds_per_tick=8)
+    assert sorted(lat) == [r["id"] for r in reqs]
+    assert all(v >= 0 for v in lat.values())
+    assert any(r["nx"] * r["ny"] >= 512 * 512 for r in reqs) and any(r["nx"] * r["ny"] < 512 * 512 for r in reqs)
+    assert cells == sum(r["nx"] * r["ny"] * r["iterations"] for r in reqs)
+    assert total > 0
