@@ -211,8 +211,11 @@ __device__ __forceinline__ void st_pair(float *p, size_t k, float a, float b, bo
  * tile's new fluxes.  A pair reads its centre values as 8-byte words and
  * shares its inner neighbours, so a cell costs about half the shared-memory
  * and store instructions of one cell per thread; the arithmetic of each
- * cell is unchanged. */
-template <bool MAINTAIN, int F>
+ * cell is unchanged.  INNER: the tile and its 2-cell halo lie inside the
+ * grid and the outputs take pair stores (fwe_inner_tile), so every edge
+ * clamp and store-width test below is known to be the identity / true and
+ * drops out; the cells' values are the same either way. */
+template <bool MAINTAIN, int F, bool INNER = false>
 __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials,
                                             int bx, int by, int nbx, int nby, FweSmem &sm)
 {
@@ -311,17 +314,17 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
   const int ty = tid >> 4, pk = tid & 15;
   const int gy = y0 + ty, gx = x0 + 2 * pk;
   const int cc = 4 + 2 * pk; /* smem column of the first cell */
-  if (gx < nx && gy < ny)
+  if (INNER || (gx < nx && gy < ny))
   {
-    const bool second = gx + 1 < nx;
+    const bool second = INNER || gx + 1 < nx;
     const int  l = ty + 1, q = ty + 2;
     /* flux neighbours: rows and columns clamped to the grid (new fluxes are
      * derived: outside the grid they are the edge cell's own values) */
-    const int  ln = clampi(gy - 1, 0, ny - 1) - (y0 - 1);
-    const int  ls = clampi(gy + 1, 0, ny - 1) - (y0 - 1);
-    const int  cw0 = gx > 0 ? cc - 1 : cc;          /* west of the first cell  */
-    const int  ce0 = second ? cc + 1 : cc;          /* east of the first cell  */
-    const int  ce1 = gx + 2 < nx ? cc + 2 : cc + 1; /* east of the second cell */
+    const int  ln = INNER ? ty : clampi(gy - 1, 0, ny - 1) - (y0 - 1);
+    const int  ls = INNER ? ty + 2 : clampi(gy + 1, 0, ny - 1) - (y0 - 1);
+    const int  cw0 = INNER || gx > 0 ? cc - 1 : cc;          /* west of the first cell  */
+    const int  ce0 = second ? cc + 1 : cc;                   /* east of the first cell  */
+    const int  ce1 = INNER || gx + 2 < nx ? cc + 2 : cc + 1; /* east of the second cell */
     const float2 flc = lds2(&sm.fn[0][l][cc]), frc = lds2(&sm.fn[1][l][cc]), ftc = lds2(&sm.fn[2][l][cc]),
                  fbc = lds2(&sm.fn[3][l][cc]);
     const float2 ftn = lds2(&sm.fn[2][ln][cc]), fbs = lds2(&sm.fn[3][ls][cc]);
@@ -339,7 +342,7 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
       water_cell<false>(c, d1.y, flc.y, frc.y, ftc.y, fbc.y, frc.x, fle1, ftn.y, fbs.y, d2b, ub, vb);
     }
     const size_t k = (size_t)gy * nx + gx;
-    const bool   vec = io.vec != 0;
+    const bool   vec = INNER || io.vec != 0;
     if (FLOW_ONLY)
     {
       /* flow_simulation: the depth after the water pass is the next step's
@@ -398,13 +401,23 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
   }
 }
 
+/* the tile at (x0, y0) and its 2-cell halo lie inside the grid, and the
+ * outputs take pair stores: fwe_compute's INNER form applies */
+__device__ __forceinline__ bool fwe_inner_tile(const FweIo &io, int nx, int ny, int x0, int y0)
+{
+  return io.vec != 0 && x0 >= 2 && x0 + FT_TX + 2 <= nx && y0 >= 2 && y0 + FT_TY + 2 <= ny;
+}
+
 template <bool MAINTAIN, int F>
 __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F)) k_vp_fwe(FweIo io, VpConst c, VpScalars *sc, double *partials)
 {
   __shared__ FweSmem sm;
   fwe_stage_cp_async(io, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm);
   __syncthreads();
-  fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  if (fwe_inner_tile(io, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY))
+    fwe_compute<MAINTAIN, F, true>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  else
+    fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
 /* The same step with the input tiles fetched by TMA.  A tile whose loads
@@ -429,7 +442,10 @@ __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
     }
     return;
   }
-  fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  if (fwe_inner_tile(io, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY))
+    fwe_compute<MAINTAIN, F, true>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  else
+    fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
 /* advection of one cell: s_new = bilinear(s1, (i - dt u, j - dt v)) */
