@@ -448,17 +448,6 @@ __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
     fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
-/* advection of one cell: s_new = bilinear(s1, (i - dt u, j - dt v)) */
-__device__ __forceinline__ float advect_cell(const float *__restrict__ s1, int i, int j, float u, float v,
-                                             const VpConst &c)
-{
-  const float  x = fsub((float)i, fmul(c.dt, u));
-  const float  y = fsub((float)j, fmul(c.dt, v));
-  const Tap    t = linear_tap(x, y, c.nx, c.ny);
-  const size_t r0 = (size_t)t.j0 * c.nx, r1 = (size_t)t.j1 * c.nx;
-  return blend(t, __ldg(s1 + r0 + t.i0), __ldg(s1 + r0 + t.i1), __ldg(s1 + r1 + t.i0), __ldg(s1 + r1 + t.i1));
-}
-
 /* Launch one k_vp_fwe (tma false) or k_vp_fwe_tma (maps != NULL) step on
  * stream s with the kernel specialised for the step's options
  * (hm_vpipes_fwe_cp_async.cu, hm_vpipes_fwe_tma.cu). */
