@@ -93,3 +93,16 @@ def test_cpp_dropin_links(built_lib, tmp_path, source):
                         "-Wl,-rpath," + libdir, "-Wl,--no-undefined", "-o", exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert os.path.exists(exe)
+
+
+def test_c_abi_is_plain_c(built_lib, tmp_path):
+    """include/hm_erosion.h compiles as pedantic C11 without warnings, and a C
+    caller (tests/c/abi_example.c) links against the library."""
+    import subprocess
+    libdir = os.path.dirname(built_lib)
+    exe = str(tmp_path / "abi_example")
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                        os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", "abi_example.c"), "-L", libdir,
+                        "-lhm_erosion", "-Wl,-rpath," + libdir, "-Wl,--no-undefined", "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
