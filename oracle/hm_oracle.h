@@ -17,6 +17,13 @@
  *             HighMap/include/highmap/operator.hpp:405-418
  *   vpipes  : HighMap/src/gpu_opencl/kernels/hydraulic_vpipes.cl:5-211,
  *             HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:15-178
+ * and the callers and relatives of the two (each declaration below cites
+ * its lines): thermal_auto_bedrock, flow_simulation and
+ * flow_simulation_viscous, sediment_deposition and sediment_layer (with
+ * gradient_talus and laplace), the post-filter of snow_simulation, and the
+ * talus stencils ridge, scree, schott, olsen, flatten, inflate and rib.
+ * The host loops of those callers are evaluated in their source order, one
+ * rounding per operation.
  *
  * Parity pin: the restatement is checked against the reference's own kernel
  * text compiled for the CPU (oracle/ref_harness.cpp, built into oracle/_ref/
