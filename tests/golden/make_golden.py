@@ -29,8 +29,13 @@ from highmap_b200.inputs import fbm  # noqa: E402
 from oracle import pyoracle as po  # noqa: E402
 
 
+# where _save writes (the fixtures' own directory; a test regenerates into a
+# temporary one to check that the committed files are what this script makes)
+OUT_DIR = HERE
+
+
 def _save(name, **arrays):
-    path = os.path.join(HERE, name + ".npz")
+    path = os.path.join(OUT_DIR, name + ".npz")
     np.savez_compressed(path, **arrays)
     print("wrote", path)
 

@@ -342,3 +342,28 @@ def test_flow_simulation_viscous_matches_reference_text(shape):
         a = po.flow_simulation_viscous(z, 0.04, dm, 25, 0.5, dry, 1.3, power)
         b = po.ref_flow_simulation_viscous(z, 0.04, dm, 25, 0.5, dry, 1.3, power)
         assert np.array_equal(a, b, equal_nan=True)
+
+
+@ref_only
+def test_golden_fixtures_regenerate_bit_exact(tmp_path):
+    """Every committed fixture is exactly what tests/golden/make_golden.py
+    makes from the reference's kernel text: regenerate all groups into a
+    temporary directory and compare array by array."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    mg.OUT_DIR = str(tmp_path)
+    for group in mg.GROUPS.values():
+        group()
+    made = sorted(os.path.basename(p) for p in glob.glob(os.path.join(str(tmp_path), "*.npz")))
+    committed = sorted(os.path.basename(p) for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    assert made == committed
+    for name in made:
+        a = np.load(os.path.join(str(tmp_path), name))
+        b = np.load(os.path.join(GOLDEN, name))
+        assert sorted(a.files) == sorted(b.files), name
+        for k in a.files:
+            assert a[k].dtype == b[k].dtype, (name, k)
+            floating = np.issubdtype(a[k].dtype, np.floating)
+            assert np.array_equal(a[k], b[k], equal_nan=floating), (name, k)
