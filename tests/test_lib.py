@@ -49,6 +49,28 @@ def test_argument_checks_without_device(built_lib):
                          None) == L.HM_ERR_INVALID_ARGUMENT
     assert b"NULL" in lib.hm_last_error()
     assert lib.hm_status_string(L.HM_ERR_OUT_OF_MEMORY) == b"out of device memory"
+    # the callers and relatives check their context first too
+    zp = C.c_void_p(z.ctypes.data)
+    f = C.c_float
+    calls = {
+        "sediment_layer": lambda: lib.hm_sediment_layer(None, zp, 4, 4, zp, zp, 1, 1, None),
+        "sediment_layer_device": lambda: lib.hm_sediment_layer_device(None, zp, 4, 4, zp, zp, 1, 1, None, None),
+        "snow_post_filter": lambda: lib.hm_snow_post_filter(None, zp, zp, 4, 4, f(0.1), 1, f(0.2)),
+        "snow_post_filter_device": lambda: lib.hm_snow_post_filter_device(None, zp, zp, 4, 4, f(0.1), 1, f(0.2),
+                                                                          None),
+        "thermal_flatten": lambda: lib.hm_thermal_flatten(None, zp, 4, 4, zp, 1, f(0.5), f(0.0), None),
+        "thermal_inflate": lambda: lib.hm_thermal_inflate(None, zp, 4, 4, zp, 1, None),
+        "thermal_rib": lambda: lib.hm_thermal_rib(None, zp, 4, 4, 1, None),
+        "thermal_relief_device": lambda: lib.hm_thermal_relief_device(None, 4, zp, 4, 4, zp, f(0.5), f(0.0), 1, None,
+                                                                      None),
+        "flow_simulation_viscous": lambda: lib.hm_flow_simulation_viscous(None, zp, 4, 4, f(0.01), zp, 1, f(0.5),
+                                                                          f(0.0), f(1.0), f(2.5), zp),
+        "flow_simulation_viscous_device": lambda: lib.hm_flow_simulation_viscous_device(
+            None, zp, 4, 4, f(0.01), zp, 1, f(0.5), f(0.0), f(1.0), f(2.5), zp, None),
+    }
+    for name, call in calls.items():
+        assert call() == L.HM_ERR_INVALID_ARGUMENT, name
+        assert b"NULL" in lib.hm_last_error(), name
 
 
 def test_defaults_match_reference_signature(built_lib):
