@@ -61,14 +61,17 @@ def _args():
     ap.add_argument("--size", type=int, default=N_SIDE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=["plain", "batch", "serve", "sweep", "extras"], default="plain",
+    ap.add_argument("--form", choices=["plain", "batch", "serve", "sweep", "extras", "parity"], default="plain",
                     help="plain: the drop-in headline; batch: 256 mixed jobs batched vs plain calls; "
                          "serve: Poisson request stream, continuous batching vs plain FIFO; "
                          "sweep: thermal and vpipes at 1024^2..16384^2, 200 iterations, rates and errors; "
-                         "extras: thermal_auto_bedrock, flow_simulation and the sibling talus stencils at 4096^2")
+                         "extras: thermal_auto_bedrock, flow_simulation and the sibling talus stencils at 4096^2; "
+                         "parity: thermal x500 and vpipes x1000 at 4096^2, GPU vs the reference's kernel text and "
+                         "fp64 on the host cores")
     ap.add_argument("--sizes", default="1024,2048,4096,8192,16384", help="grid sides of the sweep form")
     ap.add_argument("--jobs", type=int, default=256, help="jobs of the batch form")
-    ap.add_argument("--requests", type=int, default=100, help="requests per rate of the serve form")
+    ap.add_argument("--requests", type=int, default=10000, help="requests per rate of the serve form")
+    ap.add_argument("--rates", default="40,120", help="arrival rates (requests/s) of the serve form")
     ap.add_argument("--vpipes-launch", default=None,
                     help="fused vpipes launch shape 'tpb,radius,rows' (default: built-in choice)")
     a = ap.parse_args()
@@ -234,12 +237,30 @@ def _composite(cells, rate_t, rate_v):
     return cells * (THERMAL_ITERS + VPIPES_ITERS) / step_s
 
 
+REF_THERMAL_EXTRA = 8  # thermal iterations a reference step adds beyond its 1-iteration call
+REF_VPIPES_EXTRA = 4   # vpipes iterations likewise
+
+
 def run_reference(a):
+    """The reference's CPU implementation of the path (its kernel text
+    compiled for the host, oracle/_ref; the restatement where that library
+    is absent) on all host threads.
+
+    A full step of the workload (500 thermal + 1000 vpipes iterations at
+    4096^2) takes minutes on the host, so each timed step is a bounded
+    sample of it: one thermal call of 1 iteration and one of
+    1 + REF_THERMAL_EXTRA, one vpipes call of 1 and one of
+    1 + REF_VPIPES_EXTRA, all on the full inputs.  The per-iteration cost
+    of each solver is the difference of the two calls, summed over the
+    timed steps, so a call's fixed costs (copies of the inputs, buffer
+    set-up, thread start-up) are not charged to its iterations; the
+    metric is the composite rate of 500 + 1000 iterations at those
+    per-iteration costs.  `ms_per_step` is the measured time of one sample
+    step; the time a full workload step would take is extrapolated
+    (`workload_ms_per_step_extrapolated`)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import numpy as np
-
     from oracle import pyoracle as po
     n = a.size
     cells = float(n) * n
@@ -248,35 +269,47 @@ def run_reference(a):
     kind = "reference" if use_ref else "port"
     th = po.ref_thermal if use_ref else po.thermal
     vp = po.ref_vpipes if use_ref else po.vpipes
-    p1 = po.VpipesParams.make(**dict(CONFIG2_VPIPES, iterations=1))
+    mt, mv = REF_THERMAL_EXTRA, REF_VPIPES_EXTRA
+    pv_short = po.VpipesParams.make(**dict(CONFIG2_VPIPES, iterations=1))
+    pv_long = po.VpipesParams.make(**dict(CONFIG2_VPIPES, iterations=1 + mv))
+
+    def timed(fn):
+        t = time.perf_counter()
+        fn()
+        return time.perf_counter() - t
 
     def step():
-        t0 = time.perf_counter()
-        th(z, talus, 1, bedrock=bed)
-        t1 = time.perf_counter()
-        vp(z, p1)
-        t2 = time.perf_counter()
-        return t1 - t0, t2 - t1
+        t1 = timed(lambda: th(z, talus, 1, bedrock=bed))
+        tk = timed(lambda: th(z, talus, 1 + mt, bedrock=bed))
+        v1 = timed(lambda: vp(z, pv_short))
+        vk = timed(lambda: vp(z, pv_long))
+        return tk - t1, vk - v1, t1 + tk + v1 + vk
 
     for _ in range(a.warmup):
         step()
-    tt = tv = 0.0
+    dt_th = dt_vp = wall = 0.0
     for _ in range(a.steps):
-        x, y = step()
-        tt += x
-        tv += y
-    rate_t = cells * a.steps / tt
-    rate_v = cells * a.steps / tv
+        x, y, w = step()
+        dt_th += x
+        dt_vp += y
+        wall += w
+    # guard against a difference at the timer's resolution
+    rate_t = cells * mt * a.steps / max(dt_th, 1e-9)
+    rate_v = cells * mv * a.steps / max(dt_vp, 1e-9)
     value = _composite(cells, rate_t, rate_v)
-    ms = 1e3 * cells * (THERMAL_ITERS + VPIPES_ITERS) / value
     cores = po.num_threads()
-    sample = ("each step: 1 thermal + 1 vpipes iteration on the full %dx%d inputs, extrapolated to %d + %d "
-              "iterations" % (n, n, THERMAL_ITERS, VPIPES_ITERS))
+    sample = ("each step: thermal calls of 1 and %d iterations and vpipes calls of 1 and %d iterations on the full "
+              "%dx%d inputs; per-iteration cost = difference of the two calls (fixed per-call costs excluded), "
+              "extrapolated to %d + %d iterations" % (1 + mt, 1 + mv, n, n, THERMAL_ITERS, VPIPES_ITERS))
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": _config(n),
-        "per_solver": {"thermal_cell_updates_per_s": rate_t, "vpipes_cell_updates_per_s": rate_v},
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": _config(n),
+        "extrapolated": True,
+        "workload_ms_per_step_extrapolated": 1e3 * cells * (THERMAL_ITERS + VPIPES_ITERS) / value,
+        "per_solver": {"thermal_cell_updates_per_s": rate_t, "vpipes_cell_updates_per_s": rate_v,
+                       "thermal_iterations_differenced": mt * a.steps,
+                       "vpipes_iterations_differenced": mv * a.steps},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -583,6 +616,114 @@ def run_sweep(a):
     return 0
 
 
+# ---------------------------------------------------------------- parity
+
+def _material(z, s=None):
+    """fp64 sum of the terrain (plus suspended sediment for vpipes)."""
+    import numpy as np
+    t = float(z.astype(np.float64).sum())
+    return t + (float(s.astype(np.float64).sum()) if s is not None else 0.0)
+
+
+def run_parity(a):
+    """The plain drop-in configuration at full length on the full grid,
+    GPU against the reference's kernel text on the host cores and against
+    an fp64 run of the same scheme: thermal (talus map, bedrock 0.3 z,
+    500 iterations) and vpipes (1000 iterations) at 4096^2.
+
+    Thermal runs twice on the GPU: in the bedrock mode the benchmark
+    measures (update, then clamp to the bedrock), compared with the fp32
+    and fp64 oracle (the reference text has only the literal mode), and in
+    the reference's literal mode, compared with the reference text itself.
+    Vpipes is compared with the reference text (fp32) and the fp64 oracle.
+    Each comparison reports max and mean |difference| as a fraction of the
+    input's height range, the relative L1 distance of HighMap's array
+    comparison, bit-exactness, and mass drift: |sum z_T - sum z_0| /
+    sum |z_0| for thermal, the same over terrain plus suspended sediment
+    for vpipes (rain and evaporation change the water itself)."""
+    import numpy as np
+    import torch
+
+    from highmap_b200 import gpu as G
+    from oracle import pyoracle as po
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if not G.init_opencl():
+        raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
+    if not po.ref_available():
+        raise RuntimeError("the reference's kernel text (oracle/_ref/libhm_ref.so) is not built")
+    ctx = G.Context(local)
+    n = a.size
+    z0, talus, bed = _inputs(n)
+    base = _material(z0)
+    den = float(np.abs(z0.astype(np.float64)).sum())
+    t0 = time.perf_counter()
+
+    # GPU: host buffers through the C-ABI, as a caller of the drop-in would
+    z_int = z0.copy()
+    G.thermal(z_int, talus, THERMAL_ITERS, bedrock=bed, ctx=ctx)
+    z_lit = z0.copy()
+    G.thermal(z_lit, talus, THERMAL_ITERS, bedrock=bed, bedrock_mode=G.BEDROCK_LITERAL, ctx=ctx)
+    z_vp = z0.copy()
+    s_vp = np.empty_like(z0)
+    w_vp = np.empty_like(z0)
+    G.hydraulic_vpipes(z_vp, iterations=VPIPES_ITERS, water_depth=w_vp, sediment=s_vp, ctx=ctx, **CONFIG2_VPIPES)
+    ctx.close()
+    t_gpu = time.perf_counter() - t0
+
+    # host: the reference's kernel text and the oracle, all cores
+    t1 = time.perf_counter()
+    o32_int, _ = po.thermal(z0, talus, THERMAL_ITERS, bedrock=bed)
+    o64_int, _ = po.thermal(z0, talus, THERMAL_ITERS, bedrock=bed, dtype=np.float64)
+    r_lit, _ = po.ref_thermal(z0, talus, THERMAL_ITERS, bedrock=bed)
+    pp = po.VpipesParams.make(**dict(CONFIG2_VPIPES, iterations=VPIPES_ITERS))
+    r_vp = po.ref_vpipes(z0, pp)
+    o64_vp = po.vpipes(z0, pp, dtype=np.float64)
+    t_cpu = time.perf_counter() - t1
+
+    def drift(m):
+        return abs(m - base) / den
+
+    th = {
+        "intended_bedrock": {
+            "gpu_vs_oracle_fp32": _errors(z_int, o32_int, z0),
+            "gpu_vs_fp64": _errors(z_int, o64_int, z0),
+            "oracle_fp32_vs_fp64": _errors(o32_int, o64_int, z0),
+            "mass_drift": {"gpu": drift(_material(z_int)), "oracle_fp32": drift(_material(o32_int)),
+                           "fp64": drift(_material(o64_int))}},
+        "literal_bedrock": {
+            "gpu_vs_reference_text": _errors(z_lit, r_lit, z0),
+            "mass_drift": {"gpu": drift(_material(z_lit)), "reference_text": drift(_material(r_lit))}},
+    }
+    rz, rw, rs = r_vp[0], r_vp[1], r_vp[2]
+    vp = {
+        "gpu_vs_reference_text": {"z": _errors(z_vp, rz, z0), "sediment": _errors(s_vp, rs, z0),
+                                  "water_depth": _errors(w_vp, rw, z0)},
+        "gpu_vs_fp64": {"z": _errors(z_vp, o64_vp[0], z0), "sediment": _errors(s_vp, o64_vp[2], z0)},
+        "reference_text_vs_fp64": {"z": _errors(rz, o64_vp[0], z0), "sediment": _errors(rs, o64_vp[2], z0)},
+        "material_drift": {"gpu": drift(_material(z_vp, s_vp)), "reference_text": drift(_material(rz, rs)),
+                           "fp64": drift(_material(o64_vp[0], o64_vp[2]))},
+        "water_depth_max": {"gpu": float(w_vp.max()), "reference_text": float(rw.max())},
+    }
+    tol = {"thermal": 1e-4, "vpipes": 1e-3}
+    ok = (th["intended_bedrock"]["gpu_vs_oracle_fp32"]["max_abs_of_range"] <= tol["thermal"] and
+          th["literal_bedrock"]["gpu_vs_reference_text"]["max_abs_of_range"] <= tol["thermal"] and
+          vp["gpu_vs_reference_text"]["z"]["max_abs_of_range"] <= tol["vpipes"])
+    out = {"metric": "max/mean abs error (fraction of the height range) and mass drift after the full iteration "
+                     "counts, GPU vs the reference's kernel text and vs fp64",
+           "value": vp["gpu_vs_reference_text"]["z"]["max_abs_of_range"], "unit": "fraction of height range",
+           "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic", "form": "parity",
+           "within_tolerance": ok, "tolerance_of_range": tol,
+           "config": dict(_config(n), workload="plain drop-ins at full length, %dx%d: thermal x%d, vpipes x%d"
+                          % (n, n, THERMAL_ITERS, VPIPES_ITERS)),
+           "host": {"cores": po.num_threads(), "cpu_s": t_cpu, "gpu_path_s": t_gpu},
+           "thermal": th, "vpipes": vp}
+    print(json.dumps(out), flush=True)
+    return 0 if ok else 1
+
+
 # ---------------------------------------------------------------- extras
 
 AUTO_BEDROCK_BYTES = 16.0  # z in and out, talus, z0 (the bedrock grid is folded away)
@@ -792,14 +933,15 @@ def run_form(a):
                           "iterations": "uniform 50..1000", "kinds": "half thermal, half vpipes"},
                "detail": r}
     else:
-        r = forms.run_serve_benchmark(n_requests=a.requests, rates=(10.0, 30.0, 100.0))
+        rates = tuple(float(x) for x in a.rates.split(","))
+        r = forms.run_serve_benchmark(n_requests=a.requests, rates=rates)
         best = max(r["sweep"], key=lambda x: x["served"]["cell_updates_per_s"])
         out = {"metric": "served cell-updates/s and p50/p99 latency, Poisson requests (256..4096, 20..2000 "
                          "iterations), continuous batching vs plain FIFO",
                "value": best["served"]["cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": 1,
                "higher_is_better": True, "dtype": "f32", "data": "synthetic", "form": "serve",
                "config": {"workload": "served form", "requests_per_rate": a.requests,
-                          "budget_bytes": 120 << 30, "rates_per_s": [10.0, 30.0, 100.0]},
+                          "budget_bytes": 120 << 30, "rates_per_s": list(rates)},
                "detail": r}
     print(json.dumps(out), flush=True)
     return 0
@@ -813,6 +955,8 @@ def main():
         return run_sweep(a)
     if a.form == "extras":
         return run_extras(a)
+    if a.form == "parity":
+        return run_parity(a)
     if a.form != "plain":
         return run_form(a)
     return run_ours(a)

@@ -78,9 +78,36 @@ def _plain(s, z, ctx, stream):
         G.hydraulic_vpipes_device(z, p, ctx=ctx, stream=stream)
 
 
-def run_batch_benchmark(n_jobs=256, seed=0, check=4):
+def _peak_rates(ctx, stream, side=2048, iters=200):
+    """Cell-updates/s of one large plain solve of each kind (the plain
+    path's speed where launches are not the limit)."""
+    import torch
+    out = {}
+    z0 = torch.from_numpy(fbm(side, side, seed=99)).cuda()
+    for kind in ("thermal", "vpipes"):
+        s = dict(kind=kind, nx=side, ny=side, iterations=iters, talus=1.0 / side, rain=1e-4)
+        z = z0.clone()
+        _plain(s, z, ctx, stream)
+        z = z0.clone()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _plain(s, z, ctx, stream)
+        e1.record()
+        torch.cuda.synchronize()
+        out[kind] = side * side * iters / (e0.elapsed_time(e1) * 1e-3)
+    return out
+
+
+def run_batch_benchmark(n_jobs=256, seed=0):
     """Aggregate cell-updates/s of the batched run and of plain per-job
-    calls on the same jobs; `check` jobs are compared bit for bit."""
+    calls on the same jobs, every job's result compared bit for bit.
+
+    Also the ceiling of the ratio on this job mix: the plain path runs a
+    large grid near its own per-cell speed, so batching can only win back
+    what plain calls lose on grids too small to fill the GPU.  ideal_s is
+    the whole mix at the per-cell speed of one large plain solve of each
+    kind; plain_s / ideal_s bounds any batched form's speed-up, and the
+    per-size breakdown shows where plain calls lose time."""
     import torch
     specs = batch_specs(n_jobs, seed)
     fields = _inputs(specs)
@@ -88,21 +115,25 @@ def run_batch_benchmark(n_jobs=256, seed=0, check=4):
     cells = sum(s["nx"] * s["ny"] * s["iterations"] for s in specs)
     ctx = G.Context(torch.cuda.current_device())
     stream = torch.cuda.current_stream().cuda_stream
+    peak = _peak_rates(ctx, stream)
 
-    # plain: one call per job, device-resident inputs
-    zs = [h.cuda() for h in host]
-    _plain(specs[0], zs[0].clone(), ctx, stream)  # warm the workspace
+    # plain: one call per job, device-resident inputs, each timed
+    big = max(specs, key=lambda s: s["nx"] * s["ny"])
+    for kind in ("thermal", "vpipes"):  # warm the workspace at the largest size
+        _plain(dict(big, kind=kind, iterations=2), host[0].new_zeros((big["ny"], big["nx"])).cuda(), ctx, stream)
     torch.cuda.synchronize()
     zs = [h.cuda() for h in host]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in specs]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for s, z in zip(specs, zs):
+    for s, z, (a, b) in zip(specs, zs, ev):
+        a.record()
         _plain(s, z, ctx, stream)
+        b.record()
     e1.record()
     torch.cuda.synchronize()
     plain_s = e0.elapsed_time(e1) * 1e-3
-    plain_out = [z[:4].cpu() for z in zs[:check]]
-    del zs
+    per_job = [a.elapsed_time(b) * 1e-3 for a, b in ev]
 
     # batched: every job in one graph-captured batch
     zb = [h.cuda() for h in host]
@@ -112,14 +143,31 @@ def run_batch_benchmark(n_jobs=256, seed=0, check=4):
     B.run(jobs, use_graph=True, ctx=ctx)
     torch.cuda.synchronize()
     batch_s = time.perf_counter() - t0
-    same = all(torch.equal(z[:4].cpu(), p) for z, p in zip(zb[:check], plain_out))
+    mismatched = [k for k, (a, b) in enumerate(zip(zb, zs)) if not torch.equal(a, b)]
+    del zs, zb
     ctx.close()
+
+    ideal_s = sum(s["nx"] * s["ny"] * s["iterations"] / peak[s["kind"]] for s in specs)
+    bands = []
+    for lo, hi in ((0, 256 * 256), (256 * 256, 512 * 512), (512 * 512, 1024 * 1024), (1024 * 1024, 1 << 30)):
+        idx = [k for k, s in enumerate(specs) if lo <= s["nx"] * s["ny"] < hi]
+        if not idx:
+            continue
+        w = sum(specs[k]["nx"] * specs[k]["ny"] * specs[k]["iterations"] for k in idx)
+        t = sum(per_job[k] for k in idx)
+        ideal = sum(specs[k]["nx"] * specs[k]["ny"] * specs[k]["iterations"] / peak[specs[k]["kind"]] for k in idx)
+        bands.append({"cells_from": lo, "cells_below": hi, "jobs": len(idx), "share_of_work": w / cells,
+                      "plain_s": t, "share_of_plain_time": t / plain_s, "plain_over_ideal": t / ideal})
     return {
         "jobs": n_jobs, "cell_updates": cells,
         "batched_cell_updates_per_s": cells / batch_s, "plain_cell_updates_per_s": cells / plain_s,
         "speedup": plain_s / batch_s, "batched_s": batch_s, "plain_s": plain_s,
-        "batched_includes": "admission, state init, graph capture and instantiation, all rounds",
-        "bit_identical_to_plain_sample": same,
+        "batched_includes": "admission, state init, graph capture and instantiation, all rounds (host clock)",
+        "plain_includes": "one device call per job, back to back (CUDA events)",
+        "peak_plain_cell_updates_per_s_2048": peak,
+        "ideal_s_at_peak_rates": ideal_s, "speedup_ceiling": plain_s / ideal_s,
+        "by_size": bands,
+        "jobs_compared": n_jobs, "jobs_bit_identical": n_jobs - len(mismatched), "mismatched_jobs": mismatched,
     }
 
 
@@ -227,7 +275,7 @@ class CudaLanes:
 
 
 def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=64, large_cells=1024 * 1024, lanes=None,
-          clock=time.perf_counter, sleep=time.sleep):
+          clock=time.perf_counter, sleep=time.sleep, on_done=None):
     """Size-aware continuous batching: returns per-request latencies (s) and
     totals.
 
@@ -242,7 +290,8 @@ def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=64, large_cells=10
     next batched job completes, at most `rounds_per_tick` rounds (which
     bounds how long an arrival waits for admission).  `lanes` is the device
     side (CudaLanes over `pool` by default); `clock` and `sleep` the time
-    source."""
+    source; `on_done(request, handle)` (optional) sees every completed
+    request with its lane's handle, whose first item is the result grid."""
     own = lanes is None
     if own:
         lanes = CudaLanes(pool)
@@ -264,6 +313,8 @@ def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=64, large_cells=10
             r = big[0]
             lat[r["id"]] = clock() - t0 - r["arrival"]
             cells += r["nx"] * r["ny"] * r["iterations"]
+            if on_done:
+                on_done(r, big[1])
             big = None
         if big is None and big_queue:
             r = big_queue.pop(0)
@@ -287,9 +338,11 @@ def serve(reqs, pool, budget_bytes=120 << 30, rounds_per_tick=64, large_cells=10
         done_t = clock() - t0
         for jid in list(active):
             if lanes.status(jid)[1]:
-                r, _ = active.pop(jid)
+                r, job = active.pop(jid)
                 lat[r["id"]] = done_t - r["arrival"]
                 cells += r["nx"] * r["ny"] * r["iterations"]
+                if on_done:
+                    on_done(r, job)
                 lanes.release(jid)
     total = clock() - t0
     if own:
@@ -323,43 +376,48 @@ def _pct(v, q):
     return float(np.percentile(np.asarray(v), q)) if v else None
 
 
-def run_serve_benchmark(n_requests=200, rates=(2.0, 8.0, 32.0), seed=0, check=3):
+def run_serve_benchmark(n_requests=10000, rates=(40.0, 120.0), seed=0, sample_every=100):
     """Throughput and p50/p99 latency of the served form and of the plain
-    path for each arrival rate; `check` requests are re-solved alone and
-    compared bit for bit with their served result."""
+    path (first come first served, one call per request) for each arrival
+    rate, on the same request stream.  Every `sample_every`-th request's
+    served result is kept and compared with the same request solved alone
+    by the plain path: bit-identical count and max abs difference as a
+    fraction of the request's input height range."""
     import torch
     pool = FieldPool()
     out = []
     for rate in rates:
         reqs = serve_requests(n_requests, rate, seed)
-        lat_b, cells_b, tot_b = serve(reqs, pool)
-        lat_p, cells_p, tot_p = serve_plain(reqs, pool)
-        out.append({
-            "rate_per_s": rate, "requests": n_requests,
-            "served": {"cell_updates_per_s": cells_b / tot_b, "p50_s": _pct(list(lat_b.values()), 50),
-                       "p99_s": _pct(list(lat_b.values()), 99), "wall_s": tot_b},
-            "plain": {"cell_updates_per_s": cells_p / tot_p, "p50_s": _pct(list(lat_p.values()), 50),
-                      "p99_s": _pct(list(lat_p.values()), 99), "wall_s": tot_p},
-        })
-    # results of the served path equal the plain path's
-    reqs = serve_requests(check, 100.0, seed + 1, hi=512, it_hi=200)
-    b = B.Batch(G.Context(torch.cuda.current_device()))
-    zs, ids = [], []
-    for r in reqs:
-        z = pool.take(r["id"], r["nx"], r["ny"])
-        zs.append(z)
-        torch.cuda.current_stream().synchronize()
-        ids.append(b.add(_job(r, z)))
-    while not all(b.status(i)[1] for i in ids):
-        b.step(16)
-    b.synchronize()
-    ctx = G.Context(torch.cuda.current_device())
-    same = True
-    for r, z in zip(reqs, zs):
-        w = pool.take(r["id"], r["nx"], r["ny"])
-        _plain(r, w, ctx, torch.cuda.current_stream().cuda_stream)
+        kept = {}
+
+        def keep(r, handle):
+            if r["id"] % sample_every == 0:
+                kept[r["id"]] = (r, handle[0])
+        lat_b, cells_b, tot_b = serve(reqs, pool, on_done=keep)
         torch.cuda.synchronize()
-        same = same and bool(torch.equal(w, z))
-    b.close()
-    ctx.close()
-    return {"sweep": out, "bit_identical_to_plain_sample": same}
+        lat_p, cells_p, tot_p = serve_plain(reqs, pool)
+        # served results against the plain path, request by request
+        ctx = G.Context(torch.cuda.current_device())
+        same, worst = 0, 0.0
+        for rid, (r, z) in sorted(kept.items()):
+            z0 = pool.take(r["id"], r["nx"], r["ny"])
+            w = z0.clone()
+            _plain(r, w, ctx, torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            rng = float(z0.max() - z0.min()) or 1.0
+            worst = max(worst, float((w - z).abs().max()) / rng)
+            same += int(torch.equal(w, z))
+        ctx.close()
+        lb, lp = list(lat_b.values()), list(lat_p.values())
+        out.append({
+            "rate_per_s": rate, "requests": n_requests, "completed": {"served": len(lb), "plain": len(lp)},
+            "served": {"cell_updates_per_s": cells_b / tot_b, "p50_s": _pct(lb, 50), "p99_s": _pct(lb, 99),
+                       "wall_s": tot_b},
+            "plain": {"cell_updates_per_s": cells_p / tot_p, "p50_s": _pct(lp, 50), "p99_s": _pct(lp, 99),
+                      "wall_s": tot_p},
+            "throughput_ratio": (cells_b / tot_b) / (cells_p / tot_p),
+            "vs_plain": {"sampled": len(kept), "bit_identical": same, "max_abs_of_range": worst},
+        })
+        del kept
+        torch.cuda.empty_cache()
+    return {"sweep": out}

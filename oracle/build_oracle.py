@@ -10,8 +10,8 @@
   _common_math.cl and _common_rand.cl) compiled for the CPU behind
   ``ref_shim.h``, linked
   with the host-driver restatement ``ref_harness.cpp``.  Built only where
-  the reference tree is present (``HM_REFERENCE_ROOT``, default
-  /root/reference); the kernel files are read in place and streamed to the
+  the reference tree is present (``HM_REFERENCE_ROOT``, default: a
+  ``reference`` directory beside the repository); the kernel files are read in place and streamed to the
   compiler, nothing of them is written anywhere but the object in _ref/.
 
 Run: ``python oracle/build_oracle.py`` (``build()`` in the repository's
@@ -38,7 +38,12 @@ CFLAGS = ["-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-march=x86-64-v2"]
 
 
 def reference_root() -> str:
-    return os.environ.get("HM_REFERENCE_ROOT", "/root/reference")
+    """The HighMap checkout: HM_REFERENCE_ROOT, else a directory named
+    ``reference`` beside the repository's root."""
+    env = os.environ.get("HM_REFERENCE_ROOT")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 
 def _run(cmd, **kw):

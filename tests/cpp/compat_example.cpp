@@ -6,7 +6,7 @@
  * requested solver, writes the results as raw float32 for the test to
  * compare with the oracle.
  *
- * usage: compat_example <thermal|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition|layer|flatten|inflate|rib|viscous>
+ * usage: compat_example <thermal|config1|thermal_scalar|thermal_mask|auto_bedrock|auto_bedrock_mask|vpipes|flow|ridge|scree|schott|olsen|deposition|layer|flatten|inflate|rib|viscous>
  *        nx ny in.f32 out_prefix
  */
 #include <cstdio>
@@ -55,6 +55,15 @@ int main(int argc, char **argv)
       hmap::Array mask(shape, 0.25f);
       hmap::gpu::thermal(z, &mask, talus, 50, nullptr, &depo);
     }
+    write_raw(out + "_z.f32", z);
+    write_raw(out + "_depo.f32", depo);
+  }
+  else if (mode == "config1")
+  {
+    /* the thermal benchmark configuration: uniform talus 1/256, no bedrock,
+     * 100 iterations, deposition map */
+    hmap::Array depo;
+    hmap::gpu::thermal(z, 1.f / 256.f, 100, nullptr, &depo);
     write_raw(out + "_z.f32", z);
     write_raw(out + "_depo.f32", depo);
   }

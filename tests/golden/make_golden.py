@@ -8,7 +8,7 @@ thermal_ridge.cl, thermal_scree.cl, thermal_schott.cl, thermal_olsen.cl) compile
 for the CPU by oracle/build_oracle.py and driven by oracle/ref_harness.cpp
 (Jacobi form).  Run in a checkout where the reference tree is present:
 
-    python tests/golden/make_golden.py [thermal] [vpipes] [flow_simulation] [siblings] [deposition]
+    python tests/golden/make_golden.py [thermal] [config1] [vpipes] [flow_simulation] [siblings] [deposition]
                                      [layer] [snow] [relief] [viscous]
 
 Each .npz holds the inputs, the parameters and the outputs of one case.
@@ -193,7 +193,30 @@ def viscous_cases():
               power=np.float32(2.5), out_d=out)
 
 
-GROUPS = {"thermal": thermal_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases,
+def _digest(a):
+    """sha256 of an array's bytes, as 32 uint8 values."""
+    import hashlib
+    return np.frombuffer(hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest(), dtype=np.uint8).copy()
+
+
+def config1_cases():
+    """The thermal benchmark configuration run on the CPU, verbatim: a
+    256 x 256 fBm heightmap (seed 1, base wavenumber 4, 8 octaves,
+    persistence 0.5, lacunarity 2, remapped to [0, 1]), uniform talus
+    1/256, no bedrock, 100 iterations, heights and deposition map.  At
+    768 KB the arrays themselves would dwarf the other fixtures, so the
+    fixture keeps sha256 digests of the input and of the reference text's
+    two outputs; the test regenerates the input and checks its digest
+    first."""
+    n = 256
+    z = fbm(n, n, seed=1)
+    talus = np.float32(1.0 / n)
+    zo, depo = po.ref_thermal(z, np.full_like(z, talus), 100, deposition=True)
+    _save("config1_thermal_256", z_sha256=_digest(z), talus=talus, iterations=np.int32(100),
+          out_z_sha256=_digest(zo), out_depo_sha256=_digest(depo))
+
+
+GROUPS = {"thermal": thermal_cases, "config1": config1_cases, "vpipes": vpipes_cases, "flow_simulation": flow_simulation_cases,
           "siblings": sibling_cases, "deposition": deposition_cases,
           "layer": layer_cases, "snow": snow_cases, "relief": relief_cases,
           "viscous": viscous_cases}

@@ -46,6 +46,16 @@ def test_thermal(gpu, example, tmp_path):
     assert np.array_equal(load("depo"), depo)
 
 
+def test_config1_through_cpp(gpu, example, tmp_path):
+    """The thermal benchmark configuration (256^2 fBm seed 1, talus 1/256,
+    100 iterations) through hmap::gpu::thermal(Array&, float, ...)."""
+    z = fbm(256, 256, seed=1)
+    load = _run(example, "config1", z, tmp_path)
+    want, depo = po.thermal(z, np.float32(1 / 256), 100, deposition=True)
+    assert np.array_equal(load("z"), want)
+    assert np.array_equal(load("depo"), depo)
+
+
 def test_thermal_mask(gpu, example, tmp_path):
     z = fbm(128, 128, seed=4)
     load = _run(example, "thermal_mask", z, tmp_path)

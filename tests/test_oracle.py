@@ -32,6 +32,22 @@ def _params(g):
     return po.VpipesParams.make(**json.loads(str(g["params"])))
 
 
+def test_config1_golden_digests():
+    """The thermal benchmark configuration (256^2 fBm seed 1, talus 1/256,
+    100 iterations): the generated input and the oracle's heights and
+    deposition map have the digests of the reference text's outputs."""
+    import hashlib
+
+    def digest(a):
+        return np.frombuffer(hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest(), dtype=np.uint8)
+    g = _load("config1_thermal_256")
+    z0 = fbm(256, 256, seed=1)
+    assert np.array_equal(digest(z0), g["z_sha256"])
+    z, depo = po.thermal(z0, np.float32(g["talus"]), int(g["iterations"]), deposition=True)
+    assert np.array_equal(digest(z), g["out_z_sha256"])
+    assert np.array_equal(digest(depo), g["out_depo_sha256"])
+
+
 @pytest.mark.parametrize("name", ["thermal_uniform", "thermal_talus_map", "thermal_masked", "thermal_small_3x3",
                                   "thermal_small_5x17", "thermal_small_33x7"])
 def test_thermal_golden_bit_exact(name):
