@@ -42,6 +42,7 @@ EXPORTED = (
     "hm_batch_synchronize", "hm_batch_job_status", "hm_batch_release", "hm_batch_bytes_in_use",
     "hm_batch_round", "hm_batch_run",
     "hm_autotune", "hm_autotune_save", "hm_autotune_load", "hm_autotune_clear", "hm_vpipes_set_algorithm",
+    "hm_debug_tma_expect_extra",
 )
 
 HM_JOB_THERMAL = 1
@@ -168,6 +169,7 @@ def _declare(lib):
     lib.hm_batch_run.argtypes = [vp, vp, i, i]
     lib.hm_autotune.argtypes = [vp, i, i, i, i, vp]
     lib.hm_vpipes_set_algorithm.argtypes = [i]
+    lib.hm_debug_tma_expect_extra.argtypes = [C.c_uint]
     lib.hm_autotune_save.argtypes = [C.c_char_p]
     lib.hm_autotune_load.argtypes = [C.c_char_p, C.POINTER(i)]
     for name in EXPORTED:

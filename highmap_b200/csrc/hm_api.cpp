@@ -544,16 +544,19 @@ int hm_vpipes(hm_context *ctx, float *z, int nx, int ny, const hm_vpipes_params 
     cudaStreamSynchronize(s);
     return st;
   }
-  HM_CUDA_TRY(cudaMemcpyAsync(z, dz, nbytes, cudaMemcpyDeviceToHost, s));
-  if (dd) HM_CUDA_TRY(cudaMemcpyAsync(water_depth, dd, nbytes, cudaMemcpyDeviceToHost, s));
-  if (ds) HM_CUDA_TRY(cudaMemcpyAsync(sediment, ds, nbytes, cudaMemcpyDeviceToHost, s));
-  if (du) HM_CUDA_TRY(cudaMemcpyAsync(vel_u, du, nbytes, cudaMemcpyDeviceToHost, s));
-  if (dv) HM_CUDA_TRY(cudaMemcpyAsync(vel_v, dv, nbytes, cudaMemcpyDeviceToHost, s));
+  /* a tile whose loads timed out wrote nothing: report it before the
+   * results reach the caller's buffers, which then keep their contents */
   unsigned dev_error = 0;
   HM_CUDA_TRY(cudaMemcpyAsync(&dev_error, hm::vpipes_error_word(scr, nx, ny), sizeof dev_error,
                               cudaMemcpyDeviceToHost, s));
   HM_CUDA_TRY(cudaStreamSynchronize(s));
   if (dev_error) return hm::fail(HM_ERR_TIMEOUT, "hm_vpipes: tile loads timed out on the device");
+  HM_CUDA_TRY(cudaMemcpyAsync(z, dz, nbytes, cudaMemcpyDeviceToHost, s));
+  if (dd) HM_CUDA_TRY(cudaMemcpyAsync(water_depth, dd, nbytes, cudaMemcpyDeviceToHost, s));
+  if (ds) HM_CUDA_TRY(cudaMemcpyAsync(sediment, ds, nbytes, cudaMemcpyDeviceToHost, s));
+  if (du) HM_CUDA_TRY(cudaMemcpyAsync(vel_u, du, nbytes, cudaMemcpyDeviceToHost, s));
+  if (dv) HM_CUDA_TRY(cudaMemcpyAsync(vel_v, dv, nbytes, cudaMemcpyDeviceToHost, s));
+  HM_CUDA_TRY(cudaStreamSynchronize(s));
   return HM_OK;
 }
 

@@ -5,9 +5,12 @@
  * One elected thread arms a CTA-local mbarrier with the byte count of the
  * tiles and issues cp.async.bulk.tensor loads (no cluster multicast: every
  * CTA fetches its own tiles from this GPU's memory); the other threads wait
- * on the barrier's phase.  Waits are bounded: after HM_TMA_SPIN_LIMIT polls
- * the waiter gives up and reports failure so the kernel can record an error
- * and return instead of hanging.
+ * on the barrier's phase.  A waiting warp asks to be suspended until the
+ * phase completes (mbarrier.try_wait with a suspend-time hint), so it
+ * spends no issue slots polling while the boxes are in flight.  Waits are
+ * bounded twice over: by HM_TMA_WAIT_NS of the global timer and by
+ * HM_TMA_SPIN_LIMIT polls; the waiter then gives up and reports failure so
+ * the kernel can record an error and return instead of hanging.
  *
  * Tensor-map rules the host side keeps (cuTensorMapEncodeTiled): 16-byte
  * aligned base, row pitch a multiple of 16 bytes, innermost box extent a
@@ -25,6 +28,14 @@ namespace hm
 {
 
 constexpr unsigned HM_TMA_SPIN_LIMIT = 1u << 22;
+/* one wait window: a second of the global timer (the boxes of a tile land
+ * within microseconds) */
+constexpr unsigned long long HM_TMA_WAIT_NS = 1000000000ull;
+/* longest a waiting warp asks to be suspended per poll (ns); it resumes as
+ * soon as the phase completes.  0 selects the form without a hint. */
+#ifndef HM_TMA_SUSPEND_NS
+#define HM_TMA_SUSPEND_NS 20000u
+#endif
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -56,11 +67,40 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
   return ok != 0;
 }
 
-/* bounded wait for the barrier phase `parity` to complete */
+/* the same test, the warp suspended until the phase completes or
+ * `hint_ns` nanoseconds have passed */
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t *bar, unsigned parity, unsigned hint_ns)
+{
+  unsigned ok;
+  asm volatile("{\n"
+               ".reg .pred p;\n"
+               "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+               "selp.u32 %0, 1, 0, p;\n"
+               "}\n"
+               : "=r"(ok)
+               : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+               : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+/* bounded wait for the barrier phase `parity` to complete: true once it
+ * has, false after HM_TMA_WAIT_NS or HM_TMA_SPIN_LIMIT polls */
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
 {
+  const unsigned long long t0 = global_ns();
   for (unsigned i = 0; i < HM_TMA_SPIN_LIMIT; i++)
-    if (mbar_try_wait(bar, parity)) return true;
+  {
+    if (HM_TMA_SUSPEND_NS ? mbar_try_wait_suspend(bar, parity, HM_TMA_SUSPEND_NS) : mbar_try_wait(bar, parity))
+      return true;
+    if (global_ns() - t0 > HM_TMA_WAIT_NS) return false;
+  }
   return false;
 }
 

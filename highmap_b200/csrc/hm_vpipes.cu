@@ -156,6 +156,8 @@ struct FusedCfg
 static FusedCfg g_cfg_override = {0, 0, 0};
 /* step kernels: 0 = tiled (k_vp_fwe + k_vp_advect), 1 = streaming (k_vp_fused) */
 static int g_algo_override = -1;
+/* bytes a TMA tile's barrier expects beyond its boxes (hm_debug_tma_expect_extra) */
+static unsigned g_tma_extra_tx = 0;
 
 FusedCfg vpipes_pick_config(int nx, int ny)
 {
@@ -350,6 +352,7 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
   io.s1 = s1;
   io.u = u_buf;
   io.v = v_buf;
+  io.tma_extra_tx = g_tma_extra_tx;
   {
     /* pair stores: an even row length and 8-byte aligned outputs */
     auto al8 = [](const void *q) { return ((uintptr_t)q & 7u) == 0; };
@@ -508,6 +511,15 @@ extern "C" int hm_vpipes_set_algorithm(int algo)
   hm::clear_error();
   if (algo < -1 || algo > 2) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes_set_algorithm: unknown algorithm");
   hm::g_algo_override = algo;
+  return HM_OK;
+}
+
+extern "C" int hm_debug_tma_expect_extra(unsigned bytes)
+{
+  hm::clear_error();
+  if (bytes % 16u != 0u || bytes > 4096u)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_debug_tma_expect_extra: bytes must be a multiple of 16, at most 4096");
+  hm::g_tma_extra_tx = bytes;
   return HM_OK;
 }
 

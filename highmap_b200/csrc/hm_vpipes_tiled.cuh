@@ -90,6 +90,8 @@ struct FweIo
   float       *u_out, *v_out; /* last step: velocity outputs, nullable */
   int          vec;           /* nx even and every output 8-byte aligned: pair stores */
   int          flow_only;     /* flow_simulation step (FWE_FLOWONLY kernels) */
+  unsigned     tma_extra_tx;  /* bytes a TMA tile's barrier expects beyond its boxes: 0, or the
+                               * test hook's count, which makes every tile's wait run out */
 };
 
 /* tensor maps of the seven input fields of one step (TMA staging):
@@ -136,7 +138,8 @@ __device__ __forceinline__ void fwe_stage_cp_async(const FweIo &io, int nx, int 
  * box; the edge test depends only on the tile, so the barrier inside it is
  * uniform).  Returns false, uniformly across the CTA, if the loads did not
  * complete in time. */
-__device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int ny, int x0, int y0, FweSmem &sm)
+__device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int ny, int x0, int y0, FweSmem &sm,
+                                              unsigned extra_tx)
 {
   const int tid = threadIdx.x;
   if (tid == 0)
@@ -147,7 +150,7 @@ __device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int n
   __syncthreads();
   if (tid == 0)
   {
-    mbar_arrive_expect_tx(&sm.bar, FWE_TMA_BYTES);
+    mbar_arrive_expect_tx(&sm.bar, FWE_TMA_BYTES + extra_tx);
     tma_load_2d(&sm.z[0][0], &maps.z, x0 - 4, y0 - 2, &sm.bar);
     tma_load_2d(&sm.d[0][0], &maps.d, x0 - 4, y0 - 2, &sm.bar);
     tma_load_2d(&sm.s[0][0], &maps.s, x0 - 4, y0 - 1, &sm.bar);
@@ -429,7 +432,7 @@ __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
     k_vp_fwe_tma(FweIo io, const __grid_constant__ FweMaps maps, VpConst c, VpScalars *sc, double *partials)
 {
   __shared__ FweSmem sm;
-  if (!fwe_stage_tma(maps, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm))
+  if (!fwe_stage_tma(maps, c.nx, c.ny, blockIdx.x * FT_TX, blockIdx.y * FT_TY, sm, io.tma_extra_tx))
   {
     if (threadIdx.x == 0) atomicOr(&sc->error, 1u);
     if (MAINTAIN)

@@ -520,6 +520,13 @@ def vpipes_set_algorithm(algo: int = VPIPES_AUTO) -> None:
     L.check(L.lib().hm_vpipes_set_algorithm(int(algo)))
 
 
+def debug_tma_expect_extra(nbytes: int = 0) -> None:
+    """Test hook: every TMA-staged vpipes tile expects ``nbytes`` more than
+    its boxes deliver, so its bounded wait runs out and the call reports
+    HM_ERR_TIMEOUT (0 turns it off)."""
+    L.check(L.lib().hm_debug_tma_expect_extra(int(nbytes)))
+
+
 def thermal_set_launch(rows: int = 0) -> None:
     """Output rows per CTA of the blocked thermal kernel (0: built-in)."""
     L.check(L.lib().hm_thermal_set_launch(int(rows)))

@@ -620,6 +620,17 @@ int hm_vpipes_set_launch(int tpb, int radius, int rows);
 #define HM_VPIPES_TILED_CP_ASYNC 2
 int hm_vpipes_set_algorithm(int algo);
 
+/* Fault injection for tests of the device-side timeout (no counterpart in
+ * the reference, whose OpenCL path has no device-side wait), process-wide:
+ * every TMA-staged vpipes tile arms its barrier with `bytes` more than its
+ * boxes deliver.  Every box still lands, but the barrier's phase cannot
+ * complete, so each tile's bounded wait runs out (about two seconds), the
+ * tile records the timeout and returns, and hm_vpipes reports
+ * HM_ERR_TIMEOUT with the caller's buffers untouched (hm_vpipes_device, being
+ * asynchronous, does not wait to read the error).  bytes must be a multiple
+ * of 16 and at most 4096; 0 (the default) turns it off. */
+int hm_debug_tma_expect_extra(unsigned bytes);
+
 /* Output rows per CTA of the temporally blocked thermal kernel,
  * process-wide (8..4096; 0 restores the built-in choice).  Results do not
  * depend on it. */
