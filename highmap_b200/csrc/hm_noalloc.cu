@@ -8,17 +8,24 @@
  * synchronises the whole device, which stalls every other stream).  For
  * them, hm_thermal_device_noalloc keeps its one piece of scratch memory,
  * the Jacobi ping-pong grid, in a statically reserved device array of
- * HM_NOALLOC_MAX_CELLS floats (16 MiB) that every GPU which loads this
- * library holds until the process exits.  The caller still passes z,
+ * HM_NOALLOC_MAX_CELLS floats (16 MiB).  The caller still passes z,
  * talus and bedrock; nothing here calls cudaMalloc, cudaFree or an
  * allocating library routine.
  *
- * Set-up: the device address of the array is looked up once per device,
- * by the first call made on that device, with that device current
- * (cudaGetSymbolAddress).  Make that first call before any stream
- * capture begins.  In host code the array's name is only a host-side
- * handle, never a device address, so only the looked-up pointer is passed
- * to the kernels.
+ * When the memory is taken: with CUDA's lazy module loading (the default
+ * since CUDA 12.2) the array, like the kernels' code, is placed on a GPU
+ * when the first call on that device loads them, not when the library is
+ * loaded; it is then held until the process exits.  An application that
+ * hands all free device memory to its own pool at start-up must therefore
+ * make its first call on each device before that (or run with
+ * CUDA_MODULE_LOADING=EAGER, which loads everything when the context is
+ * created).  Make that first call before any stream capture begins, too.
+ *
+ * Set-up: every call looks up the array's device address on the current
+ * device (cudaGetSymbolAddress, a table lookup once the module is loaded),
+ * so a context recreated after cudaDeviceReset gets the new address.  In
+ * host code the array's name is only a host-side handle, never a device
+ * address, so only the looked-up pointer is passed to the kernels.
  *
  * Sharing: every call on a device uses the same array, which keeps the
  * last call's contents.  The step kernel writes every cell of the grid it
@@ -40,30 +47,22 @@ namespace
 
 static __device__ __align__(256) float hm_noalloc_scratch[HM_NOALLOC_MAX_CELLS];
 
-constexpr int kMaxDevices = 64;
-std::mutex    g_setup_mutex;
-float        *g_scratch[kMaxDevices] = {};
+std::mutex g_setup_mutex;
 
-/* Device address of the scratch array on the current device; looked up
- * once per device. */
+/* Device address of the scratch array on the current device, looked up
+ * on every call (the first lookup on a device loads the module). */
 int scratch_for_current_device(int *device, float **out)
 {
   int         dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return hm::cuda_fail(e, "hm_thermal_device_noalloc: cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices)
-    return hm::fail(HM_ERR_NO_DEVICE, "hm_thermal_device_noalloc: device index out of range");
+  float                      *ptr = nullptr;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch[dev])
-  {
-    float *ptr = nullptr;
-    e = cudaGetSymbolAddress((void **)&ptr, hm_noalloc_scratch);
-    if (e != cudaSuccess) return hm::cuda_fail(e, "hm_thermal_device_noalloc: cudaGetSymbolAddress");
-    if (!ptr) return hm::fail(HM_ERR_CUDA, "hm_thermal_device_noalloc: scratch array has no device address");
-    g_scratch[dev] = ptr;
-  }
+  e = cudaGetSymbolAddress((void **)&ptr, hm_noalloc_scratch);
+  if (e != cudaSuccess) return hm::cuda_fail(e, "hm_thermal_device_noalloc: cudaGetSymbolAddress");
+  if (!ptr) return hm::fail(HM_ERR_CUDA, "hm_thermal_device_noalloc: scratch array has no device address");
   *device = dev;
-  *out = g_scratch[dev];
+  *out = ptr;
   return HM_OK;
 }
 

@@ -520,14 +520,17 @@ int hm_flow_simulation_viscous_device(hm_context  *ctx,
  * allocator owns the device memory, or a loop that must not stall on
  * cudaMalloc/cudaFree): the same solve as hm_thermal_device without the
  * deposition map and mask, with the Jacobi scratch grid taken from a
- * statically reserved device array of HM_NOALLOC_MAX_CELLS floats that
- * every GPU loading the library holds until exit.  No allocation, no
- * context.  Grids larger than HM_NOALLOC_MAX_CELLS cells are refused with
- * HM_ERR_INVALID_ARGUMENT.  Runs on the calling thread's current device;
- * the first call on a device looks up the array's address and should come
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race and must be serialised by the caller.  talus NULL selects
- * talus_value; bedrock is nullable. */
+ * statically reserved device array of HM_NOALLOC_MAX_CELLS floats (16 MiB).
+ * No allocation, no context.  Grids larger than HM_NOALLOC_MAX_CELLS cells
+ * are refused with HM_ERR_INVALID_ARGUMENT.  Runs on the calling thread's
+ * current device and looks up the array's address there on every call.
+ * With CUDA's lazy module loading (the default) the array is placed on a
+ * GPU by the first call on that device and held until exit: make that
+ * first call before an application pool claims the free device memory
+ * (or set CUDA_MODULE_LOADING=EAGER) and before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  talus NULL selects talus_value; bedrock is
+ * nullable. */
 #define HM_NOALLOC_MAX_CELLS (1 << 22)
 int hm_thermal_device_noalloc(float       *z,
                               int          nx,

@@ -8,15 +8,18 @@ grid is a statically reserved device array instead of workspace memory.
 Checked through the C-ABI against the allocating entry point
 hm_thermal_device on two calls in a row (the array keeps the first call's
 contents when the second starts), within the thermal tests' bar: max abs
-error <= 1e-4 of the height range, and bit-exact.  Also: a grid larger than
-the array is refused before any device work.  This file is collected last
-so a stop-at-first-failure run has already run every other test; it also
-passes on its own in a fresh process (the first call does the per-device
-set-up).
+error <= 1e-4 of the height range, and bit-exact.  Also: a repeated call
+leaves the device's free memory unchanged; the entry point works in a
+process that never created a context; a grid larger than the array is
+refused before any device work.  This file is collected last so a
+stop-at-first-failure run has already run every other test; it also passes
+on its own in a fresh process (the first call loads the array).
 """
 import ctypes as C
 import os
 import re
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -83,3 +86,53 @@ def test_noalloc_refuses_oversized_grid(gpu):
     assert st == L.HM_ERR_INVALID_ARGUMENT
     assert b"no-allocation limit" in lib.hm_last_error()
     assert torch.equal(z, before)
+
+
+def test_noalloc_repeated_call_allocates_nothing(gpu):
+    """After a first call (which loads the kernels and the array), the same
+    call again leaves the device's free memory exactly as it was."""
+    import torch
+    from highmap_b200 import _lib as L
+
+    lib = L.lib()
+    nx = ny = 2048
+    z = torch.from_numpy(fbm(nx, ny, seed=3)).cuda()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def call():
+        L.check(lib.hm_thermal_device_noalloc(_p(z), nx, ny, None, C.c_float(1.0 / nx), 20, None,
+                                              gpu.BEDROCK_INTENDED, stream))
+        torch.cuda.synchronize()
+    call()
+    free_before = torch.cuda.mem_get_info()[0]
+    call()
+    assert torch.cuda.mem_get_info()[0] == free_before
+
+
+_NO_CONTEXT = r"""
+import ctypes as C, sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np, torch
+from highmap_b200 import _lib as L
+from highmap_b200.inputs import fbm
+from oracle import pyoracle as po
+lib = L.lib()
+nx, ny = 300, 200
+z0 = fbm(nx, ny, seed=5)
+z = torch.from_numpy(z0).cuda()
+st = lib.hm_thermal_device_noalloc(C.c_void_p(z.data_ptr()), nx, ny, None, C.c_float(1.0 / nx), 25, None, 0,
+                                   C.c_void_p(torch.cuda.current_stream().cuda_stream))
+torch.cuda.synchronize()
+assert st == 0, lib.hm_last_error()
+want, _ = po.thermal(z0, np.float32(1.0 / nx), 25)
+assert np.array_equal(z.cpu().numpy(), want)
+print("no-context ok")
+"""
+
+
+def test_noalloc_in_a_process_without_context(gpu):
+    """In a fresh process that never calls hm_init or creates an
+    hm_context, the first call sets itself up and gives the oracle's bits."""
+    r = subprocess.run([sys.executable, "-c", _NO_CONTEXT, ROOT], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "no-context ok" in r.stdout
