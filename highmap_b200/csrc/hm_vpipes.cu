@@ -215,12 +215,16 @@ static size_t defer_cap(int nx, int ny)
   return cap < 4096 ? 4096 : cap;
 }
 
+/* grids of the scratch: state copy B (7), state A's d, s and fluxes (6),
+ * two copies of u, v and s1 (6: a folded step reads the previous step's
+ * and writes its own) */
+constexpr size_t VP_GRIDS = 19;
+
 size_t vpipes_scratch_bytes(int nx, int ny)
 {
   const size_t n = align_up((size_t)nx * ny, 64);
-  /* state copy B (7 grids), state A's d, s and fluxes (6 grids), u, v and
-   * s1, fp64 partials, the scalar block, the deferred list */
-  return n * sizeof(float) * 16 + partials_bytes(nx, ny) + align_up(sizeof(VpScalars), 256) +
+  /* the grids, fp64 partials, the scalar block, the deferred list */
+  return n * sizeof(float) * VP_GRIDS + partials_bytes(nx, ny) + align_up(sizeof(VpScalars), 256) +
          align_up(defer_cap(nx, ny) * sizeof(Deferred), 256);
 }
 
@@ -319,6 +323,14 @@ static bool encode_grid_map(CUtensorMap *m, const float *base, int nx, int ny, i
 
 static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
+bool adv_maps(const float *u, const float *v, const float *s1, int nx, int ny, AdvMaps *m)
+{
+  if (nx % 4 != 0 || nx < 40 || ny < FS_H) return false;
+  if (!aligned16(u) || !aligned16(v) || !aligned16(s1)) return false;
+  return encode_grid_map(&m->u, u, nx, ny, FT_H1) && encode_grid_map(&m->v, v, nx, ny, FT_H1) &&
+         encode_grid_map(&m->s1, s1, nx, ny, FS_H);
+}
+
 /* tensor maps of one state copy; false if the grid or buffers do not meet
  * the TMA rules (row pitch and bases 16-byte aligned, boxes no larger than
  * the grid) */
@@ -334,14 +346,24 @@ bool fwe_maps(const VpFields &f, int nx, int ny, FweMaps *m)
          encode_grid_map(&m->fb, f.fb, nx, ny, FT_H1);
 }
 
+/* The steps of vpipes_core with the tiled kernels.  The first step is
+ * k_vp_fwe(_tma); every later step is k_vp_step(_tma), which advects the
+ * previous step's sediment inside its own tile: u, v and s1 alternate
+ * between two copies (step k writes copy k % 2 and reads copy (k - 1) % 2),
+ * and the last step's advection runs as k_vp_advect after the loop.  Tiles
+ * are fetched by TMA where the grid and buffers allow it and allow_tma is
+ * set, else by cp.async. */
 static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &p, const VpConst &c, VpFields &A,
-                              VpFields &B, float *u_buf, float *v_buf, float *s1, const float *rain,
-                              float *water_depth, float *sediment, float *vel_u, float *vel_v, VpScalars *sc,
-                              double *partials, bool allow_tma, cudaStream_t s)
+                              VpFields &B, float *const u_buf[2], float *const v_buf[2], float *const s1_buf[2],
+                              const float *rain, float *water_depth, float *sediment, float *vel_u, float *vel_v,
+                              VpScalars *sc, double *partials, bool allow_tma, cudaStream_t s)
 {
   const size_t n = (size_t)nx * ny;
   FweMaps      maps[2];
+  AdvMaps      am[2];
   const bool   tma = allow_tma && fwe_maps(A, nx, ny, &maps[0]) && fwe_maps(B, nx, ny, &maps[1]);
+  const bool   step_tma = tma && adv_maps(u_buf[0], v_buf[0], s1_buf[0], nx, ny, &am[0]) &&
+                        adv_maps(u_buf[1], v_buf[1], s1_buf[1], nx, ny, &am[1]);
   FweIo        io;
   memset(&io, 0, sizeof io);
   io.rain = rain;
@@ -349,15 +371,13 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
   io.diffusion = p.flux_diffusion != 0;
   io.pl_one = p.pipe_length == 1.f;
   io.kexp_one = p.k_discharge_exp == 1.f;
-  io.s1 = s1;
-  io.u = u_buf;
-  io.v = v_buf;
   io.tma_extra_tx = g_tma_extra_tx;
   {
     /* pair stores: an even row length and 8-byte aligned outputs */
     auto al8 = [](const void *q) { return ((uintptr_t)q & 7u) == 0; };
-    const void *outs[] = {A.z, A.d, A.fl, A.fr, A.ft, A.fb, B.z, B.d, B.fl, B.fr, B.ft, B.fb, s1, u_buf, v_buf,
-                          vel_u, vel_v};
+    const void *outs[] = {A.z,      A.d,      A.fl,     A.fr,     A.ft,      A.fb,      B.z,   B.d,   B.fl, B.fr,
+                          B.ft,     B.fb,     s1_buf[0], s1_buf[1], u_buf[0], u_buf[1], v_buf[0], v_buf[1], vel_u,
+                          vel_v};
     bool        ok = nx % 2 == 0;
     for (const void *q : outs) ok = ok && al8(q);
     io.vec = ok ? 1 : 0;
@@ -367,25 +387,40 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
   const dim3 g2((nx + 255) / 256, row_groups < 65535 ? row_groups : 65535);
   VpFields  *cur = &A, *nxt = &B;
   int        parity = 0;
+  int        buf = 0; /* copy of u, v, s1 the current step writes */
   for (int it = 0; it < p.iterations; it++)
   {
     const bool last = it == p.iterations - 1;
     io.in = VpState{cur->z, cur->d, cur->s, cur->fl, cur->fr, cur->ft, cur->fb};
     io.out = VpStateOut{nxt->z, nxt->d, nxt->s, nxt->fl, nxt->fr, nxt->ft, nxt->fb, nullptr, nullptr};
+    io.s1 = s1_buf[buf];
+    io.u = u_buf[buf];
+    io.v = v_buf[buf];
+    io.s1_prev = s1_buf[buf ^ 1];
     io.u_out = last ? vel_u : nullptr;
     io.v_out = last ? vel_v : nullptr;
-    if (io.u_out && !io.v_out) io.v_out = v_buf;
-    if (io.v_out && !io.u_out) io.u_out = u_buf;
+    if (io.u_out && !io.v_out) io.v_out = io.v;
+    if (io.v_out && !io.u_out) io.u_out = io.u;
     io.parity = parity;
-    const int rc = tma ? launch_fwe_tma(io, maps[cur == &A ? 0 : 1], c, sc, partials, g1, s)
-                       : launch_fwe_cp_async(io, c, sc, partials, g1, s);
+    const FweMaps &mp = maps[cur == &A ? 0 : 1];
+    int            rc;
+    if (it > 0)
+      rc = step_tma ? launch_step_tma(io, mp, am[buf ^ 1], c, sc, partials, g1, s)
+                    : launch_step_cp_async(io, u_buf[buf ^ 1], v_buf[buf ^ 1], c, sc, partials, g1, s);
+    else rc = tma ? launch_fwe_tma(io, mp, c, sc, partials, g1, s) : launch_fwe_cp_async(io, c, sc, partials, g1, s);
     if (rc) return rc;
-    k_vp_advect<ADV_R><<<g2, 256, 0, s>>>(s1, u_buf, v_buf, nxt->s, c);
-    HM_LAUNCH_CHECK("k_vp_advect");
+    /* the advection of this step is folded into the next step's tiles; the
+     * last step's runs here */
+    if (last)
+    {
+      k_vp_advect<ADV_R><<<g2, 256, 0, s>>>(io.s1, io.u, io.v, nxt->s, c);
+      HM_LAUNCH_CHECK("k_vp_advect");
+    }
     VpFields *t = cur;
     cur = nxt;
     nxt = t;
     parity ^= 1;
+    buf ^= 1;
   }
   if (cur->z != z) HM_CUDA_TRY(cudaMemcpyAsync(z, cur->z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
   if (water_depth)
@@ -405,7 +440,7 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
 const unsigned *vpipes_error_word(const void *scratch_buf, int nx, int ny)
 {
   const size_t na = align_up((size_t)nx * ny, 64);
-  const char  *partials = (const char *)scratch_buf + 16 * na * sizeof(float);
+  const char  *partials = (const char *)scratch_buf + VP_GRIDS * na * sizeof(float);
   return &((const VpScalars *)(partials + partials_bytes(nx, ny)))->error;
 }
 
@@ -439,8 +474,11 @@ int vpipes_core(float *z,
   B.fr = base + 10 * na;
   B.ft = base + 11 * na;
   B.fb = base + 12 * na;
-  float     *u_buf = base + 13 * na, *v_buf = base + 14 * na, *s1_buf = base + 15 * na;
-  double    *partials = (double *)(base + 16 * na);
+  float *const u2[2] = {base + 13 * na, base + 16 * na};
+  float *const v2[2] = {base + 14 * na, base + 17 * na};
+  float *const s12[2] = {base + 15 * na, base + 18 * na};
+  float       *u_buf = u2[0], *v_buf = v2[0];
+  double      *partials = (double *)(base + VP_GRIDS * na);
   VpScalars *sc = (VpScalars *)((char *)partials + partials_bytes(nx, ny));
   VpDefer    df;
   df.list = (Deferred *)((char *)sc + align_up(sizeof(VpScalars), 256));
@@ -458,8 +496,8 @@ int vpipes_core(float *z,
   const FusedCfg cfg = vpipes_pick_config(nx, ny);
   const int      algo = vpipes_pick_algo(nx, ny);
   if (algo == 0 || algo == 2)
-    return vpipes_tiled_steps(z, nx, ny, p, c, A, B, u_buf, v_buf, s1_buf, rain, water_depth, sediment, vel_u, vel_v,
-                              sc, partials, algo == 0, s);
+    return vpipes_tiled_steps(z, nx, ny, p, c, A, B, u2, v2, s12, rain, water_depth, sediment, vel_u, vel_v, sc,
+                              partials, algo == 0, s);
   VpStep         st;
   st.rain = rain;
   st.H = cfg.h;

@@ -116,8 +116,10 @@ __device__ __forceinline__ void flow_cell(const VpConst &c,
     nb = fadd(fmul(c1, nb), f_diff);
   }
   T sum = fadd(fadd(fadd(nl, nr), nt), nb);
-  /* k = sum > 1e-5 ? d1 * l * l / (sum * dt) : 0, clamped to [0, 1] */
-  T kq = fdiv(fmul(fmul(d1c, bc<T>(c.pl)), bc<T>(c.pl)), fmul(sum, bc<T>(c.dt)));
+  /* k = sum > 1e-5 ? d1 * l * l / (sum * dt) : 0, clamped to [0, 1]; with
+   * l = 1 the two products are d1 itself (x * 1 is exact for every x) */
+  const T num = PL_ONE ? d1c : fmul(fmul(d1c, bc<T>(c.pl)), bc<T>(c.pl));
+  T       kq = fdiv(num, fmul(sum, bc<T>(c.dt)));
   T k = sel_gt(sum, bc<T>(1e-5f), kq, zero);
   k = rmin(rmax(k, zero), bc<T>(1.f));
   fl = fmul(nl, k);

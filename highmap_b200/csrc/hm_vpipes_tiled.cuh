@@ -14,11 +14,22 @@
  *   k_vp_advect  advection (:186-211): s = bilinear(s1, x - dt u), a gather
  *                from s1 in global memory, so the footprint may lie
  *                anywhere.
+ *   k_vp_step(_tma)  every step after the first: the previous step's
+ *                advection and this step's flow, water and erosion in one
+ *                tile.  Besides z, d and the fluxes it stages the previous
+ *                step's u and v (1-cell halo) and s1 (a 4-cell halo); each
+ *                cell of the tile and its ring gathers its advected sediment
+ *                from the staged s1, or from s1 in global memory where the
+ *                back-traced sample falls outside the staged box (s1 of the
+ *                previous step is complete in memory, so that read is exact
+ *                and needs no replay).  One kernel per step; the last step's
+ *                advection runs as k_vp_advect after the loop.
  *
  * HBM traffic per cell and step: 7 fields read and 9 written by k_vp_fwe,
- * 3 read (plus the gather, mostly L2) and 1 written by k_vp_advect: 80 B.
- * Every read of the step comes from the old state copy or from this
- * step's s1 / u / v, never from a grid this step writes, so tiles need no
+ * 3 read (plus the gather, mostly L2) and 1 written by k_vp_advect: 80 B;
+ * k_vp_step reads and writes 9 fields: 72 B.  Every read of a step comes
+ * from the old state copy or from the previous step's s1 / u / v
+ * (double-buffered), never from a grid the step writes, so tiles need no
  * ordering between them.
  */
 #ifndef HM_VPIPES_TILED_CUH
@@ -68,15 +79,35 @@ constexpr int fwe_min_blocks(int flags) { return (flags & FWE_FLOWONLY) ? 6 : 5;
  * 128-byte aligned. */
 constexpr int FW = 40;
 
+/* rows of the staged s1 box of k_vp_step(_tma): y0-4 .. y0+19 (region 1
+ * and a reach of 2.5 cells for the bilinear taps of its cells) */
+constexpr int FS_H = FT_TY + 8;
+
+/* k_vp_step(_tma)'s staging of the previous step's velocity (region 1, in
+ * rows padded to 20) and eroded sediment (rows y0-4 .. y0+19); dead once
+ * the advected sediment is in FweSmem::s, so it shares memory with the new
+ * fluxes of the flow pass */
+struct AdvStage
+{
+  alignas(128) float u[FT_H2][FW];
+  alignas(128) float v[FT_H2][FW];
+  alignas(128) float s1[FS_H][FW];
+};
+
 struct FweSmem
 {
   alignas(128) float z[FT_H2][FW];
   alignas(128) float d[FT_H2][FW];
   alignas(128) float s[FT_H2][FW];
   alignas(128) float fo[4][FT_H2][FW];
-  alignas(16) float fn[4][FT_H1][FW];
+  union alignas(128)
+  {
+    float    fn[4][FT_H1][FW];
+    AdvStage adv;
+  };
   uint64_t bar;
 };
+static_assert(sizeof(AdvStage) <= sizeof(float) * 4 * FT_H1 * FW, "advect-in staging fits the new-flux arrays");
 
 /* the step's grids: old state in, new state out, plus this step's s1, u, v */
 struct FweIo
@@ -92,6 +123,7 @@ struct FweIo
   int          flow_only;     /* flow_simulation step (FWE_FLOWONLY kernels) */
   unsigned     tma_extra_tx;  /* bytes a TMA tile's barrier expects beyond its boxes: 0, or the
                                * test hook's count, which makes every tile's wait run out */
+  const float *s1_prev;       /* k_vp_step(_tma): the previous step's eroded sediment */
 };
 
 /* tensor maps of the seven input fields of one step (TMA staging):
@@ -101,8 +133,17 @@ struct FweMaps
   CUtensorMap z, d, s, fl, fr, ft, fb;
 };
 
+/* tensor maps of the previous step's velocity and eroded sediment
+ * (k_vp_step_tma): u and v with a 40 x 18 box, s1 with a 40 x 24 box */
+struct AdvMaps
+{
+  CUtensorMap u, v, s1;
+};
+
 /* bytes the seven TMA boxes deliver */
 constexpr unsigned FWE_TMA_BYTES = 4u * 40u * (2u * FT_H2 + 5u * FT_H1);
+/* bytes the nine boxes of k_vp_step_tma deliver */
+constexpr unsigned STEP_TMA_BYTES = 4u * 40u * (2u * FT_H2 + 6u * FT_H1 + FS_H);
 
 /* cp.async staging: z, d on the halo-2 region; s and old fluxes on the
  * halo-1 region; loads clamped to the grid, so every raw neighbour read is
@@ -129,6 +170,85 @@ __device__ __forceinline__ void fwe_stage_cp_async(const FweIo &io, int nx, int 
   }
   cp_async_commit();
   cp_async_wait<0>();
+}
+
+/* cp.async staging of a folded step (k_vp_step): z, d (region 2) and the
+ * old fluxes (region 1) clamped to the grid as fwe_stage_cp_async stages
+ * them, the previous step's u and v on region 1 and s1 on columns x0-4 ..
+ * x0+35, rows y0-4 .. y0+19, the last three at in-grid cells only (they
+ * are read nowhere else).  io.u, io.v are this step's outputs; the
+ * previous step's velocity comes in as u_prev, v_prev. */
+__device__ __forceinline__ void fwe_stage_cp_async_step(const FweIo &io, const float *u_prev, const float *v_prev,
+                                                        int nx, int ny, int x0, int y0, FweSmem &sm)
+{
+  const int tid = threadIdx.x;
+  for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
+  {
+    const int    ly = e / FT_W2, lx = e - ly * FT_W2;
+    const size_t k = (size_t)clampi(y0 - 2 + ly, 0, ny - 1) * nx + clampi(x0 - 2 + lx, 0, nx - 1);
+    cp_async4(&sm.z[ly][lx + 2], io.in.z + k);
+    cp_async4(&sm.d[ly][lx + 2], io.in.d + k);
+  }
+  for (int e = tid; e < FT_W1 * FT_H1; e += FT_NT)
+  {
+    const int    ly = e / FT_W1, lx = e - ly * FT_W1;
+    const int    gx = x0 - 1 + lx, gy = y0 - 1 + ly;
+    const size_t k = (size_t)clampi(gy, 0, ny - 1) * nx + clampi(gx, 0, nx - 1);
+    cp_async4(&sm.fo[0][ly][lx + 3], io.in.fl + k);
+    cp_async4(&sm.fo[1][ly][lx + 3], io.in.fr + k);
+    cp_async4(&sm.fo[2][ly][lx + 3], io.in.ft + k);
+    cp_async4(&sm.fo[3][ly][lx + 3], io.in.fb + k);
+    if (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
+    {
+      cp_async4(&sm.adv.u[ly][lx + 3], u_prev + k);
+      cp_async4(&sm.adv.v[ly][lx + 3], v_prev + k);
+    }
+  }
+  for (int e = tid; e < FW * FS_H; e += FT_NT)
+  {
+    const int ly = e / FW, lx = e - ly * FW;
+    const int gx = x0 - 4 + lx, gy = y0 - 4 + ly;
+    if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) cp_async4(&sm.adv.s1[ly][lx], io.s1_prev + (size_t)gy * nx + gx);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+}
+
+/* Clamp-to-edge rebuild of the staged fields on a tile that touches the
+ * grid's edge (TMA boxes read zeros outside the grid): z and d on region 2,
+ * the old fluxes and, WITH_S, the sediment on region 1.  The clamped cell
+ * is always inside the box; the edge test depends only on the tile, so the
+ * barrier inside it is uniform. */
+template <bool WITH_S>
+__device__ __forceinline__ void fwe_fix_edges(int nx, int ny, int x0, int y0, FweSmem &sm)
+{
+  const int tid = threadIdx.x;
+  if (x0 - 2 < 0 || x0 + FT_TX + 2 > nx || y0 - 2 < 0 || y0 + FT_TY + 2 > ny)
+  {
+    /* region 2: columns x0-2 .. x0+33 at smem 2 .. 37, rows y0-2 .. y0+17 */
+    for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
+    {
+      const int ly = e / FT_W2, lx = e - ly * FT_W2;
+      const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
+      if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) continue;
+      const int cy = clampi(gy, 0, ny - 1) - (y0 - 2), cx = clampi(gx, 0, nx - 1) - (x0 - 4);
+      sm.z[ly][lx + 2] = sm.z[cy][cx];
+      sm.d[ly][lx + 2] = sm.d[cy][cx];
+    }
+    /* region 1: columns x0-1 .. x0+32 at smem 3 .. 36, rows y0-1 .. y0+16 */
+    for (int e = tid; e < FT_W1 * FT_H1; e += FT_NT)
+    {
+      const int ly = e / FT_W1, lx = e - ly * FT_W1;
+      const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
+      if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) continue;
+      const int cy = clampi(gy, 0, ny - 1) - (y0 - 1), cx = clampi(gx, 0, nx - 1) - (x0 - 4);
+      if (WITH_S) sm.s[ly][lx + 3] = sm.s[cy][cx];
+#pragma unroll
+      for (int f = 0; f < 4; f++) sm.fo[f][ly][lx + 3] = sm.fo[f][cy][cx];
+    }
+    /* the copies read in-grid cells that the depth pass rewrites in place */
+    __syncthreads();
+  }
 }
 
 /* TMA staging: thread 0 arms the barrier and issues the seven box loads;
@@ -162,33 +282,93 @@ __device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int n
   bool ok = mbar_wait_bounded(&sm.bar, 0);
   if (!ok) ok = mbar_wait_bounded(&sm.bar, 0); /* loads still in flight: give them a second window */
   if (!__syncthreads_and(ok)) return false;
-  if (x0 - 2 < 0 || x0 + FT_TX + 2 > nx || y0 - 2 < 0 || y0 + FT_TY + 2 > ny)
-  {
-    /* region 2: columns x0-2 .. x0+33 at smem 2 .. 37, rows y0-2 .. y0+17 */
-    for (int e = tid; e < FT_W2 * FT_H2; e += FT_NT)
-    {
-      const int ly = e / FT_W2, lx = e - ly * FT_W2;
-      const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
-      if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) continue;
-      const int cy = clampi(gy, 0, ny - 1) - (y0 - 2), cx = clampi(gx, 0, nx - 1) - (x0 - 4);
-      sm.z[ly][lx + 2] = sm.z[cy][cx];
-      sm.d[ly][lx + 2] = sm.d[cy][cx];
-    }
-    /* region 1: columns x0-1 .. x0+32 at smem 3 .. 36, rows y0-1 .. y0+16 */
-    for (int e = tid; e < FT_W1 * FT_H1; e += FT_NT)
-    {
-      const int ly = e / FT_W1, lx = e - ly * FT_W1;
-      const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-      if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) continue;
-      const int cy = clampi(gy, 0, ny - 1) - (y0 - 1), cx = clampi(gx, 0, nx - 1) - (x0 - 4);
-      sm.s[ly][lx + 3] = sm.s[cy][cx];
-#pragma unroll
-      for (int f = 0; f < 4; f++) sm.fo[f][ly][lx + 3] = sm.fo[f][cy][cx];
-    }
-    /* the copies read in-grid cells that the depth pass rewrites in place */
-    __syncthreads();
-  }
+  fwe_fix_edges<true>(nx, ny, x0, y0, sm);
   return true;
+}
+
+/* TMA staging of k_vp_step_tma: z and d (region 2), the old fluxes
+ * (region 1), the previous step's u and v (region 1) and s1 (rows y0-4 ..
+ * y0+19), then the clamp-to-edge rebuild of z, d and the fluxes on edge
+ * tiles.  The sediment needs none: it is advected at clamped cells, and u,
+ * v and s1 are only read at in-grid cells.  Returns false, uniformly across
+ * the CTA, if the loads did not complete in time. */
+__device__ __forceinline__ bool fwe_stage_tma_step(const FweMaps &maps, const AdvMaps &am, int nx, int ny, int x0,
+                                                   int y0, FweSmem &sm, unsigned extra_tx)
+{
+  const int tid = threadIdx.x;
+  if (tid == 0)
+  {
+    mbar_init(&sm.bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0)
+  {
+    mbar_arrive_expect_tx(&sm.bar, STEP_TMA_BYTES + extra_tx);
+    tma_load_2d(&sm.z[0][0], &maps.z, x0 - 4, y0 - 2, &sm.bar);
+    tma_load_2d(&sm.d[0][0], &maps.d, x0 - 4, y0 - 2, &sm.bar);
+    tma_load_2d(&sm.fo[0][0][0], &maps.fl, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.fo[1][0][0], &maps.fr, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.fo[2][0][0], &maps.ft, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.fo[3][0][0], &maps.fb, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.adv.u[0][0], &am.u, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.adv.v[0][0], &am.v, x0 - 4, y0 - 1, &sm.bar);
+    tma_load_2d(&sm.adv.s1[0][0], &am.s1, x0 - 4, y0 - 4, &sm.bar);
+  }
+  bool ok = mbar_wait_bounded(&sm.bar, 0);
+  if (!ok) ok = mbar_wait_bounded(&sm.bar, 0); /* loads still in flight: give them a second window */
+  if (!__syncthreads_and(ok)) return false;
+  fwe_fix_edges<false>(nx, ny, x0, y0, sm);
+  return true;
+}
+
+/* Advected sediment of the tile and its ring (region 1) into sm.s:
+ * s(i, j) = bilinear(s1, (i - dt u, j - dt v)) with the previous step's u,
+ * v and s1, exactly as k_vp_advect evaluates it.  A ring cell outside the
+ * grid takes the value of its clamp-to-edge cell (the reference's
+ * clamped read of s there), so it is computed at that cell.  Taps inside
+ * the staged s1 box (columns x0-4 .. x0+35, rows y0-4 .. y0+19) read shared
+ * memory, the rest s1 in global memory.  INNER: region 1 lies inside the
+ * grid, so no cell is clamped. */
+template <bool INNER>
+__device__ __forceinline__ void advect_region1(const VpConst &c, const float *__restrict__ s1g, int x0, int y0,
+                                               FweSmem &sm)
+{
+  const int nx = c.nx, ny = c.ny;
+  for (int e = threadIdx.x; e < FT_W1 * FT_H1; e += FT_NT)
+  {
+    const int l = e / FT_W1, cc = 3 + (e - l * FT_W1);
+    int       gx = x0 - 4 + cc, gy = y0 - 1 + l;
+    if (!INNER)
+    {
+      gx = clampi(gx, 0, nx - 1);
+      gy = clampi(gy, 0, ny - 1);
+    }
+    const float uu = sm.adv.u[gy - (y0 - 1)][gx - (x0 - 4)];
+    const float vv = sm.adv.v[gy - (y0 - 1)][gx - (x0 - 4)];
+    const float x = fsub((float)gx, fmul(c.dt, uu));
+    const float y = fsub((float)gy, fmul(c.dt, vv));
+    const Tap   t = linear_tap(x, y, nx, ny);
+    const int   bi0 = t.i0 - (x0 - 4), bi1 = t.i1 - (x0 - 4);
+    const int   bj0 = t.j0 - (y0 - 4), bj1 = t.j1 - (y0 - 4);
+    float       g00, g10, g01, g11;
+    if (bi0 >= 0 && bi1 < FW && bj0 >= 0 && bj1 < FS_H)
+    {
+      g00 = sm.adv.s1[bj0][bi0];
+      g10 = sm.adv.s1[bj0][bi1];
+      g01 = sm.adv.s1[bj1][bi0];
+      g11 = sm.adv.s1[bj1][bi1];
+    }
+    else
+    {
+      const size_t r0 = (size_t)t.j0 * nx, r1 = (size_t)t.j1 * nx;
+      g00 = __ldg(s1g + r0 + t.i0);
+      g10 = __ldg(s1g + r0 + t.i1);
+      g01 = __ldg(s1g + r1 + t.i0);
+      g11 = __ldg(s1g + r1 + t.i1);
+    }
+    sm.s[l][cc] = blend(t, g00, g10, g01, g11);
+  }
 }
 
 __device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
@@ -451,6 +631,67 @@ __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
     fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
 }
 
+/* A step after the first with cp.async staging (grids the TMA rules
+ * exclude): the previous step's advection and this step's flow, water and
+ * erosion in one tile; u_prev, v_prev and io.s1_prev hold the previous
+ * step's velocity and eroded sediment. */
+template <bool MAINTAIN, int F>
+__global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
+    k_vp_step(FweIo io, const float *__restrict__ u_prev, const float *__restrict__ v_prev, VpConst c,
+              VpScalars *sc, double *partials)
+{
+  __shared__ FweSmem sm;
+  const int x0 = blockIdx.x * FT_TX, y0 = blockIdx.y * FT_TY;
+  fwe_stage_cp_async_step(io, u_prev, v_prev, c.nx, c.ny, x0, y0, sm);
+  __syncthreads();
+  /* the advected sediment is written here and read after fwe_compute's
+   * first barrier */
+  if (fwe_inner_tile(io, c.nx, c.ny, x0, y0))
+  {
+    advect_region1<true>(c, io.s1_prev, x0, y0, sm);
+    fwe_compute<MAINTAIN, F, true>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  }
+  else
+  {
+    advect_region1<false>(c, io.s1_prev, x0, y0, sm);
+    fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  }
+}
+
+/* The same with the nine input boxes fetched by TMA (am holds the maps of
+ * the previous step's u, v and s1).  Timeouts as k_vp_fwe_tma. */
+template <bool MAINTAIN, int F>
+__global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
+    k_vp_step_tma(FweIo io, const __grid_constant__ FweMaps maps, const __grid_constant__ AdvMaps am, VpConst c,
+                  VpScalars *sc, double *partials)
+{
+  __shared__ FweSmem sm;
+  const int x0 = blockIdx.x * FT_TX, y0 = blockIdx.y * FT_TY;
+  if (!fwe_stage_tma_step(maps, am, c.nx, c.ny, x0, y0, sm, io.tma_extra_tx))
+  {
+    if (threadIdx.x == 0) atomicOr(&sc->error, 1u);
+    if (MAINTAIN)
+    {
+      const float v0 = sc->v0;
+      float      *outp = &sc->add[io.parity ^ 1];
+      grid_sum_commit<FT_NT>(0.0, partials, &sc->ticket, gridDim.x * gridDim.y,
+                             blockIdx.y * gridDim.x + blockIdx.x,
+                             [&](double total) { *outp = fsub(v0, (float)total); });
+    }
+    return;
+  }
+  if (fwe_inner_tile(io, c.nx, c.ny, x0, y0))
+  {
+    advect_region1<true>(c, io.s1_prev, x0, y0, sm);
+    fwe_compute<MAINTAIN, F, true>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  }
+  else
+  {
+    advect_region1<false>(c, io.s1_prev, x0, y0, sm);
+    fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+  }
+}
+
 /* Launch one k_vp_fwe (tma false) or k_vp_fwe_tma (maps != NULL) step on
  * stream s with the kernel specialised for the step's options
  * (hm_vpipes_fwe_cp_async.cu, hm_vpipes_fwe_tma.cu). */
@@ -458,11 +699,20 @@ int launch_fwe_cp_async(const FweIo &io, const VpConst &c, VpScalars *sc, double
                         cudaStream_t s);
 int launch_fwe_tma(const FweIo &io, const FweMaps &maps, const VpConst &c, VpScalars *sc, double *partials,
                    dim3 grid, cudaStream_t s);
+/* Launch one k_vp_step_tma step (hm_vpipes_step_tma.cu); io.s1_prev and am
+ * hold the previous step's s1, u and v. */
+int launch_step_tma(const FweIo &io, const FweMaps &maps, const AdvMaps &am, const VpConst &c, VpScalars *sc,
+                    double *partials, dim3 grid, cudaStream_t s);
+/* Launch one k_vp_step (cp.async staging, hm_vpipes_step_cp_async.cu). */
+int launch_step_cp_async(const FweIo &io, const float *u_prev, const float *v_prev, const VpConst &c, VpScalars *sc,
+                         double *partials, dim3 grid, cudaStream_t s);
 
 /* tensor maps of one state copy (hm_vpipes.cu); false if the grid or the
  * buffers do not meet the TMA rules (row pitch and bases 16-byte aligned,
  * boxes no larger than the grid) */
 bool fwe_maps(const VpFields &f, int nx, int ny, FweMaps *m);
+/* tensor maps of one copy of s1, u, v for k_vp_step_tma; false as above */
+bool adv_maps(const float *u, const float *v, const float *s1, int nx, int ny, AdvMaps *m);
 
 /* template flags of a step's options */
 inline int fwe_flags(const FweIo &io, const VpConst &c)
@@ -470,6 +720,27 @@ inline int fwe_flags(const FweIo &io, const VpConst &c)
   if (io.flow_only) return FWE_FLOWONLY | (io.diffusion ? FWE_DIFF : 0);
   if (!io.pl_one || !io.kexp_one) return FWE_GENERIC;
   return (io.diffusion ? FWE_DIFF : 0) | (io.rain ? FWE_RAINMAP : 0) | (c.rps != 0.f ? FWE_RAINSTEP : 0);
+}
+
+/* The same for the erosion steps only (no flow-only words). */
+template <template <bool, int> class K, class Launch>
+int step_dispatch(bool maintain, int f, Launch launch)
+{
+#define HM_STEP_CASE(FF)                                                                                               \
+  case FF: return maintain ? launch(K<true, FF>::fn()) : launch(K<false, FF>::fn());
+  switch (f)
+  {
+    HM_STEP_CASE(0)
+    HM_STEP_CASE(1)
+    HM_STEP_CASE(2)
+    HM_STEP_CASE(3)
+    HM_STEP_CASE(4)
+    HM_STEP_CASE(5)
+    HM_STEP_CASE(6)
+    HM_STEP_CASE(7)
+  default: return maintain ? launch(K<true, FWE_GENERIC>::fn()) : launch(K<false, FWE_GENERIC>::fn());
+  }
+#undef HM_STEP_CASE
 }
 
 /* Launch the kernel K<MAINTAIN, F> for run-time (maintain, f), f one of

@@ -203,3 +203,26 @@ def test_tiled_staging(gpu, shape, case):
     for a, b in zip(got[gpu.VPIPES_TILED], got[gpu.VPIPES_TILED_CP_ASYNC]):
         assert np.array_equal(a, b)
     _check(got[gpu.VPIPES_TILED], want, z0, exact=not pkw.get("maintain_water_volume", 1))
+
+
+@pytest.mark.parametrize("iterations", [1, 2, 3, 8])
+@pytest.mark.parametrize("case", ["config2", "fast_water"])
+def test_folded_advection_step_counts(gpu, iterations, case):
+    """Every step after the first advects the previous step's sediment
+    inside its own tile (its staged s1 box, or s1 in memory for samples
+    beyond it, which fast water forces), and the last step's advection runs
+    after the loop: every step count, the first step alone included, gives
+    the oracle's bits with TMA and with cp.async staging."""
+    z0 = fbm(132, 129, seed=21)
+    pkw = dict({"config2": CONFIG2, "fast_water": FAST}[case], iterations=iterations)
+    want = po.vpipes(z0, po.VpipesParams.make(**pkw))
+    got = {}
+    try:
+        for algo in (gpu.VPIPES_TILED, gpu.VPIPES_TILED_CP_ASYNC):
+            gpu.vpipes_set_algorithm(algo)
+            got[algo] = _run_gpu(gpu, z0, pkw)
+    finally:
+        gpu.vpipes_set_algorithm(gpu.VPIPES_AUTO)
+    for a, b in zip(got[gpu.VPIPES_TILED], got[gpu.VPIPES_TILED_CP_ASYNC]):
+        assert np.array_equal(a, b)
+    _check(got[gpu.VPIPES_TILED], want, z0, exact=True)
