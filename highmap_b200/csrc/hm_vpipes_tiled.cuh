@@ -66,7 +66,10 @@ constexpr int FWE_FLOWONLY = 16; /* flow and water passes only (flow_simulation)
  * code although a few words then spill.  The flow-only form
  * (flow_simulation) fits 40 registers, six CTAs per SM; a looser bound
  * lets the compiler take 46 and costs the sixth CTA (5 % slower). */
-constexpr int fwe_min_blocks(int flags) { return (flags & FWE_FLOWONLY) ? 6 : 5; }
+#ifndef HM_FWE_BLOCKS
+#define HM_FWE_BLOCKS 5
+#endif
+constexpr int fwe_min_blocks(int flags) { return (flags & FWE_FLOWONLY) ? 6 : HM_FWE_BLOCKS; }
 
 /* Shared-memory layout of the staged fields, one for both staging modes.
  * Every array row covers the 40 columns x0-4 .. x0+35 (a TMA box must start
@@ -377,14 +380,36 @@ __device__ __forceinline__ void   sts2(float *p, float a, float b) { *reinterpre
 /* Store the values of a cell pair (columns gx, gx + 1 of row offset k = the
  * pair's first cell): one 8-byte store when both cells are in the grid and
  * the grids allow it, else one or two 4-byte stores. */
+#ifndef HM_ST_HINT
+#define HM_ST_HINT 0
+#endif
+#ifndef HM_EARLY_STORES
+#define HM_EARLY_STORES 0
+#endif
+__device__ __forceinline__ void st1(float *p, float a)
+{
+#if HM_ST_HINT == 2
+  __stcs(p, a);
+#else
+  *p = a;
+#endif
+}
+__device__ __forceinline__ void st2(float *p, float a, float b)
+{
+#if HM_ST_HINT == 2
+  __stcs(reinterpret_cast<float2 *>(p), make_float2(a, b));
+#else
+  *reinterpret_cast<float2 *>(p) = make_float2(a, b);
+#endif
+}
 __device__ __forceinline__ void st_pair(float *p, size_t k, float a, float b, bool second, bool vec)
 {
   if (second && vec)
-    *reinterpret_cast<float2 *>(p + k) = make_float2(a, b);
+    st2(p + k, a, b);
   else
   {
-    p[k] = a;
-    if (second) p[k + 1] = b;
+    st1(p + k, a);
+    if (second) st1(p + k + 1, b);
   }
 }
 
@@ -539,6 +564,23 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
     }
     else
     {
+      const float dea = fmul(d2a, c.keep), deb = fmul(d2b, c.keep);
+#if HM_EARLY_STORES
+      /* what the water pass produced, stored before the erosion arithmetic
+       * so its registers are free there */
+      st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
+      st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
+      st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
+      st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
+      st_pair(io.out.d, k, dea, deb, second, vec);
+      st_pair(io.u, k, ua, ub, second, vec);
+      st_pair(io.v, k, va, vb, second, vec);
+      if (io.u_out)
+      {
+        st_pair(io.u_out, k, ua, ub, second, vec);
+        st_pair(io.v_out, k, va, vb, second, vec);
+      }
+#endif
       const float2 zc = lds2(&sm.z[q][cc]), zn = lds2(&sm.z[q - 1][cc]), zs = lds2(&sm.z[q + 1][cc]);
       const float  zw = sm.z[q][cc - 1], ze = sm.z[q][cc + 2];
       const float2 s0 = lds2(&sm.s[l][cc]), sn = lds2(&sm.s[l - 1][cc]), ss = lds2(&sm.s[l + 1][cc]);
@@ -554,15 +596,13 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
         erosion_cell<false>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
         erosion_cell<false>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
       }
-      const float  dea = fmul(d2a, c.keep), deb = fmul(d2b, c.keep);
+#if !HM_EARLY_STORES
       /* the cells' new fluxes, stored here where a warp writes whole rows */
       st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
       st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
       st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
       st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
-      st_pair(io.out.z, k, zoa, zob, second, vec);
       st_pair(io.out.d, k, dea, deb, second, vec);
-      st_pair(io.s1, k, soa, sob, second, vec);
       st_pair(io.u, k, ua, ub, second, vec);
       st_pair(io.v, k, va, vb, second, vec);
       if (io.u_out)
@@ -570,6 +610,9 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
         st_pair(io.u_out, k, ua, ub, second, vec);
         st_pair(io.v_out, k, va, vb, second, vec);
       }
+#endif
+      st_pair(io.out.z, k, zoa, zob, second, vec);
+      st_pair(io.s1, k, soa, sob, second, vec);
       part = (double)dea;
       if (second) part += (double)deb;
     }
