@@ -7,20 +7,24 @@
  * erosion nodes calls them one after another.  Small grids cannot fill a
  * B200 on their own, so here every admitted job's grid is cut into tiles
  * and the tiles of all jobs form packed lists:
- *   vpipes tiles  : 32 x 16 tiles of the flow / water / erosion step
- *                   (fwe_compute of hm_vpipes_tiled.cuh, cp.async staging),
- *                   then advection tiles of 256 columns x 16 rows;
- *   thermal tiles : 16 rows of 512 columns, a warp per 64 (column pairs,
- *                   for even rows on aligned grids) or of 256 columns, a
- *                   warp per 32 (hm_thermal_sweep.cuh).
- * A round advances every active job by one step: one persistent launch
- * whose CTAs (as many as fit on the device) take vpipes and thermal tiles
- * from an atomic counter, then one persistent launch over the advection
- * tiles.  Jobs are listed by remaining steps, longest first, so the active
- * tiles of every round are a prefix of each list.  A job's step s reads
- * state copy s & 1 and writes the other; per-job volume sums use the
- * deterministic last-tile finish of hm_reduce.cuh.  hm_batch_run captures
- * all rounds of a batch into one CUDA graph.
+ *   vpipes tiles  : 32 x 16 tiles of a step (hm_vpipes_tiled.cuh,
+ *                   cp.async staging): the first step's flow / water /
+ *                   erosion, and for every later step the previous step's
+ *                   advection folded into the same tile;
+ *   thermal tiles : th_rows rows of 512 columns, a warp per 64 (column
+ *                   pairs, for even rows on aligned grids) or of 256
+ *                   columns, a warp per 32 (hm_thermal_sweep.cuh).
+ * A round advances every active job by one step: ONE persistent launch
+ * whose CTAs take vpipes and thermal tiles from an atomic counter.  A
+ * vpipes job's last advection runs when the job finishes.  Jobs are
+ * listed by remaining steps, longest first, so the active tiles of every
+ * round are a prefix of each list.  A job's step s reads state copy s & 1
+ * and writes the other, and writes copy s & 1 of its s1, u, v while its
+ * tiles gather the previous step's from the other; per-job volume sums use
+ * the deterministic last-tile finish of hm_reduce.cuh.  hm_batch_run
+ * captures all rounds of a batch into one CUDA graph.  The persistent CTA
+ * count and the thermal tile's rows come from the autotuner
+ * (hm_autotune with HM_TUNE_BATCH) or a built-in choice.
  *
  * Results are bit-identical to solving each job alone (the same per-cell
  * code, the same Jacobi steps).
@@ -39,6 +43,7 @@
 #include "hm_thermal.h"
 #include "hm_thermal_math.cuh"
 #include "hm_thermal_sweep.cuh"
+#include "hm_tune.h"
 #include "hm_vpipes.h"
 #include "hm_vpipes_tiled.cuh"
 
@@ -47,17 +52,14 @@ namespace hm
 
 constexpr int BT = FT_NT;  /* threads per CTA (8 warps)                  */
 constexpr int TH_W = 256;  /* thermal tile: a warp per 32 columns        */
-constexpr int TH_H = 16;   /* rows of a thermal tile                     */
-constexpr int AD_W = 256;  /* advection tile: a thread per column        */
-constexpr int AD_H = 16;   /* rows of an advection tile                  */
 
 /* device-side description of one job */
 struct BJob
 {
   int       kind, nx, ny, iters;
   long long start; /* global round of the job's first step */
-  int       nbx, nby;   /* fwe or thermal tiles */
-  int       anx, any;   /* advection tiles (vpipes) */
+  int       nbx, nby;   /* vpipes step or thermal tiles */
+  int       th_rows;    /* rows of a thermal tile */
   /* thermal: tz[s & 1] holds step s */
   float       *tz[2];
   const float *talus;
@@ -65,10 +67,11 @@ struct BJob
   const float *bed;
   int          bed_mode;
   int          pairs; /* column-pair sweep (even nx, 8-byte aligned grids) */
-  /* vpipes: cp[s & 1] holds step s; s1, u, v carry a step's eroded
-   * sediment and velocity from the fwe tiles to the advection tiles */
+  /* vpipes: cp[s & 1] holds step s; step s writes s1[s & 1], u[s & 1],
+   * v[s & 1] (its eroded sediment and velocity), which step s + 1's tiles
+   * advect */
   VpFields     cp[2];
-  float       *s1, *u, *v;
+  float       *s1[2], *u[2], *v[2];
   VpConst      c;
   int          maintain, diffusion, pl_one, kexp_one;
   int          vec; /* pair stores (even nx, 8-byte aligned outputs) */
@@ -87,9 +90,10 @@ __device__ __forceinline__ void job_io(const BJob &J, int step, FweIo &io)
   const VpFields &in = J.cp[par], &out = J.cp[par ^ 1];
   io.in = VpState{in.z, in.d, in.s, in.fl, in.fr, in.ft, in.fb};
   io.out = VpStateOut{out.z, out.d, out.s, out.fl, out.fr, out.ft, out.fb, nullptr, nullptr};
-  io.s1 = J.s1;
-  io.u = J.u;
-  io.v = J.v;
+  io.s1 = J.s1[par];
+  io.u = J.u[par];
+  io.v = J.v[par];
+  io.s1_prev = J.s1[par ^ 1];
   io.rain = J.rain;
   io.parity = par;
   io.maintain = J.maintain;
@@ -99,8 +103,8 @@ __device__ __forceinline__ void job_io(const BJob &J, int step, FweIo &io)
   const bool last = step == J.iters - 1;
   io.u_out = last ? J.u_out : nullptr;
   io.v_out = last ? J.v_out : nullptr;
-  if (io.u_out && !io.v_out) io.v_out = J.v;
-  if (io.v_out && !io.u_out) io.u_out = J.u;
+  if (io.u_out && !io.v_out) io.v_out = io.v;
+  if (io.v_out && !io.u_out) io.u_out = io.u;
   io.vec = J.vec;
   io.flow_only = 0;
 }
@@ -108,7 +112,7 @@ __device__ __forceinline__ void job_io(const BJob &J, int step, FweIo &io)
 template <bool TMAP, int BED>
 __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int by)
 {
-  const int y0 = by * TH_H, y1 = min(J.ny, y0 + TH_H);
+  const int y0 = by * J.th_rows, y1 = min(J.ny, y0 + J.th_rows);
   if (J.pairs)
   {
     const int wx = bx * 2 * TH_W + (threadIdx.x >> 5) * 64;
@@ -121,8 +125,10 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
     thermal_sweep_warp<TMAP, TalusExchange<BED>>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
 }
 
-/* One round, first launch: every active vpipes fwe tile and thermal tile,
- * taken by persistent CTAs from an atomic counter. */
+/* One round: every active vpipes tile and thermal tile, taken by
+ * persistent CTAs from an atomic counter.  A vpipes tile of a job's first
+ * step stages the job's sediment; later steps advect the previous step's
+ * eroded sediment into the tile (fwe_stage_cp_async_step, advect_region1). */
 __global__ void __launch_bounds__(BT, 3)
     k_batch_round(const BJob *__restrict__ jobs,
                   const int4 *__restrict__ vt,
@@ -137,6 +143,7 @@ __global__ void __launch_bounds__(BT, 3)
   /* the current vpipes tile's step description, staged once per tile */
   __shared__ FweIo   s_io;
   __shared__ VpConst s_c;
+  __shared__ int     s_step;
   for (;;)
   {
     __syncthreads(); /* the previous tile is done with the shared state */
@@ -147,7 +154,8 @@ __global__ void __launch_bounds__(BT, 3)
       if (t < nv)
       {
         const BJob &J = jobs[vt[t].x];
-        job_io(J, (int)(round - J.start), s_io);
+        s_step = (int)(round - J.start);
+        job_io(J, s_step, s_io);
         s_c = J.c;
       }
     }
@@ -158,8 +166,14 @@ __global__ void __launch_bounds__(BT, 3)
     {
       const int4  tl = vt[t];
       const BJob &J = jobs[tl.x];
-      fwe_stage_cp_async(s_io, J.nx, J.ny, tl.y * FT_TX, tl.z * FT_TY, sm);
+      const int   x0 = tl.y * FT_TX, y0 = tl.z * FT_TY;
+      const int   step = s_step;
+      if (step == 0)
+        fwe_stage_cp_async(s_io, J.nx, J.ny, x0, y0, sm);
+      else
+        fwe_stage_cp_async_step(s_io, J.u[(step & 1) ^ 1], J.v[(step & 1) ^ 1], J.nx, J.ny, x0, y0, sm);
       __syncthreads();
+      if (step > 0) advect_region1<false>(s_c, s_io.s1_prev, x0, y0, sm);
       if (J.maintain)
         fwe_compute<true, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
       else
@@ -184,31 +198,6 @@ __global__ void __launch_bounds__(BT, 3)
         else thermal_tile<false, BED_LITERAL>(J, par, tl.y, tl.z);
       }
     }
-  }
-}
-
-/* One round, second launch: the advection tiles of the active vpipes jobs
- * (s of the new state from this step's s1, u, v). */
-__global__ void __launch_bounds__(BT, 4)
-    k_batch_advect(const BJob *__restrict__ jobs, const int4 *__restrict__ at, int na, long long round,
-                   unsigned *counter)
-{
-  __shared__ int s_tile;
-  for (;;)
-  {
-    __syncthreads();
-    if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
-    __syncthreads();
-    const int t = s_tile;
-    if (t >= na) return;
-    const int4  tl = at[t];
-    const BJob &J = jobs[tl.x];
-    const int   par = (int)((round - J.start) & 1);
-    const int   i = tl.y * AD_W + (int)threadIdx.x;
-    if (i >= J.nx) continue;
-    const int y1 = min(J.ny, (tl.z + 1) * AD_H);
-    for (int jb = tl.z * AD_H; jb < y1; jb += ADV_R)
-      advect_rows<ADV_R>(J.s1, J.u, J.v, J.cp[par ^ 1].s, J.c, i, jb);
   }
 }
 
@@ -239,7 +228,8 @@ size_t job_bytes(const hm_job &j)
   if (j.kind == HM_JOB_THERMAL) return n * (1 + (j.deposition_map ? 1 : 0));
   const size_t tiles = (size_t)((j.nx + hm::FT_TX - 1) / hm::FT_TX) * ((j.ny + hm::FT_TY - 1) / hm::FT_TY);
   const size_t parts = std::max(tiles, hm::vpipes_init_partials());
-  return n * 16 + align_up(parts * sizeof(double), 256) + align_up(sizeof(hm::VpScalars), 256);
+  /* state copies A (but z) and B, two copies of s1, u, v */
+  return n * 19 + align_up(parts * sizeof(double), 256) + align_up(sizeof(hm::VpScalars), 256);
 }
 
 int check_job(const hm_job &j)
@@ -275,7 +265,7 @@ struct hm_batch
   std::vector<HJob> jobs;
   long long         round = 0;
   int               grid_cap = 0; /* persistent CTAs of k_batch_round  */
-  int               grid_cap_adv = 0; /* persistent CTAs of k_batch_advect */
+  int               th_rows = 16; /* rows of a thermal tile            */
   /* device tables */
   hm::BJob         *d_jobs = nullptr;
   size_t            d_jobs_cap = 0;
@@ -341,6 +331,16 @@ int finalize_job(hm_batch *b, HJob &h)
   else
   {
     const hm::VpFields &f = h.dev.cp[par];
+    if (j.iterations > 0)
+    {
+      /* the last step's advection (every earlier one ran in the next step's
+       * tiles): s of the final state from that step's s1, u, v */
+      const int  lb = (j.iterations - 1) & 1;
+      const int  row_groups = (j.ny + hm::ADV_R - 1) / hm::ADV_R;
+      const dim3 g2((j.nx + 255) / 256, row_groups < 65535 ? row_groups : 65535);
+      hm::k_vp_advect<hm::ADV_R><<<g2, 256, 0, s>>>(h.dev.s1[lb], h.dev.u[lb], h.dev.v[lb], f.s, h.dev.c);
+      HM_LAUNCH_CHECK("k_vp_advect");
+    }
     if (f.z != j.z) HM_CUDA_TRY(cudaMemcpyAsync(j.z, f.z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
     if (j.water_depth)
     {
@@ -374,14 +374,14 @@ struct Plan
 };
 
 /* Packed tile lists of the active jobs (cached in the batch, rebuilt and
- * uploaded only when a job is admitted or finishes): vpipes fwe tiles,
- * thermal tiles, vpipes advection tiles, each in the order of act; cum*[m]
+ * uploaded only when a job is admitted or finishes): vpipes step tiles and
+ * thermal tiles, each in the order of act; cum*[m]
  * counts the tiles of the first m jobs, so the tiles of the jobs that still
  * have steps left at a round are a prefix of each list. */
 struct TileLists
 {
   std::vector<int>    act;
-  std::vector<size_t> vcum, tcum, acum;
+  std::vector<size_t> vcum, tcum;
 };
 
 int plan_rounds(hm_batch *b, int rounds, Plan &pl)
@@ -397,26 +397,20 @@ int plan_rounds(hm_batch *b, int rounds, Plan &pl)
     /* every active job advances by the same number of steps per round, so
      * this order holds until the set of jobs changes */
     std::stable_sort(tl.act.begin(), tl.act.end(), [&](int x, int y) { return remaining(x) > remaining(y); });
-    std::vector<int4> vt, tt, at;
+    std::vector<int4> vt, tt;
     tl.vcum.assign(1, 0);
     tl.tcum.assign(1, 0);
-    tl.acum.assign(1, 0);
     for (int k : tl.act)
     {
       const HJob &h = b->jobs[k];
       for (int by = 0; by < h.dev.nby; by++)
         for (int bx = 0; bx < h.dev.nbx; bx++)
           (h.desc.kind == HM_JOB_VPIPES ? vt : tt).push_back(make_int4(k, bx, by, 0));
-      if (h.desc.kind == HM_JOB_VPIPES)
-        for (int by = 0; by < h.dev.any; by++)
-          for (int bx = 0; bx < h.dev.anx; bx++) at.push_back(make_int4(k, bx, by, 0));
       tl.vcum.push_back(vt.size());
       tl.tcum.push_back(tt.size());
-      tl.acum.push_back(at.size());
     }
     std::vector<int4> all(vt);
     all.insert(all.end(), tt.begin(), tt.end());
-    all.insert(all.end(), at.begin(), at.end());
     if ((st = grow(&b->d_tiles, &b->d_tiles_cap, std::max<size_t>(all.size(), 1), b->stream))) return st;
     /* pageable source: the call returns once the data is staged */
     if (!all.empty())
@@ -434,7 +428,7 @@ int plan_rounds(hm_batch *b, int rounds, Plan &pl)
   pl.N = std::min(rounds, maxrem);
   if ((st = upload_jobs(b))) return st;
   if (pl.N == 0) return HM_OK;
-  if ((st = grow(&b->d_counters, &b->counters_cap, 2 * (size_t)pl.N, b->stream))) return st;
+  if ((st = grow(&b->d_counters, &b->counters_cap, (size_t)pl.N, b->stream))) return st;
   return HM_OK;
 }
 
@@ -442,27 +436,20 @@ int launch_rounds(hm_batch *b, const Plan &pl)
 {
   if (pl.N > 0)
   {
-    HM_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, 2 * (size_t)pl.N * sizeof(unsigned), b->stream));
+    HM_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, (size_t)pl.N * sizeof(unsigned), b->stream));
     const TileLists &tl = *b->lists;
-    const size_t     nv = tl.vcum.back(), nt = tl.tcum.back();
+    const size_t     nv = tl.vcum.back();
     size_t           m = pl.act.size();
     for (int r = 0; r < pl.N; r++)
     {
       /* the jobs (a prefix of act) that still have steps left at this round */
       while (m > 0 && pl.rem[m - 1] <= r) m--;
-      const size_t iv = tl.vcum[m], it = tl.tcum[m], ia = tl.acum[m];
+      const size_t iv = tl.vcum[m], it = tl.tcum[m];
       const int total = (int)(iv + it);
       const int grid = std::max(1, std::min(b->grid_cap, total));
       hm::k_batch_round<<<grid, hm::BT, 0, b->stream>>>(b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it,
-                                                        b->round + r, b->d_counters + 2 * r);
+                                                        b->round + r, b->d_counters + r);
       HM_LAUNCH_CHECK("k_batch_round");
-      if (ia > 0)
-      {
-        const int grid2 = std::max(1, std::min(b->grid_cap_adv, (int)ia));
-        hm::k_batch_advect<<<grid2, hm::BT, 0, b->stream>>>(b->d_jobs, b->d_tiles + nv + nt, (int)ia,
-                                                            b->round + r, b->d_counters + 2 * r + 1);
-        HM_LAUNCH_CHECK("k_batch_advect");
-      }
     }
   }
   for (int k : pl.act)
@@ -549,12 +536,18 @@ int hm_batch_create(hm_context *ctx, hm_batch **out)
     cuuint64_t keep = ~(cuuint64_t)0;
     HM_CUDA_TRY(cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   }
-  int per_sm = 0, per_sm_adv = 0, sms = 0;
+  int per_sm = 0, sms = 0;
   HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hm::k_batch_round, hm::BT, 0));
-  HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_adv, hm::k_batch_advect, hm::BT, 0));
   HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+  /* persistent CTAs per SM and thermal tile rows: the tuned choice, or all
+   * CTAs that fit and 16 rows */
+  hm::TuneEntry te;
+  if (hm::tuned_batch(&te))
+  {
+    if (te.tpb >= 1) per_sm = std::min(per_sm, te.tpb);
+    if (te.rows >= 1) b->th_rows = te.rows;
+  }
   b->grid_cap = std::max(1, per_sm) * std::max(1, sms);
-  b->grid_cap_adv = std::max(1, per_sm_adv) * std::max(1, sms);
   *out = b;
   return HM_OK;
 }
@@ -597,8 +590,9 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
     auto al8 = [](const void *p) { return ((uintptr_t)p & 7u) == 0; };
     d.pairs = job->nx % 2 == 0 && al8(d.tz[0]) && al8(d.tz[1]) && (!d.talus || al8(d.talus)) && (!d.bed || al8(d.bed));
     const int tw = d.pairs ? 2 * hm::TH_W : hm::TH_W;
+    d.th_rows = b->th_rows;
     d.nbx = (job->nx + tw - 1) / tw;
-    d.nby = (job->ny + hm::TH_H - 1) / hm::TH_H;
+    d.nby = (job->ny + d.th_rows - 1) / d.th_rows;
     if (job->deposition_map)
     {
       h.z0 = base + na;
@@ -612,8 +606,6 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
     p.iterations = job->iterations;
     d.nbx = (job->nx + hm::FT_TX - 1) / hm::FT_TX;
     d.nby = (job->ny + hm::FT_TY - 1) / hm::FT_TY;
-    d.anx = (job->nx + hm::AD_W - 1) / hm::AD_W;
-    d.any = (job->ny + hm::AD_H - 1) / hm::AD_H;
     hm::VpFields A{job->z, base + 0 * na, base + 1 * na, base + 2 * na, base + 3 * na, base + 4 * na, base + 5 * na};
     hm::VpFields B{base + 6 * na, base + 7 * na, base + 8 * na, base + 9 * na, base + 10 * na, base + 11 * na,
                    base + 12 * na};
@@ -627,12 +619,15 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
     d.rain = job->rain_map;
     d.u_out = job->vel_u;
     d.v_out = job->vel_v;
-    d.s1 = base + 13 * na;
-    d.u = base + 14 * na;
-    d.v = base + 15 * na;
+    d.s1[0] = base + 13 * na;
+    d.u[0] = base + 14 * na;
+    d.v[0] = base + 15 * na;
+    d.s1[1] = base + 16 * na;
+    d.u[1] = base + 17 * na;
+    d.v[1] = base + 18 * na;
     d.vec = job->nx % 2 == 0 && ((uintptr_t)job->z & 7u) == 0 && ((uintptr_t)job->vel_u & 7u) == 0 &&
             ((uintptr_t)job->vel_v & 7u) == 0;
-    d.partials = (double *)(base + 16 * na);
+    d.partials = (double *)(base + 19 * na);
     const size_t tiles = (size_t)d.nbx * d.nby;
     const size_t parts = std::max(tiles, hm::vpipes_init_partials());
     d.sc = (hm::VpScalars *)((char *)d.partials + align_up(parts * sizeof(double), 256));

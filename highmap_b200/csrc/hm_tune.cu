@@ -8,14 +8,20 @@
  *   vpipes  : threads per CTA (strip width) x staged advection radius x
  *             output rows per CTA (the occupancy / halo / warm-up trade);
  *   thermal : steps per launch (temporal-block depth 1, 2, 4, 8) x rows
- *             per CTA of the blocked kernel.
+ *             per CTA of the blocked kernel;
+ *   batch   : persistent CTAs per SM (occupancy) x rows of a thermal tile
+ *             of the batched form's round kernel, on a synthetic mixed
+ *             batch (one entry for the process).
  * The solvers consult the table whenever the caller leaves the choice to
  * the library (time_block 0, no hm_vpipes_set_launch override).  Results
  * never depend on the shape; only the speed does.
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstring>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -35,6 +41,8 @@ namespace
 
 std::mutex                                   g_mu;
 std::map<std::pair<int, int>, TuneEntry>     g_vp, g_th; /* size class -> shape */
+TuneEntry                                    g_batch;
+bool                                         g_batch_set = false;
 
 int pow2_class(int v)
 {
@@ -73,6 +81,14 @@ bool tuned_vpipes(int nx, int ny, TuneEntry *out)
   return true;
 }
 
+bool tuned_batch(TuneEntry *out)
+{
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_batch_set) return false;
+  *out = g_batch;
+  return true;
+}
+
 bool tuned_thermal(int nx, int ny, TuneEntry *out)
 {
   std::lock_guard<std::mutex> lk(g_mu);
@@ -84,13 +100,131 @@ bool tuned_thermal(int nx, int ny, TuneEntry *out)
 
 } // namespace hm
 
+namespace hm
+{
+namespace
+{
+
+/* Tunes the batched form: each candidate (CTAs per SM, thermal tile rows)
+ * runs 3 warm-up and `steps` timed rounds of the same synthetic batch. */
+int autotune_batch(hm_context *ctx, int side_max, int steps, hm_tune_result *result)
+{
+  cudaStream_t         s = ctx->stream;
+  const int            sides[8] = {128, 192, 256, 384, 512, 768, 1024, 1536};
+  std::vector<hm_job>  jobs;
+  std::vector<float *> bufs;
+  int                  st = HM_OK;
+  for (int k = 0; k < 16 && !st; k++)
+  {
+    const int side = std::min(sides[k % 8], std::max(side_max, 128));
+    hm_job    j;
+    memset(&j, 0, sizeof j);
+    j.kind = (k & 1) ? HM_JOB_VPIPES : HM_JOB_THERMAL;
+    j.nx = side;
+    j.ny = side - (k & 2 ? 64 : 0);
+    j.iterations = steps + 3;
+    float      *z = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&z, (size_t)j.nx * j.ny * sizeof(float), s);
+    if (e != cudaSuccess)
+    {
+      cudaGetLastError();
+      st = cuda_fail(e, "hm_autotune: batch job allocation");
+      break;
+    }
+    bufs.push_back(z);
+    j.z = z;
+    j.talus_value = 1.f / (float)j.nx;
+    hm_vpipes_default_params(&j.vpipes);
+    j.vpipes.maintain_water_volume = 0;
+    j.vpipes.flux_diffusion = 0;
+    j.vpipes.dt = 0.1f;
+    j.vpipes.gravity = 9.81f;
+    j.vpipes.rain_per_step = 1e-4f;
+    j.vpipes.initial_water = 0.f;
+    jobs.push_back(j);
+  }
+  std::vector<TuneEntry> cands;
+  for (int per_sm = 1; per_sm <= 3; per_sm++)
+    for (int rows : {8, 16, 32}) cands.push_back(TuneEntry{per_sm, 0, rows, 0, 0.f});
+  int   best = -1;
+  float best_ms = 0.f;
+  for (size_t c = 0; c < cands.size() && !st; c++)
+  {
+    {
+      std::lock_guard<std::mutex> lk(g_mu);
+      g_batch = cands[c];
+      g_batch_set = true;
+    }
+    for (size_t k = 0; k < jobs.size(); k++) k_synthetic_terrain<<<592, 256, 0, s>>>(bufs[k], jobs[k].nx, jobs[k].ny);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+    {
+      st = cuda_fail(e, "hm_autotune: synthetic terrain");
+      break;
+    }
+    hm_batch *b = nullptr;
+    if ((st = hm_batch_create(ctx, &b))) break;
+    for (size_t k = 0; k < jobs.size() && !st; k++)
+    {
+      int id;
+      st = hm_batch_add(b, &jobs[k], &id);
+    }
+    float ms = 0.f;
+    if (!st) st = hm_batch_step(b, 3);
+    if (!st) st = hm_batch_synchronize(b);
+    if (!st)
+    {
+      const auto t0 = std::chrono::steady_clock::now();
+      st = hm_batch_step(b, steps);
+      if (!st) st = hm_batch_synchronize(b);
+      ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    hm_batch_destroy(b);
+    cands[c].ms_per_step = ms / steps;
+    if (!st && (best < 0 || ms < best_ms))
+    {
+      best = (int)c;
+      best_ms = ms;
+    }
+  }
+  for (float *z : bufs) cudaFreeAsync(z, s);
+  cudaStreamSynchronize(s);
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (st || best < 0)
+  {
+    g_batch_set = false;
+    return st ? st : fail(HM_ERR_CUDA, "hm_autotune: no batch candidate ran");
+  }
+  g_batch = cands[best];
+  g_batch_set = true;
+  if (result)
+  {
+    memset(result, 0, sizeof *result);
+    result->tpb = g_batch.tpb;
+    result->rows = g_batch.rows;
+    result->ms_per_step = g_batch.ms_per_step;
+    result->candidates = (int)cands.size();
+  }
+  return HM_OK;
+}
+
+} // namespace
+} // namespace hm
+
 extern "C" {
 
 int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_result *result)
 {
   hm::clear_error();
-  if (!ctx || (kind != HM_JOB_THERMAL && kind != HM_JOB_VPIPES) || nx < 3 || ny < 3 || steps < 1)
+  if (!ctx || (kind != HM_JOB_THERMAL && kind != HM_JOB_VPIPES && kind != HM_TUNE_BATCH) || nx < 3 || ny < 3 ||
+      steps < 1)
     return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_autotune: bad argument");
+  if (kind == HM_TUNE_BATCH)
+  {
+    int st = hm::use_device(ctx->device);
+    if (st) return st;
+    return hm::autotune_batch(ctx, nx > ny ? nx : ny, steps, result);
+  }
   int st = hm::use_device(ctx->device);
   if (st) return st;
   cudaStream_t s = ctx->stream;
@@ -212,6 +346,8 @@ int hm_autotune_save(const char *path)
   for (auto &kv : hm::g_th)
     fprintf(f, "thermal %d %d %d %d %d %d %.6f\n", kv.first.first, kv.first.second, kv.second.tpb,
             kv.second.radius, kv.second.rows, kv.second.block, kv.second.ms_per_step);
+  if (hm::g_batch_set)
+    fprintf(f, "batch 0 0 %d 0 %d 0 %.6f\n", hm::g_batch.tpb, hm::g_batch.rows, hm::g_batch.ms_per_step);
   fclose(f);
   return HM_OK;
 }
@@ -247,6 +383,13 @@ int hm_autotune_load(const char *path, int *loaded_out)
       hm::g_th[{cx, cy}] = e;
       loaded++;
     }
+    else if (k == "batch" && e.tpb >= 1 && e.tpb <= 3 && (e.rows == 8 || e.rows == 16 || e.rows == 32))
+    {
+      std::lock_guard<std::mutex> lk(hm::g_mu);
+      hm::g_batch = e;
+      hm::g_batch_set = true;
+      loaded++;
+    }
   }
   hm_vpipes_set_launch(0, 0, 0);
   fclose(f);
@@ -259,6 +402,7 @@ void hm_autotune_clear(void)
   std::lock_guard<std::mutex> lk(hm::g_mu);
   hm::g_vp.clear();
   hm::g_th.clear();
+  hm::g_batch_set = false;
 }
 
 } // extern "C"

@@ -13,6 +13,9 @@ struct TuneEntry
 /* the tuned shape for this grid's size class, if any */
 bool tuned_vpipes(int nx, int ny, TuneEntry *out);
 bool tuned_thermal(int nx, int ny, TuneEntry *out);
+/* the batched form's tuned choice (tpb: persistent CTAs per SM, rows:
+ * thermal tile rows), if any */
+bool tuned_batch(TuneEntry *out);
 } // namespace hm
 
 #endif

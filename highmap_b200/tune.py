@@ -2,7 +2,9 @@
 
 ``autotune(kind, nx, ny)`` times every candidate launch shape of a solver on
 a synthetic terrain of that size and keeps the fastest for its size class;
-solves that leave the choice to the library then use it.  ``save`` /
+solves that leave the choice to the library then use it.  ``BATCH`` tunes
+the batched form (persistent CTAs per SM, thermal tile rows) on a synthetic
+mixed batch with sides up to max(nx, ny); batches created afterwards use it.  ``save`` /
 ``load`` keep the table between processes.
 """
 from __future__ import annotations
@@ -14,6 +16,7 @@ from .gpu import Context, default_context
 
 THERMAL = L.HM_JOB_THERMAL
 VPIPES = L.HM_JOB_VPIPES
+BATCH = 3  # HM_TUNE_BATCH: the batched form's CTAs per SM (tpb) and thermal tile rows (rows)
 
 
 def autotune(kind: int, nx: int, ny: int, steps: int = 20, ctx: Context | None = None) -> dict:

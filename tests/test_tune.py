@@ -15,13 +15,16 @@ def test_load_skips_invalid_lines(built_lib, tmp_path):
                  "vpipes 10 10 999 2 64 0 0.100\n"      # unsupported threads per CTA
                  "thermal 9 9 0 0 128 8 0.050\n"
                  "thermal 9 8 0 0 128 99 0.050\n"       # unsupported block depth
+                 "batch 0 0 2 0 16 0 0.300\n"
+                 "batch 0 0 7 0 16 0 0.300\n"           # unsupported CTAs per SM
                  "garbage line\n")
     tune.clear()
-    assert tune.load(str(p)) == 2
+    assert tune.load(str(p)) == 3
     out = tmp_path / "out.txt"
     tune.save(str(out))
     lines = [l for l in out.read_text().splitlines() if not l.startswith("#")]
-    assert sorted(l.split()[0] for l in lines) == ["thermal", "vpipes"]
+    assert sorted(l.split()[0] for l in lines) == ["batch", "thermal", "vpipes"]
+    assert "batch 0 0 2 0 16 0" in out.read_text()
     tune.clear()
 
 
@@ -51,4 +54,38 @@ def test_autotune_then_parity(gpu, tmp_path):
     tune.save(str(p))
     tune.clear()
     assert tune.load(str(p)) == 2
+    tune.clear()
+
+
+@pytest.mark.gpu
+def test_autotune_batch_then_bit_identical(gpu):
+    """The batched form's tuner picks a valid occupancy and thermal tile
+    height; a batch run with that choice still equals solo solves."""
+    import torch
+
+    from highmap_b200 import batch as B
+    from highmap_b200 import tune
+    tune.clear()
+    r = tune.autotune(tune.BATCH, 512, 512, steps=4)
+    assert r["tpb"] in (1, 2, 3) and r["rows"] in (8, 16, 32) and r["ms_per_step"] > 0
+    assert r["candidates"] == 9
+    specs = [("thermal", 200, 136, 23), ("vpipes", 264, 136, 17), ("vpipes", 96, 40, 9), ("thermal", 72, 520, 31)]
+    zs, jobs, solo = [], [], []
+    cfg = dict(maintain_water_volume=0, flux_diffusion=0, dt=0.1, gravity=9.81, rain_per_step=1e-4,
+               initial_water=0.0)
+    for k, (kind, nx, ny, it) in enumerate(specs):
+        z0 = torch.from_numpy(fbm(nx, ny, seed=30 + k)).cuda()
+        z = z0.clone()
+        zs.append(z)
+        jobs.append(B.thermal_job(z, 1.0 / nx, it) if kind == "thermal" else B.vpipes_job(z, it, **cfg))
+        w = z0.clone()
+        if kind == "thermal":
+            gpu.thermal_device(w, 1.0 / nx, it)
+        else:
+            gpu.hydraulic_vpipes_device(w, gpu.vpipes_params(**dict(cfg, iterations=it)))
+        solo.append(w)
+    B.run(jobs, use_graph=True)
+    torch.cuda.synchronize()
+    for z, w in zip(zs, solo):
+        assert torch.equal(z, w)
     tune.clear()
