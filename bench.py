@@ -68,6 +68,8 @@ def _args():
                          "extras: thermal_auto_bedrock, flow_simulation and the sibling talus stencils at 4096^2; "
                          "parity: thermal x500 and vpipes x1000 at 4096^2, GPU vs the reference's kernel text and "
                          "fp64 on the host cores")
+    ap.add_argument("--parity-part", choices=["all", "gpu", "host"], default="all",
+                    help="parity form: both sides, or only the GPU or host side (sha256 digests link the two)")
     ap.add_argument("--sizes", default="1024,2048,4096,8192,16384", help="grid sides of the sweep form")
     ap.add_argument("--jobs", type=int, default=256, help="jobs of the batch form")
     ap.add_argument("--requests", type=int, default=10000, help="requests per rate of the serve form")
@@ -625,101 +627,124 @@ def _material(z, s=None):
     return t + (float(s.astype(np.float64).sum()) if s is not None else 0.0)
 
 
+def _digest(x):
+    import hashlib
+
+    import numpy as np
+    return hashlib.sha256(np.ascontiguousarray(x).tobytes()).hexdigest()
+
+
 def run_parity(a):
     """The plain drop-in configuration at full length on the full grid,
     GPU against the reference's kernel text on the host cores and against
     an fp64 run of the same scheme: thermal (talus map, bedrock 0.3 z,
     500 iterations) and vpipes (1000 iterations) at 4096^2.
 
-    Thermal runs twice on the GPU: in the bedrock mode the benchmark
-    measures (update, then clamp to the bedrock), compared with the fp32
-    and fp64 oracle (the reference text has only the literal mode), and in
-    the reference's literal mode, compared with the reference text itself.
-    Vpipes is compared with the reference text (fp32) and the fp64 oracle.
-    Each comparison reports max and mean |difference| as a fraction of the
+    Thermal runs twice: in the bedrock mode the benchmark measures (update,
+    then clamp to the bedrock), compared with the fp32 and fp64 oracle (the
+    reference text has only the literal mode), and in the reference's
+    literal mode, compared with the reference text itself.  Vpipes is
+    compared with the reference text (fp32) and the fp64 oracle.  Each
+    comparison reports max and mean |difference| as a fraction of the
     input's height range, the relative L1 distance of HighMap's array
-    comparison, bit-exactness, and mass drift: |sum z_T - sum z_0| /
+    comparison and bit-exactness; mass drift is |sum z_T - sum z_0| /
     sum |z_0| for thermal, the same over terrain plus suspended sediment
-    for vpipes (rain and evaporation change the water itself)."""
-    import numpy as np
-    import torch
+    for vpipes (rain and evaporation change the water itself).
 
-    from highmap_b200 import gpu as G
+    --parity-part gpu runs only the GPU solves and host runs only the
+    host-side ones (reference text, fp32 and fp64 oracle and every
+    statistic against fp64); each prints sha256 digests of its outputs.
+    Where a GPU digest equals the host digest of the same field the two
+    results are bit-identical, so every statistic of the host result holds
+    for the GPU's.  `all` (the default) runs both and compares directly."""
+    import numpy as np
+
     from oracle import pyoracle as po
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if not G.init_opencl():
-        raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
-    if not po.ref_available():
-        raise RuntimeError("the reference's kernel text (oracle/_ref/libhm_ref.so) is not built")
-    ctx = G.Context(local)
+    part = a.parity_part
     n = a.size
     z0, talus, bed = _inputs(n)
     base = _material(z0)
     den = float(np.abs(z0.astype(np.float64)).sum())
-    t0 = time.perf_counter()
-
-    # GPU: host buffers through the C-ABI, as a caller of the drop-in would
-    z_int = z0.copy()
-    G.thermal(z_int, talus, THERMAL_ITERS, bedrock=bed, ctx=ctx)
-    z_lit = z0.copy()
-    G.thermal(z_lit, talus, THERMAL_ITERS, bedrock=bed, bedrock_mode=G.BEDROCK_LITERAL, ctx=ctx)
-    z_vp = z0.copy()
-    s_vp = np.empty_like(z0)
-    w_vp = np.empty_like(z0)
-    G.hydraulic_vpipes(z_vp, iterations=VPIPES_ITERS, water_depth=w_vp, sediment=s_vp, ctx=ctx, **CONFIG2_VPIPES)
-    ctx.close()
-    t_gpu = time.perf_counter() - t0
-
-    # host: the reference's kernel text and the oracle, all cores
-    t1 = time.perf_counter()
-    o32_int, _ = po.thermal(z0, talus, THERMAL_ITERS, bedrock=bed)
-    o64_int, _ = po.thermal(z0, talus, THERMAL_ITERS, bedrock=bed, dtype=np.float64)
-    r_lit, _ = po.ref_thermal(z0, talus, THERMAL_ITERS, bedrock=bed)
-    pp = po.VpipesParams.make(**dict(CONFIG2_VPIPES, iterations=VPIPES_ITERS))
-    r_vp = po.ref_vpipes(z0, pp)
-    o64_vp = po.vpipes(z0, pp, dtype=np.float64)
-    t_cpu = time.perf_counter() - t1
 
     def drift(m):
         return abs(m - base) / den
 
-    th = {
-        "intended_bedrock": {
-            "gpu_vs_oracle_fp32": _errors(z_int, o32_int, z0),
-            "gpu_vs_fp64": _errors(z_int, o64_int, z0),
-            "oracle_fp32_vs_fp64": _errors(o32_int, o64_int, z0),
-            "mass_drift": {"gpu": drift(_material(z_int)), "oracle_fp32": drift(_material(o32_int)),
-                           "fp64": drift(_material(o64_int))}},
-        "literal_bedrock": {
-            "gpu_vs_reference_text": _errors(z_lit, r_lit, z0),
-            "mass_drift": {"gpu": drift(_material(z_lit)), "reference_text": drift(_material(r_lit))}},
-    }
-    rz, rw, rs = r_vp[0], r_vp[1], r_vp[2]
-    vp = {
-        "gpu_vs_reference_text": {"z": _errors(z_vp, rz, z0), "sediment": _errors(s_vp, rs, z0),
-                                  "water_depth": _errors(w_vp, rw, z0)},
-        "gpu_vs_fp64": {"z": _errors(z_vp, o64_vp[0], z0), "sediment": _errors(s_vp, o64_vp[2], z0)},
-        "reference_text_vs_fp64": {"z": _errors(rz, o64_vp[0], z0), "sediment": _errors(rs, o64_vp[2], z0)},
-        "material_drift": {"gpu": drift(_material(z_vp, s_vp)), "reference_text": drift(_material(rz, rs)),
-                           "fp64": drift(_material(o64_vp[0], o64_vp[2]))},
-        "water_depth_max": {"gpu": float(w_vp.max()), "reference_text": float(rw.max())},
-    }
-    tol = {"thermal": 1e-4, "vpipes": 1e-3}
-    ok = (th["intended_bedrock"]["gpu_vs_oracle_fp32"]["max_abs_of_range"] <= tol["thermal"] and
-          th["literal_bedrock"]["gpu_vs_reference_text"]["max_abs_of_range"] <= tol["thermal"] and
-          vp["gpu_vs_reference_text"]["z"]["max_abs_of_range"] <= tol["vpipes"])
     out = {"metric": "max/mean abs error (fraction of the height range) and mass drift after the full iteration "
                      "counts, GPU vs the reference's kernel text and vs fp64",
-           "value": vp["gpu_vs_reference_text"]["z"]["max_abs_of_range"], "unit": "fraction of height range",
-           "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic", "form": "parity",
-           "within_tolerance": ok, "tolerance_of_range": tol,
+           "unit": "fraction of height range", "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
+           "data": "synthetic", "form": "parity", "parity_part": part,
+           "tolerance_of_range": {"thermal": 1e-4, "vpipes": 1e-3},
            "config": dict(_config(n), workload="plain drop-ins at full length, %dx%d: thermal x%d, vpipes x%d"
                           % (n, n, THERMAL_ITERS, VPIPES_ITERS)),
-           "host": {"cores": po.num_threads(), "cpu_s": t_cpu, "gpu_path_s": t_gpu},
-           "thermal": th, "vpipes": vp}
+           "input_sha256": _digest(z0)}
+    gpu = host = None
+    if part in ("all", "gpu"):
+        import torch
+
+        from highmap_b200 import gpu as G
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if not G.init_opencl():
+            raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
+        ctx = G.Context(int(os.environ.get("LOCAL_RANK", "0")))
+        t0 = time.perf_counter()
+        # host buffers through the C-ABI, as a caller of the drop-in would
+        z_int = z0.copy()
+        G.thermal(z_int, talus, THERMAL_ITERS, bedrock=bed, ctx=ctx)
+        z_lit = z0.copy()
+        G.thermal(z_lit, talus, THERMAL_ITERS, bedrock=bed, bedrock_mode=G.BEDROCK_LITERAL, ctx=ctx)
+        z_vp = z0.copy()
+        s_vp = np.empty_like(z0)
+        w_vp = np.empty_like(z0)
+        G.hydraulic_vpipes(z_vp, iterations=VPIPES_ITERS, water_depth=w_vp, sediment=s_vp, ctx=ctx,
+                           **CONFIG2_VPIPES)
+        ctx.close()
+        gpu = {"thermal_intended": z_int, "thermal_literal": z_lit, "vpipes_z": z_vp, "vpipes_sediment": s_vp,
+               "vpipes_water": w_vp}
+        out["gpu"] = {"seconds": time.perf_counter() - t0,
+                      "sha256": {k: _digest(v) for k, v in gpu.items()},
+                      "mass_drift": {"thermal_intended": drift(_material(z_int)),
+                                     "thermal_literal": drift(_material(z_lit)),
+                                     "vpipes_material": drift(_material(z_vp, s_vp))}}
+    if part in ("all", "host"):
+        if not po.ref_available():
+            raise RuntimeError("the reference's kernel text (oracle/_ref/libhm_ref.so) is not built")
+        t1 = time.perf_counter()
+        o32_int, _ = po.thermal(z0, talus, THERMAL_ITERS, bedrock=bed)
+        o64_int, _ = po.thermal(z0, talus, THERMAL_ITERS, bedrock=bed, dtype=np.float64)
+        r_lit, _ = po.ref_thermal(z0, talus, THERMAL_ITERS, bedrock=bed)
+        o64_lit, _ = po.thermal(z0, talus, THERMAL_ITERS, bedrock=bed, bedrock_mode=po.BEDROCK_LITERAL,
+                                dtype=np.float64)
+        pp = po.VpipesParams.make(**dict(CONFIG2_VPIPES, iterations=VPIPES_ITERS))
+        r_vp = po.ref_vpipes(z0, pp)
+        o64_vp = po.vpipes(z0, pp, dtype=np.float64)
+        host = {"thermal_intended": o32_int, "thermal_literal": r_lit, "vpipes_z": r_vp[0],
+                "vpipes_sediment": r_vp[2], "vpipes_water": r_vp[1]}
+        out["host"] = {
+            "seconds": time.perf_counter() - t1, "cores": po.num_threads(),
+            "what": {"thermal_intended": "fp32 oracle (pinned to the reference text in every mode it has)",
+                     "thermal_literal": "reference kernel text", "vpipes_*": "reference kernel text"},
+            "sha256": {k: _digest(v) for k, v in host.items()},
+            "vs_fp64": {"thermal_intended": _errors(o32_int, o64_int, z0),
+                        "thermal_literal": _errors(r_lit, o64_lit, z0),
+                        "vpipes_z": _errors(r_vp[0], o64_vp[0], z0),
+                        "vpipes_sediment": _errors(r_vp[2], o64_vp[2], z0)},
+            "mass_drift": {"thermal_intended": drift(_material(o32_int)),
+                           "thermal_intended_fp64": drift(_material(o64_int)),
+                           "thermal_literal": drift(_material(r_lit)),
+                           "vpipes_material": drift(_material(r_vp[0], r_vp[2])),
+                           "vpipes_material_fp64": drift(_material(o64_vp[0], o64_vp[2]))},
+            "water_depth_max": float(r_vp[1].max())}
+    ok = True
+    if gpu is not None and host is not None:
+        cmp = {k: _errors(gpu[k], host[k], z0) for k in gpu}
+        out["gpu_vs_host"] = cmp
+        tol = {"thermal_intended": 1e-4, "thermal_literal": 1e-4, "vpipes_z": 1e-3, "vpipes_sediment": 1e-3,
+               "vpipes_water": 1e-3}
+        ok = all(cmp[k]["max_abs_of_range"] <= tol[k] for k in cmp)
+        out["within_tolerance"] = ok
+        out["value"] = cmp["vpipes_z"]["max_abs_of_range"]
     print(json.dumps(out), flush=True)
     return 0 if ok else 1
 
