@@ -66,10 +66,7 @@ constexpr int FWE_FLOWONLY = 16; /* flow and water passes only (flow_simulation)
  * code although a few words then spill.  The flow-only form
  * (flow_simulation) fits 40 registers, six CTAs per SM; a looser bound
  * lets the compiler take 46 and costs the sixth CTA (5 % slower). */
-#ifndef HM_FWE_BLOCKS
-#define HM_FWE_BLOCKS 5
-#endif
-constexpr int fwe_min_blocks(int flags) { return (flags & FWE_FLOWONLY) ? 6 : HM_FWE_BLOCKS; }
+constexpr int fwe_min_blocks(int flags) { return (flags & FWE_FLOWONLY) ? 6 : 5; }
 
 /* Shared-memory layout of the staged fields, one for both staging modes.
  * Every array row covers the 40 columns x0-4 .. x0+35 (a TMA box must start
@@ -333,11 +330,67 @@ __device__ __forceinline__ bool fwe_stage_tma_step(const FweMaps &maps, const Ad
  * the staged s1 box (columns x0-4 .. x0+35, rows y0-4 .. y0+19) read shared
  * memory, the rest s1 in global memory.  INNER: region 1 lies inside the
  * grid, so no cell is clamped. */
+/* advected sediment of one region-1 cell: column gx, row gy of the grid
+ * (clamped), at shared-memory row l and column cc */
+__device__ __forceinline__ void advect_cell(const VpConst &c, const float *__restrict__ s1g, int x0, int y0, int gx,
+                                            int gy, int l, int cc, FweSmem &sm)
+{
+  const int   nx = c.nx, ny = c.ny;
+  const float uu = sm.adv.u[gy - (y0 - 1)][gx - (x0 - 4)];
+  const float vv = sm.adv.v[gy - (y0 - 1)][gx - (x0 - 4)];
+  const float x = fsub((float)gx, fmul(c.dt, uu));
+  const float y = fsub((float)gy, fmul(c.dt, vv));
+  const Tap   t = linear_tap(x, y, nx, ny);
+  const int   bi0 = t.i0 - (x0 - 4), bi1 = t.i1 - (x0 - 4);
+  const int   bj0 = t.j0 - (y0 - 4), bj1 = t.j1 - (y0 - 4);
+  float       g00, g10, g01, g11;
+  if (bi0 >= 0 && bi1 < FW && bj0 >= 0 && bj1 < FS_H)
+  {
+    g00 = sm.adv.s1[bj0][bi0];
+    g10 = sm.adv.s1[bj0][bi1];
+    g01 = sm.adv.s1[bj1][bi0];
+    g11 = sm.adv.s1[bj1][bi1];
+  }
+  else
+  {
+    const size_t r0 = (size_t)t.j0 * nx, r1 = (size_t)t.j1 * nx;
+    g00 = __ldg(s1g + r0 + t.i0);
+    g10 = __ldg(s1g + r0 + t.i1);
+    g01 = __ldg(s1g + r1 + t.i0);
+    g11 = __ldg(s1g + r1 + t.i1);
+  }
+  sm.s[l][cc] = blend(t, g00, g10, g01, g11);
+}
+
+#ifndef HM_ADV_COLS
+#define HM_ADV_COLS 0
+#endif
+/* rows of region 1 one thread advects in the column layout */
+constexpr int ADV_ROWS = 3;
+
 template <bool INNER>
 __device__ __forceinline__ void advect_region1(const VpConst &c, const float *__restrict__ s1g, int x0, int y0,
                                                FweSmem &sm)
 {
   const int nx = c.nx, ny = c.ny;
+#if HM_ADV_COLS
+  /* thread t < 204 takes column 3 + t % 34 of region 1 and its rows
+   * ADV_ROWS (t / 34) .. + ADV_ROWS - 1: the column's index work is shared
+   * and its gathers are in flight together */
+  static_assert(FT_H1 % ADV_ROWS == 0, "region 1 splits into whole row groups");
+  const int t = threadIdx.x;
+  if (t >= FT_W1 * (FT_H1 / ADV_ROWS)) return;
+  const int cc = 3 + t % FT_W1, l0 = ADV_ROWS * (t / FT_W1);
+  int       gx = x0 - 4 + cc;
+  if (!INNER) gx = clampi(gx, 0, nx - 1);
+#pragma unroll
+  for (int r = 0; r < ADV_ROWS; r++)
+  {
+    int gy = y0 - 1 + l0 + r;
+    if (!INNER) gy = clampi(gy, 0, ny - 1);
+    advect_cell(c, s1g, x0, y0, gx, gy, l0 + r, cc, sm);
+  }
+#else
   for (int e = threadIdx.x; e < FT_W1 * FT_H1; e += FT_NT)
   {
     const int l = e / FT_W1, cc = 3 + (e - l * FT_W1);
@@ -347,31 +400,9 @@ __device__ __forceinline__ void advect_region1(const VpConst &c, const float *__
       gx = clampi(gx, 0, nx - 1);
       gy = clampi(gy, 0, ny - 1);
     }
-    const float uu = sm.adv.u[gy - (y0 - 1)][gx - (x0 - 4)];
-    const float vv = sm.adv.v[gy - (y0 - 1)][gx - (x0 - 4)];
-    const float x = fsub((float)gx, fmul(c.dt, uu));
-    const float y = fsub((float)gy, fmul(c.dt, vv));
-    const Tap   t = linear_tap(x, y, nx, ny);
-    const int   bi0 = t.i0 - (x0 - 4), bi1 = t.i1 - (x0 - 4);
-    const int   bj0 = t.j0 - (y0 - 4), bj1 = t.j1 - (y0 - 4);
-    float       g00, g10, g01, g11;
-    if (bi0 >= 0 && bi1 < FW && bj0 >= 0 && bj1 < FS_H)
-    {
-      g00 = sm.adv.s1[bj0][bi0];
-      g10 = sm.adv.s1[bj0][bi1];
-      g01 = sm.adv.s1[bj1][bi0];
-      g11 = sm.adv.s1[bj1][bi1];
-    }
-    else
-    {
-      const size_t r0 = (size_t)t.j0 * nx, r1 = (size_t)t.j1 * nx;
-      g00 = __ldg(s1g + r0 + t.i0);
-      g10 = __ldg(s1g + r0 + t.i1);
-      g01 = __ldg(s1g + r1 + t.i0);
-      g11 = __ldg(s1g + r1 + t.i1);
-    }
-    sm.s[l][cc] = blend(t, g00, g10, g01, g11);
+    advect_cell(c, s1g, x0, y0, gx, gy, l, cc, sm);
   }
+#endif
 }
 
 __device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
@@ -380,36 +411,14 @@ __device__ __forceinline__ void   sts2(float *p, float a, float b) { *reinterpre
 /* Store the values of a cell pair (columns gx, gx + 1 of row offset k = the
  * pair's first cell): one 8-byte store when both cells are in the grid and
  * the grids allow it, else one or two 4-byte stores. */
-#ifndef HM_ST_HINT
-#define HM_ST_HINT 0
-#endif
-#ifndef HM_EARLY_STORES
-#define HM_EARLY_STORES 0
-#endif
-__device__ __forceinline__ void st1(float *p, float a)
-{
-#if HM_ST_HINT == 2
-  __stcs(p, a);
-#else
-  *p = a;
-#endif
-}
-__device__ __forceinline__ void st2(float *p, float a, float b)
-{
-#if HM_ST_HINT == 2
-  __stcs(reinterpret_cast<float2 *>(p), make_float2(a, b));
-#else
-  *reinterpret_cast<float2 *>(p) = make_float2(a, b);
-#endif
-}
 __device__ __forceinline__ void st_pair(float *p, size_t k, float a, float b, bool second, bool vec)
 {
   if (second && vec)
-    st2(p + k, a, b);
+    *reinterpret_cast<float2 *>(p + k) = make_float2(a, b);
   else
   {
-    st1(p + k, a);
-    if (second) st1(p + k + 1, b);
+    p[k] = a;
+    if (second) p[k + 1] = b;
   }
 }
 
@@ -565,9 +574,12 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
     else
     {
       const float dea = fmul(d2a, c.keep), deb = fmul(d2b, c.keep);
-#if HM_EARLY_STORES
       /* what the water pass produced, stored before the erosion arithmetic
-       * so its registers are free there */
+       * so its registers are free there (the stores go through generic
+       * pointers, so the compiler keeps them after the shared-memory loads
+       * that follow them in the source: their order decides what stays
+       * live; 48 registers without spills, 2.5 % faster than storing after
+       * erosion) */
       st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
       st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
       st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
@@ -580,7 +592,6 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
         st_pair(io.u_out, k, ua, ub, second, vec);
         st_pair(io.v_out, k, va, vb, second, vec);
       }
-#endif
       const float2 zc = lds2(&sm.z[q][cc]), zn = lds2(&sm.z[q - 1][cc]), zs = lds2(&sm.z[q + 1][cc]);
       const float  zw = sm.z[q][cc - 1], ze = sm.z[q][cc + 2];
       const float2 s0 = lds2(&sm.s[l][cc]), sn = lds2(&sm.s[l - 1][cc]), ss = lds2(&sm.s[l + 1][cc]);
@@ -596,21 +607,6 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
         erosion_cell<false>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
         erosion_cell<false>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
       }
-#if !HM_EARLY_STORES
-      /* the cells' new fluxes, stored here where a warp writes whole rows */
-      st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
-      st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
-      st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
-      st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
-      st_pair(io.out.d, k, dea, deb, second, vec);
-      st_pair(io.u, k, ua, ub, second, vec);
-      st_pair(io.v, k, va, vb, second, vec);
-      if (io.u_out)
-      {
-        st_pair(io.u_out, k, ua, ub, second, vec);
-        st_pair(io.v_out, k, va, vb, second, vec);
-      }
-#endif
       st_pair(io.out.z, k, zoa, zob, second, vec);
       st_pair(io.s1, k, soa, sob, second, vec);
       part = (double)dea;
