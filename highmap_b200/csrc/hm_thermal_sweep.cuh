@@ -153,12 +153,22 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
 
   /* per row: the pair (x, y), the west neighbour of x and the east one of y */
   float vx[S2_P + 2], vy[S2_P + 2], vw[S2_P + 2], ve[S2_P + 2];
+#ifndef HM_TH_FAST
+#define HM_TH_FAST 0
+#endif
+  const bool halo_lane = lane == 0 || lane == 31;
   auto load = [&](int r, int q) {
     const float *row = a + (size_t)r * nx;
     const float2 t = __ldg(reinterpret_cast<const float2 *>(row + gxc));
     vx[q] = t.x;
     vy[q] = t.y;
+#if HM_TH_FAST
+    /* the halo value until the shuffles; only the edge lanes keep theirs */
+    vw[q] = halo_lane ? __ldg(row + hx) : 0.f;
+#else
+    (void)halo_lane;
     vw[q] = __ldg(row + hx); /* the halo value until the shuffles */
+#endif
   };
   auto exchange = [&](int q) {
     const float up = __shfl_up_sync(0xffffffffu, vy[q], 1), dn = __shfl_down_sync(0xffffffffu, vx[q], 1);
@@ -182,6 +192,23 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
     }
 #pragma unroll
     for (int q = 2; q < S2_P + 2; q++) exchange(q);
+#if HM_TH_FAST
+    /* a warp whose columns and rows are all interior: no border tests */
+    if (wx > 0 && wx + 64 < nx && j0 > 0 && j0 + S2_P < ny - 1 && j0 + S2_P <= y1)
+    {
+#pragma unroll
+      for (int q = 0; q < S2_P; q++)
+      {
+        float2 out;
+        out.x = R::cell(vx[q + 1], vw[q + 1], vx[q + 2], vx[q], vy[q + 1], vw[q], vw[q + 2], vy[q], vy[q + 2],
+                        tl[q].x, bd[q].x, first != 0, param);
+        out.y = R::cell(vy[q + 1], vx[q + 1], vy[q + 2], vy[q], ve[q + 1], vx[q], vx[q + 2], ve[q], ve[q + 2],
+                        tl[q].y, bd[q].y, first != 0, param);
+        *reinterpret_cast<float2 *>(b + (size_t)(j0 + q) * nx + gx) = out;
+      }
+    }
+    else
+#endif
 #pragma unroll
     for (int q = 0; q < S2_P; q++)
     {
