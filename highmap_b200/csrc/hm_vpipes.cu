@@ -250,6 +250,9 @@ VpConst vpipes_consts(int nx, int ny, const hm_vpipes_params &p)
   c.keep = 1.f - p.dt * p.evap_rate;
   c.rps = p.rain_per_step;
   c.fnx = (float)nx;
+  /* nx - 0.5 is a float exactly while nx < 2^23 */
+  c.xhi = nx < (1 << 22) ? (float)nx - 0.5f : 0.f;
+  c.yhi = ny < (1 << 22) ? (float)ny - 0.5f : 0.f;
   return c;
 }
 

@@ -60,6 +60,9 @@ struct VpConst
   float keep;        /* 1 - dt * evap_rate                              */
   float rps;         /* rain per step                                   */
   float fnx;         /* (float)nx, the slope scale of :156              */
+  float xhi, yhi;    /* nx - 0.5, ny - 0.5 (exact; 0 for grids too wide to
+                      * hold them exactly): sample points in [0.5, xhi) x
+                      * [0.5, yhi) need no mirror and no index clamps      */
 };
 
 /* Depth at the start of a step: the stored evaporated depth, plus the

@@ -342,8 +342,44 @@ __device__ __forceinline__ void advect_cell(const VpConst &c, const float *__res
   const float vv = sm.adv.v[gy - (y0 - 1)][gx - (x0 - 4)];
   const float x = fsub((float)gx, fmul(c.dt, uu));
   const float y = fsub((float)gy, fmul(c.dt, vv));
-  const Tap   t = linear_tap(x, y, nx, ny);
-  const int   bi0 = t.i0 - (x0 - 4), bi1 = t.i1 - (x0 - 4);
+  if (x >= 0.5f && x < c.xhi && y >= 0.5f && y < c.yhi)
+  {
+    /* The sample point lies inside the texel centres: the mirror of
+     * linear_tap returns the coordinate itself, floor(x - 0.5) lies in
+     * [0, nx - 2], so i0 needs no clamp and i1 = i0 + 1 (rows likewise).
+     * The same rounded operations as linear_tap, without the identities. */
+    Tap         tp;
+    const float xm = fsub(x, 0.5f), ym = fsub(y, 0.5f);
+    const float fx = floorf(xm), fy = floorf(ym);
+    tp.a = fsub(xm, fx);
+    tp.b = fsub(ym, fy);
+    tp.i0 = (int)fx;
+    tp.j0 = (int)fy;
+    tp.i1 = tp.i0 + 1;
+    tp.j1 = tp.j0 + 1;
+    const int bi = tp.i0 - (x0 - 4), bj = tp.j0 - (y0 - 4);
+    float     g00, g10, g01, g11;
+    if ((unsigned)bi < (unsigned)(FW - 1) && (unsigned)bj < (unsigned)(FS_H - 1))
+    {
+      const float *r = &sm.adv.s1[bj][bi];
+      g00 = r[0];
+      g10 = r[1];
+      g01 = r[FW];
+      g11 = r[FW + 1];
+    }
+    else
+    {
+      const float *r = s1g + (size_t)tp.j0 * nx + tp.i0;
+      g00 = __ldg(r);
+      g10 = __ldg(r + 1);
+      g01 = __ldg(r + nx);
+      g11 = __ldg(r + nx + 1);
+    }
+    sm.s[l][cc] = blend(tp, g00, g10, g01, g11);
+    return;
+  }
+  const Tap t = linear_tap(x, y, nx, ny);
+  const int bi0 = t.i0 - (x0 - 4), bi1 = t.i1 - (x0 - 4);
   const int   bj0 = t.j0 - (y0 - 4), bj1 = t.j1 - (y0 - 4);
   float       g00, g10, g01, g11;
   if (bi0 >= 0 && bi1 < FW && bj0 >= 0 && bj1 < FS_H)
