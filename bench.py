@@ -179,11 +179,13 @@ def _vp_kernels(shape):
     """Kernels of one vpipes step for the launch shape in use."""
     if shape and shape.get("tpb"):
         return "k_vp_fused + k_vp_fixup"
-    return "k_vp_fwe + k_vp_advect"
+    return ("k_vp_step_tma: the previous step's advection folded into this step's tile (the first step is "
+            "k_vp_fwe_tma, the last step's advection k_vp_advect)")
 
 
 def _traffic():
-    """dram bytes per vpipes launch from the committed ncu summary, if any."""
+    """DRAM bytes (read + write) of one vpipes step kernel launch at 4096^2
+    from the committed ncu summary, if any."""
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
             t = json.load(f)
