@@ -130,12 +130,13 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
  * step stages the job's sediment; later steps advect the previous step's
  * eroded sediment into the tile (fwe_stage_cp_async_step, advect_region1).
  * F: FWE_RTOPTS when every active vpipes job has pipe length 1 and
- * discharge exponent 1 (the lean form, four CTAs per SM), else
- * FWE_GENERIC (fp64 pow on the path, three CTAs per SM).  Thread 0 takes
+ * discharge exponent 1 (the lean form without fp64 pow), else FWE_GENERIC;
+ * both at three CTAs per SM (80 registers: a bound of four spills 484
+ * bytes per thread and ran 20 % slower).  Thread 0 takes
  * the CTA's next tile index while the current tile is computed, so the
  * atomic's latency is hidden. */
 template <int F>
-__global__ void __launch_bounds__(BT, F == FWE_GENERIC ? 3 : 4)
+__global__ void __launch_bounds__(BT, 3)
     k_batch_round(const BJob *__restrict__ jobs,
                   const int4 *__restrict__ vt,
                   int nv,
