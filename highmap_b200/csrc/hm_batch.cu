@@ -740,18 +740,86 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
   hm_batch *b = nullptr;
   int       st = hm_batch_create(ctx, &b);
   if (st) return st;
-  int maxit = 0;
+  /* Jobs of at least HM_BATCH_LARGE_CELLS cells fill the GPU on their own,
+   * and the plain step kernels (specialised on the step's options, TMA
+   * staging, five CTAs per SM) run them faster than the batch's generic
+   * tiles: they go one after another through the plain solvers on a side
+   * stream, beside the rounds of the smaller jobs.  Both are in the graph. */
+  std::vector<int> large;
+  size_t           lane_bytes = 0;
+  int              maxit = 0;
   for (int k = 0; k < njobs && !st; k++)
   {
+    const hm_job &j = jobs[k];
+    if ((st = check_job(j))) break;
+    if ((long long)j.nx * j.ny >= HM_BATCH_LARGE_CELLS && j.iterations > 0)
+    {
+      large.push_back(k);
+      const size_t need = j.kind == HM_JOB_THERMAL
+                              ? hm::thermal_scratch_floats(j.nx, j.ny, j.deposition_map != nullptr) * sizeof(float)
+                              : hm::vpipes_scratch_bytes(j.nx, j.ny);
+      lane_bytes = std::max(lane_bytes, need);
+      continue;
+    }
     int id;
-    st = hm_batch_add(b, &jobs[k], &id);
-    maxit = std::max(maxit, jobs[k].iterations);
+    st = hm_batch_add(b, &j, &id);
+    maxit = std::max(maxit, j.iterations);
+  }
+  void        *lane_mem = nullptr;
+  cudaStream_t side = nullptr;
+  cudaEvent_t  fork = nullptr, join = nullptr;
+  if (!st && !large.empty())
+  {
+    cudaError_t e = cudaMallocFromPoolAsync(&lane_mem, lane_bytes, b->pool, b->stream);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+    if (e != cudaSuccess)
+    {
+      cudaGetLastError();
+      st = hm::cuda_fail(e, "hm_batch_run: large-job lane set-up");
+    }
   }
   if (!st) st = upload_jobs(b);
-  if (!st && use_graph && maxit > 0)
+  /* the large jobs' plain solves, forked from and joined to the batch
+   * stream */
+  auto launch_large = [&]() -> int {
+    if (large.empty()) return HM_OK;
+    HM_CUDA_TRY(cudaEventRecord(fork, b->stream));
+    HM_CUDA_TRY(cudaStreamWaitEvent(side, fork, 0));
+    for (int k : large)
+    {
+      const hm_job &j = jobs[k];
+      int           rc;
+      if (j.kind == HM_JOB_THERMAL)
+      {
+        hm_thermal_options o;
+        hm_thermal_default_options(&o);
+        o.bedrock_mode = j.bedrock_mode;
+        rc = hm::thermal_core(b->device, j.z, j.nx, j.ny, j.talus, j.talus_value, j.iterations, j.bedrock,
+                              j.deposition_map, nullptr, &o, (float *)lane_mem, side);
+      }
+      else
+      {
+        hm_vpipes_params p = j.vpipes;
+        p.iterations = j.iterations;
+        rc = hm::vpipes_core(j.z, j.nx, j.ny, p, j.rain_map, j.water_depth, j.sediment, j.vel_u, j.vel_v, lane_mem,
+                             side);
+      }
+      if (rc) return rc;
+    }
+    HM_CUDA_TRY(cudaEventRecord(join, side));
+    return HM_OK;
+  };
+  auto join_large = [&]() -> int {
+    if (large.empty()) return HM_OK;
+    HM_CUDA_TRY(cudaStreamWaitEvent(b->stream, join, 0));
+    return HM_OK;
+  };
+  if (!st && use_graph && (maxit > 0 || !large.empty()))
   {
-    /* every round of the batch in one graph; the host-side plan (tile
-     * lists, uploads) is made before the capture */
+    /* every round of the batch and the large lane in one graph; the
+     * host-side plan (tile lists, uploads) is made before the capture */
     Plan            pl;
     cudaGraph_t     graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -765,7 +833,9 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
     }
     if (!st)
     {
-      int rc = launch_rounds(b, pl);
+      int rc = launch_large();
+      if (!rc) rc = launch_rounds(b, pl);
+      if (!rc) rc = join_large();
       e = cudaStreamEndCapture(b->stream, &graph);
       if (rc) st = rc;
       else if (e != cudaSuccess) st = hm::cuda_fail(e, "hm_batch_run: cudaStreamEndCapture");
@@ -788,9 +858,19 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
   }
   else if (!st)
   {
-    st = run_rounds(b, maxit);
+    st = launch_large();
+    if (!st) st = run_rounds(b, maxit);
+    if (!st) st = join_large();
     if (!st) st = hm_batch_synchronize(b);
   }
+  if (lane_mem)
+  {
+    cudaFreeAsync(lane_mem, b->stream);
+    cudaStreamSynchronize(b->stream);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
+  if (side) cudaStreamDestroy(side);
   int st2 = hm_batch_destroy(b);
   return st ? st : st2;
 }

@@ -103,6 +103,25 @@ def test_batch_run_matches_oracle(gpu, use_graph):
     _verify(cases)
 
 
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_run_with_large_jobs(gpu, use_graph):
+    """Jobs of at least 2^20 cells run through the plain solvers on a side
+    stream beside the rounds of the small ones; every job still gives the
+    oracle's bits (the oracle on the large grids is bounded by the
+    iteration counts)."""
+    import torch
+    from highmap_b200 import batch as B
+    specs = [("thermal", 1024, 1024, 9, dict(talus="map", bedrock=True, depo=True)),
+             ("vpipes", 1032, 1024, 6, dict(params=CONFIG2, outputs=True)),
+             ("vpipes", 1024, 1040, 5, dict(params=dict(), outputs=True)),
+             ("thermal", 96, 80, 12, dict(talus=0.02)),
+             ("vpipes", 120, 88, 14, dict(params=CONFIG2, outputs=True))]
+    jobs, cases = _make(specs, seed0=70)
+    B.run(jobs, use_graph=use_graph)
+    torch.cuda.synchronize()
+    _verify(cases)
+
+
 def test_staggered_admission(gpu):
     """Jobs admitted at different rounds (as the served form admits them)
     still each see their own step sequence."""
