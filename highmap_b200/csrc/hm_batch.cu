@@ -701,6 +701,10 @@ int hm_batch_release(hm_batch *b, int job_id)
   if (h.mem) HM_CUDA_TRY(cudaFreeAsync(h.mem, b->stream));
   h.mem = nullptr;
   h.live = false;
+  /* a job released before it finished (cancelled) leaves the rounds: the
+   * tile lists are rebuilt without it before the next round, which would
+   * otherwise still hold tiles over the freed state */
+  if (!h.finished) b->tiles_dirty = true;
   h.finished = true;
   return HM_OK;
 }

@@ -686,7 +686,9 @@ int       hm_batch_add(hm_batch *batch, const hm_job *job, int *job_id);
 int       hm_batch_step(hm_batch *batch, int rounds);
 int       hm_batch_synchronize(hm_batch *batch);
 int       hm_batch_job_status(hm_batch *batch, int job_id, int *steps_done, int *finished);
-/* Frees a job's device state (after its outputs are read). */
+/* Frees a job's device state (after its outputs are read).  A job released
+ * before it finished is cancelled: it leaves the rounds, its outputs are not
+ * written, and the other jobs go on unaffected. */
 int       hm_batch_release(hm_batch *batch, int job_id);
 size_t    hm_batch_bytes_in_use(const hm_batch *batch);
 long long hm_batch_round(const hm_batch *batch);

@@ -122,6 +122,34 @@ def test_batch_run_with_large_jobs(gpu, use_graph):
     _verify(cases)
 
 
+def test_cancelled_job_leaves_the_others_exact(gpu):
+    """A job released before it finishes (a cancelled request) leaves the
+    rounds at once; the jobs beside it finish with the oracle's bits and the
+    batch's device memory returns to what the others hold."""
+    import torch
+    from highmap_b200 import batch as B
+    specs = [("vpipes", 200, 136, 30, dict(params=CONFIG2, outputs=True)),
+             ("vpipes", 264, 200, 40, dict(params=CONFIG2)),
+             ("thermal", 160, 120, 35, dict(talus="map", bedrock=True, depo=True)),
+             ("thermal", 320, 96, 45, dict(talus=0.02))]
+    jobs, cases = _make(specs, seed0=80)
+    b = B.Batch()
+    ids = [b.add(j) for j in jobs]
+    b.step(6)
+    cancelled = (ids[1], ids[3])
+    for i in cancelled:
+        assert not b.status(i)[1]
+        b.release(i)
+    keep = [k for k in range(len(ids)) if ids[k] not in cancelled]
+    assert b.bytes_in_use() == sum(B.job_bytes(jobs[k]) for k in keep)
+    while any(not b.status(ids[k])[1] for k in keep):
+        b.step(5)
+    b.synchronize()
+    torch.cuda.synchronize()
+    _verify([cases[k] for k in keep])
+    b.close()
+
+
 def test_staggered_admission(gpu):
     """Jobs admitted at different rounds (as the served form admits them)
     still each see their own step sequence."""
