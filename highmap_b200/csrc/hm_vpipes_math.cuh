@@ -19,8 +19,6 @@
 #ifndef HM_VPIPES_MATH_CUH
 #define HM_VPIPES_MATH_CUH
 
-#include <cfloat>
-
 namespace hm
 {
 
@@ -124,16 +122,7 @@ __device__ __forceinline__ void flow_cell(const VpConst &c,
   /* k = sum > 1e-5 ? d1 * l * l / (sum * dt) : 0, clamped to [0, 1]; with
    * l = 1 the two products are d1 itself (x * 1 is exact for every x) */
   const T num = PL_ONE ? d1c : fmul(fmul(d1c, bc<T>(c.pl)), bc<T>(c.pl));
-  const T m = fmul(sum, bc<T>(c.dt));
-  /* when num >= m > 0 with num finite, num / m >= 1 exactly, so its
-   * rounding is >= 1 and the clamp below makes k exactly 1: the division
-   * is skipped there (every other case, NaN and infinities included,
-   * divides) */
-  T kq;
-  if (m > zero && num >= m && num <= bc<T>(FLT_MAX))
-    kq = bc<T>(1.f);
-  else
-    kq = fdiv(num, m);
+  T       kq = fdiv(num, fmul(sum, bc<T>(c.dt)));
   T k = sel_gt(sum, bc<T>(1e-5f), kq, zero);
   k = rmin(rmax(k, zero), bc<T>(1.f));
   fl = fmul(nl, k);
@@ -177,14 +166,7 @@ __device__ __forceinline__ void erosion_cell(const VpConst &c,
   T       dzn = rmax(bc<T>(1e-3f), fmul(bc<T>(c.fnx), talus));
   T       salpha = rmax(bc<T>(0.01f), fdiv(dzn, hyp(bc<T>(1.f), dzn)));
   T       speed = hyp(u, v);
-  /* d2 - ratio * water_height > 0 (its sign is exact in one fma) means
-   * d2 / water_height > ratio, whose rounding is then >= ratio: the min is
-   * ratio and the division is skipped */
-  T depth;
-  if (c.water_height > 0.f && __fmaf_rn(-c.ratio, c.water_height, d2) > 0.f)
-    depth = bc<T>(c.ratio);
-  else
-    depth = rmin(fdiv(d2, bc<T>(c.water_height)), bc<T>(c.ratio));
+  T       depth = rmin(fdiv(d2, bc<T>(c.water_height)), bc<T>(c.ratio));
   T       discharge = fmul(depth, speed);
   T       pw = KEXP_ONE ? discharge : powr(discharge, c.k_exp);
   T       capa = fmul(fmul(bc<T>(c.k_capacity), pw), salpha);
