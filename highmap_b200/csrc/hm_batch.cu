@@ -744,13 +744,26 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
   hm_batch *b = nullptr;
   int       st = hm_batch_create(ctx, &b);
   if (st) return st;
-  /* Jobs of at least HM_BATCH_LARGE_CELLS cells fill the GPU on their own,
-   * and the plain step kernels (specialised on the step's options, TMA
-   * staging, five CTAs per SM) run them faster than the batch's generic
-   * tiles: they go one after another through the plain solvers on a side
-   * stream, beside the rounds of the smaller jobs.  Both are in the graph. */
+  /* Jobs of at least HM_BATCH_LARGE_CELLS cells fill most of the GPU on
+   * their own, and the plain step kernels (specialised on the step's
+   * options, TMA staging, five CTAs per SM) run them faster than the
+   * batch's generic tiles.  They go through the plain solvers on
+   * HM_BATCH_LANES side streams, each lane's jobs one after another, the
+   * lanes balanced by cell-updates (longest first onto the least loaded
+   * lane), beside the rounds of the smaller jobs.  The lanes are launched
+   * directly, before the rounds are captured, so they run while the graph
+   * is built; the batch stream joins them at the end. */
+  struct Lane
+  {
+    std::vector<int> jobs;
+    size_t           bytes = 0;
+    double           work = 0.0;
+    void            *mem = nullptr;
+    cudaStream_t     s = nullptr;
+    cudaEvent_t      join = nullptr;
+  };
+  Lane             lanes[HM_BATCH_LANES];
   std::vector<int> large;
-  size_t           lane_bytes = 0;
   int              maxit = 0;
   for (int k = 0; k < njobs && !st; k++)
   {
@@ -759,25 +772,38 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
     if ((long long)j.nx * j.ny >= HM_BATCH_LARGE_CELLS && j.iterations > 0)
     {
       large.push_back(k);
-      const size_t need = j.kind == HM_JOB_THERMAL
-                              ? hm::thermal_scratch_floats(j.nx, j.ny, j.deposition_map != nullptr) * sizeof(float)
-                              : hm::vpipes_scratch_bytes(j.nx, j.ny);
-      lane_bytes = std::max(lane_bytes, need);
       continue;
     }
     int id;
     st = hm_batch_add(b, &j, &id);
     maxit = std::max(maxit, j.iterations);
   }
-  void        *lane_mem = nullptr;
-  cudaStream_t side = nullptr;
-  cudaEvent_t  fork = nullptr, join = nullptr;
+  auto work = [&](int k) { return (double)jobs[k].nx * jobs[k].ny * jobs[k].iterations *
+                                  (jobs[k].kind == HM_JOB_VPIPES ? 5.0 : 1.0); };
+  std::stable_sort(large.begin(), large.end(), [&](int x, int y) { return work(x) > work(y); });
+  for (int k : large)
+  {
+    Lane *l = &lanes[0];
+    for (Lane &c : lanes)
+      if (c.work < l->work) l = &c;
+    const hm_job &j = jobs[k];
+    l->jobs.push_back(k);
+    l->work += work(k);
+    l->bytes = std::max(l->bytes, j.kind == HM_JOB_THERMAL
+                                      ? hm::thermal_scratch_floats(j.nx, j.ny, j.deposition_map != nullptr) * sizeof(float)
+                                      : hm::vpipes_scratch_bytes(j.nx, j.ny));
+  }
+  cudaEvent_t fork = nullptr;
   if (!st && !large.empty())
   {
-    cudaError_t e = cudaMallocFromPoolAsync(&lane_mem, lane_bytes, b->pool, b->stream);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+    cudaError_t e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    for (Lane &l : lanes)
+    {
+      if (l.jobs.empty() || e != cudaSuccess) continue;
+      e = cudaMallocFromPoolAsync(&l.mem, l.bytes, b->pool, b->stream);
+      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&l.s, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l.join, cudaEventDisableTiming);
+    }
     if (e != cudaSuccess)
     {
       cudaGetLastError();
@@ -785,50 +811,55 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
     }
   }
   if (!st) st = upload_jobs(b);
-  /* the large jobs' plain solves, forked from and joined to the batch
-   * stream */
+  /* the large jobs' plain solves, each lane forked from and joined to the
+   * batch stream */
   auto launch_large = [&]() -> int {
     if (large.empty()) return HM_OK;
     HM_CUDA_TRY(cudaEventRecord(fork, b->stream));
-    HM_CUDA_TRY(cudaStreamWaitEvent(side, fork, 0));
-    for (int k : large)
+    for (Lane &l : lanes)
     {
-      const hm_job &j = jobs[k];
-      int           rc;
-      if (j.kind == HM_JOB_THERMAL)
+      if (l.jobs.empty()) continue;
+      HM_CUDA_TRY(cudaStreamWaitEvent(l.s, fork, 0));
+      for (int k : l.jobs)
       {
-        hm_thermal_options o;
-        hm_thermal_default_options(&o);
-        o.bedrock_mode = j.bedrock_mode;
-        rc = hm::thermal_core(b->device, j.z, j.nx, j.ny, j.talus, j.talus_value, j.iterations, j.bedrock,
-                              j.deposition_map, nullptr, &o, (float *)lane_mem, side);
+        const hm_job &j = jobs[k];
+        int           rc;
+        if (j.kind == HM_JOB_THERMAL)
+        {
+          hm_thermal_options o;
+          hm_thermal_default_options(&o);
+          o.bedrock_mode = j.bedrock_mode;
+          rc = hm::thermal_core(b->device, j.z, j.nx, j.ny, j.talus, j.talus_value, j.iterations, j.bedrock,
+                                j.deposition_map, nullptr, &o, (float *)l.mem, l.s);
+        }
+        else
+        {
+          hm_vpipes_params p = j.vpipes;
+          p.iterations = j.iterations;
+          rc = hm::vpipes_core(j.z, j.nx, j.ny, p, j.rain_map, j.water_depth, j.sediment, j.vel_u, j.vel_v, l.mem,
+                               l.s);
+        }
+        if (rc) return rc;
       }
-      else
-      {
-        hm_vpipes_params p = j.vpipes;
-        p.iterations = j.iterations;
-        rc = hm::vpipes_core(j.z, j.nx, j.ny, p, j.rain_map, j.water_depth, j.sediment, j.vel_u, j.vel_v, lane_mem,
-                             side);
-      }
-      if (rc) return rc;
+      HM_CUDA_TRY(cudaEventRecord(l.join, l.s));
     }
-    HM_CUDA_TRY(cudaEventRecord(join, side));
     return HM_OK;
   };
   auto join_large = [&]() -> int {
-    if (large.empty()) return HM_OK;
-    HM_CUDA_TRY(cudaStreamWaitEvent(b->stream, join, 0));
+    for (Lane &l : lanes)
+      if (!l.jobs.empty()) HM_CUDA_TRY(cudaStreamWaitEvent(b->stream, l.join, 0));
     return HM_OK;
   };
-  if (!st && use_graph && (maxit > 0 || !large.empty()))
+  if (!st && use_graph && maxit > 0)
   {
-    /* every round of the batch and the large lane in one graph; the
-     * host-side plan (tile lists, uploads) is made before the capture */
+    /* every round of the batch in one graph; the host-side plan (tile
+     * lists, uploads) is made before the capture */
     Plan            pl;
     cudaGraph_t     graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     st = plan_rounds(b, maxit, pl);
     if (!st) st = hm_batch_synchronize(b);
+    if (!st) st = launch_large();
     cudaError_t e = cudaSuccess;
     if (!st)
     {
@@ -837,9 +868,7 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
     }
     if (!st)
     {
-      int rc = launch_large();
-      if (!rc) rc = launch_rounds(b, pl);
-      if (!rc) rc = join_large();
+      int rc = launch_rounds(b, pl);
       e = cudaStreamEndCapture(b->stream, &graph);
       if (rc) st = rc;
       else if (e != cudaSuccess) st = hm::cuda_fail(e, "hm_batch_run: cudaStreamEndCapture");
@@ -856,6 +885,7 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
       if (e != cudaSuccess) st = hm::cuda_fail(e, "hm_batch_run: cudaGraphLaunch");
       hm::count_launch(0);
     }
+    if (!st) st = join_large();
     if (!st) st = hm_batch_synchronize(b);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -867,14 +897,19 @@ int hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph)
     if (!st) st = join_large();
     if (!st) st = hm_batch_synchronize(b);
   }
-  if (lane_mem)
+  /* the lanes are done (joined, or synchronised here on an error path)
+   * before their memory goes back to the pool */
+  for (Lane &l : lanes)
+    if (l.s) cudaStreamSynchronize(l.s);
+  for (Lane &l : lanes)
+    if (l.mem) cudaFreeAsync(l.mem, b->stream);
+  cudaStreamSynchronize(b->stream);
+  for (Lane &l : lanes)
   {
-    cudaFreeAsync(lane_mem, b->stream);
-    cudaStreamSynchronize(b->stream);
+    if (l.join) cudaEventDestroy(l.join);
+    if (l.s) cudaStreamDestroy(l.s);
   }
   if (fork) cudaEventDestroy(fork);
-  if (join) cudaEventDestroy(join);
-  if (side) cudaStreamDestroy(side);
   int st2 = hm_batch_destroy(b);
   return st ? st : st2;
 }

@@ -105,8 +105,8 @@ def test_batch_run_matches_oracle(gpu, use_graph):
 
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_batch_run_with_large_jobs(gpu, use_graph):
-    """Jobs of at least 2^20 cells run through the plain solvers on a side
-    stream beside the rounds of the small ones; every job still gives the
+    """Jobs of at least 2^18 cells run through the plain solvers on side
+    streams beside the rounds of the small ones; every job still gives the
     oracle's bits (the oracle on the large grids is bounded by the
     iteration counts)."""
     import torch
@@ -114,6 +114,8 @@ def test_batch_run_with_large_jobs(gpu, use_graph):
     specs = [("thermal", 1024, 1024, 9, dict(talus="map", bedrock=True, depo=True)),
              ("vpipes", 1032, 1024, 6, dict(params=CONFIG2, outputs=True)),
              ("vpipes", 1024, 1040, 5, dict(params=dict(), outputs=True)),
+             ("thermal", 600, 520, 7, dict(talus=0.02)),
+             ("vpipes", 512, 512, 11, dict(params=FAST, outputs=True)),
              ("thermal", 96, 80, 12, dict(talus=0.02)),
              ("vpipes", 120, 88, 14, dict(params=CONFIG2, outputs=True))]
     jobs, cases = _make(specs, seed0=70)
