@@ -694,12 +694,12 @@ size_t    hm_batch_bytes_in_use(const hm_batch *batch);
 long long hm_batch_round(const hm_batch *batch);
 /* All jobs to completion in one call; use_graph != 0 captures every round
  * into one CUDA graph.  Returns after the results are written.  Jobs of at
- * least HM_BATCH_LARGE_CELLS cells, which fill most of the GPU on their
- * own, are solved by the plain step kernels on HM_BATCH_LANES side streams
- * (balanced by cell-updates) beside the rounds of the smaller jobs, in the
- * same graph; results are the same either way. */
-#define HM_BATCH_LARGE_CELLS (1 << 18)
-#define HM_BATCH_LANES 3
+ * least HM_BATCH_LARGE_CELLS cells, which fill the GPU on their own, are
+ * solved by the plain step kernels on HM_BATCH_LANES side streams (balanced
+ * by cell-updates) beside the rounds of the smaller jobs, launched while the
+ * rounds' graph is built; results are the same either way. */
+#define HM_BATCH_LARGE_CELLS (1 << 20)
+#define HM_BATCH_LANES 1
 int       hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_graph);
 
 /* ---- autotuner ----------------------------------------------------------- */

@@ -105,10 +105,10 @@ def test_batch_run_matches_oracle(gpu, use_graph):
 
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_batch_run_with_large_jobs(gpu, use_graph):
-    """Jobs of at least 2^18 cells run through the plain solvers on side
-    streams beside the rounds of the small ones; every job still gives the
-    oracle's bits (the oracle on the large grids is bounded by the
-    iteration counts)."""
+    """Jobs of at least 2^20 cells run through the plain solvers on a side
+    stream beside the rounds of the smaller ones (here also grids of 2^18
+    cells and more, batched); every job still gives the oracle's bits (the
+    oracle on the large grids is bounded by the iteration counts)."""
     import torch
     from highmap_b200 import batch as B
     specs = [("thermal", 1024, 1024, 9, dict(talus="map", bedrock=True, depo=True)),
