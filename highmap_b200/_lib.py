@@ -42,7 +42,7 @@ EXPORTED = (
     "hm_batch_synchronize", "hm_batch_job_status", "hm_batch_release", "hm_batch_bytes_in_use",
     "hm_batch_round", "hm_batch_run",
     "hm_autotune", "hm_autotune_save", "hm_autotune_load", "hm_autotune_clear", "hm_vpipes_set_algorithm",
-    "hm_debug_tma_expect_extra",
+    "hm_debug_tma_expect_extra", "hm_batch_snapshot_bytes", "hm_batch_evict", "hm_batch_restore",
 )
 
 HM_JOB_THERMAL = 1
@@ -164,6 +164,10 @@ def _declare(lib):
     lib.hm_batch_release.argtypes = [vp, i]
     lib.hm_batch_bytes_in_use.argtypes = [vp]
     lib.hm_batch_bytes_in_use.restype = C.c_size_t
+    lib.hm_batch_snapshot_bytes.argtypes = [vp, i]
+    lib.hm_batch_snapshot_bytes.restype = C.c_size_t
+    lib.hm_batch_evict.argtypes = [vp, i, vp]
+    lib.hm_batch_restore.argtypes = [vp, i, vp]
     lib.hm_batch_round.argtypes = [vp]
     lib.hm_batch_round.restype = C.c_longlong
     lib.hm_batch_run.argtypes = [vp, vp, i, i]

@@ -106,6 +106,19 @@ class Batch:
     def bytes_in_use(self) -> int:
         return int(L.lib().hm_batch_bytes_in_use(self._h))
 
+    def evict(self, job_id: int):
+        """Move an unfinished job's device state to host memory (a numpy
+        byte array); the job leaves the rounds until ``restore``."""
+        import numpy as np
+        snap = np.empty(int(L.lib().hm_batch_snapshot_bytes(self._h, int(job_id))), dtype=np.uint8)
+        L.check(L.lib().hm_batch_evict(self._h, int(job_id), snap.ctypes.data_as(C.c_void_p)))
+        return snap
+
+    def restore(self, job_id: int, snapshot) -> None:
+        """Admit an evicted job again from its snapshot; it goes on from the
+        step it had reached."""
+        L.check(L.lib().hm_batch_restore(self._h, int(job_id), snapshot.ctypes.data_as(C.c_void_p)))
+
     @property
     def round(self) -> int:
         return int(L.lib().hm_batch_round(self._h))

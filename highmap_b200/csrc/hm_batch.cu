@@ -228,8 +228,47 @@ struct HJob
   int       steps = 0;
   bool      live = false;     /* admitted and not released */
   bool      finished = false; /* outputs written            */
+  bool      evicted = false;  /* state held by the caller (hm_batch_evict) */
+  uintptr_t dev_block = 0;    /* device address of the state block the descriptor points into */
   float    *z0 = nullptr;     /* thermal input copy for the deposition map */
 };
+
+/* the pointer p moved with its block from old_base to new_base, if it
+ * points into the bytes-long block */
+template <class T>
+void rebase(T *&p, uintptr_t old_base, size_t bytes, char *new_base)
+{
+  const uintptr_t q = (uintptr_t)p;
+  if (p && q >= old_base && q < old_base + bytes) p = (T *)(new_base + (q - old_base));
+}
+
+/* every pointer of a job's descriptor into its state block, moved to the
+ * block's new address */
+void rebase_job(HJob &h, uintptr_t old_base, char *new_base)
+{
+  const size_t n = h.bytes;
+  hm::BJob    &d = h.dev;
+  for (auto &t : d.tz) rebase(t, old_base, n, new_base);
+  for (auto &f : d.cp)
+  {
+    rebase(f.z, old_base, n, new_base);
+    rebase(f.d, old_base, n, new_base);
+    rebase(f.s, old_base, n, new_base);
+    rebase(f.fl, old_base, n, new_base);
+    rebase(f.fr, old_base, n, new_base);
+    rebase(f.ft, old_base, n, new_base);
+    rebase(f.fb, old_base, n, new_base);
+  }
+  for (int k = 0; k < 2; k++)
+  {
+    rebase(d.s1[k], old_base, n, new_base);
+    rebase(d.u[k], old_base, n, new_base);
+    rebase(d.v[k], old_base, n, new_base);
+  }
+  rebase(d.partials, old_base, n, new_base);
+  rebase(d.sc, old_base, n, new_base);
+  rebase(h.z0, old_base, n, new_base);
+}
 
 size_t job_bytes(const hm_job &j)
 {
@@ -404,7 +443,7 @@ int plan_rounds(hm_batch *b, int rounds, Plan &pl)
     TileLists &tl = *b->lists;
     tl.act.clear();
     for (size_t k = 0; k < b->jobs.size(); k++)
-      if (b->jobs[k].live && !b->jobs[k].finished) tl.act.push_back((int)k);
+      if (b->jobs[k].live && !b->jobs[k].finished && !b->jobs[k].evicted) tl.act.push_back((int)k);
     /* every active job advances by the same number of steps per round, so
      * this order holds until the set of jobs changes */
     std::stable_sort(tl.act.begin(), tl.act.end(), [&](int x, int y) { return remaining(x) > remaining(y); });
@@ -594,6 +633,7 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
     cudaGetLastError();
     return hm::cuda_fail(e, "hm_batch_add: job state allocation");
   }
+  h.dev_block = (uintptr_t)h.mem;
   const size_t na = align_up((size_t)job->nx * job->ny, 64);
   float       *base = (float *)h.mem;
   hm::BJob    &d = h.dev;
@@ -714,8 +754,76 @@ size_t hm_batch_bytes_in_use(const hm_batch *b)
   if (!b) return 0;
   size_t t = 0;
   for (const HJob &h : b->jobs)
-    if (h.live) t += h.bytes;
+    if (h.live && !h.evicted) t += h.bytes;
   return t;
+}
+
+size_t hm_batch_snapshot_bytes(const hm_batch *b, int job_id)
+{
+  if (!b || job_id < 0 || job_id >= (int)b->jobs.size()) return 0;
+  const HJob &h = b->jobs[job_id];
+  return h.bytes + (size_t)h.desc.nx * h.desc.ny * sizeof(float);
+}
+
+int hm_batch_evict(hm_batch *b, int job_id, void *snapshot)
+{
+  hm::clear_error();
+  if (!b || job_id < 0 || job_id >= (int)b->jobs.size() || !snapshot)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_batch_evict: unknown job or NULL snapshot");
+  HJob &h = b->jobs[job_id];
+  if (!h.live || h.finished || h.evicted || !h.mem)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_batch_evict: the job is not an unfinished, resident job");
+  int st = hm::use_device(b->device);
+  if (st) return st;
+  /* the job's state block, then its heights (the caller's grid, which the
+   * steps update in place) */
+  char *dst = (char *)snapshot;
+  HM_CUDA_TRY(cudaMemcpyAsync(dst, h.mem, h.bytes, cudaMemcpyDeviceToHost, b->stream));
+  HM_CUDA_TRY(cudaMemcpyAsync(dst + h.bytes, h.desc.z, (size_t)h.desc.nx * h.desc.ny * sizeof(float),
+                              cudaMemcpyDeviceToHost, b->stream));
+  HM_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  HM_CUDA_TRY(cudaFreeAsync(h.mem, b->stream));
+  h.mem = nullptr;
+  h.evicted = true;
+  b->tiles_dirty = true;
+  return HM_OK;
+}
+
+int hm_batch_restore(hm_batch *b, int job_id, const void *snapshot)
+{
+  hm::clear_error();
+  if (!b || job_id < 0 || job_id >= (int)b->jobs.size() || !snapshot)
+    return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_batch_restore: unknown job or NULL snapshot");
+  HJob &h = b->jobs[job_id];
+  if (!h.live || !h.evicted) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_batch_restore: the job is not evicted");
+  int st = hm::use_device(b->device);
+  if (st) return st;
+  void       *mem = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&mem, h.bytes, b->pool, b->stream);
+  if (e != cudaSuccess)
+  {
+    cudaGetLastError();
+    return hm::cuda_fail(e, "hm_batch_restore: job state allocation");
+  }
+  const char *src = (const char *)snapshot;
+  HM_CUDA_TRY(cudaMemcpyAsync(mem, src, h.bytes, cudaMemcpyHostToDevice, b->stream));
+  HM_CUDA_TRY(cudaMemcpyAsync(h.desc.z, src + h.bytes, (size_t)h.desc.nx * h.desc.ny * sizeof(float),
+                              cudaMemcpyHostToDevice, b->stream));
+  /* the pageable source must stay valid until the copies are done */
+  HM_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  /* the state block moved: its pointers follow it.  The block held by the
+   * snapshot's job was freed at eviction, so only its old address is used,
+   * as a number. */
+  rebase_job(h, h.dev_block, (char *)mem);
+  h.mem = mem;
+  h.dev_block = (uintptr_t)mem;
+  /* the job goes on from the step it had reached: its next step is the
+   * batch's next round */
+  h.dev.start = b->round - h.steps;
+  h.evicted = false;
+  b->dirty = true;
+  b->tiles_dirty = true;
+  return HM_OK;
 }
 
 long long hm_batch_round(const hm_batch *b) { return b ? b->round : -1; }

@@ -691,6 +691,17 @@ int       hm_batch_job_status(hm_batch *batch, int job_id, int *steps_done, int 
  * written, and the other jobs go on unaffected. */
 int       hm_batch_release(hm_batch *batch, int job_id);
 size_t    hm_batch_bytes_in_use(const hm_batch *batch);
+/* Eviction under an HBM budget (no counterpart in the reference).
+ * hm_batch_evict copies an unfinished job's device state (its state block,
+ * then its heights) into `snapshot`, hm_batch_snapshot_bytes bytes of host
+ * memory, and frees the block: the job leaves the rounds and stops counting
+ * in hm_batch_bytes_in_use.  Its z grid stays the caller's.
+ * hm_batch_restore admits it again from the snapshot (z must still be
+ * valid).  The job goes on from the step it had reached with the batch's
+ * next round, and its results are the same as if it had never left. */
+size_t    hm_batch_snapshot_bytes(const hm_batch *batch, int job_id);
+int       hm_batch_evict(hm_batch *batch, int job_id, void *snapshot);
+int       hm_batch_restore(hm_batch *batch, int job_id, const void *snapshot);
 long long hm_batch_round(const hm_batch *batch);
 /* All jobs to completion in one call; use_graph != 0 captures every round
  * into one CUDA graph.  Returns after the results are written.  Jobs of at

@@ -152,6 +152,41 @@ def test_cancelled_job_leaves_the_others_exact(gpu):
     b.close()
 
 
+def test_evict_and_restore_is_bit_identical(gpu):
+    """Jobs moved to host memory mid-run (eviction under an HBM budget) and
+    admitted again later go on from the step they had reached: every job,
+    evicted or not, ends with the oracle's bits, and the evicted jobs stop
+    counting against the batch's device memory while they are out."""
+    import torch
+    from highmap_b200 import batch as B
+    specs = [("vpipes", 200, 136, 30, dict(params=CONFIG2, outputs=True)),
+             ("vpipes", 136, 120, 26, dict(params=dict(), outputs=True)),
+             ("thermal", 160, 120, 35, dict(talus="map", bedrock=True, depo=True)),
+             ("thermal", 96, 200, 28, dict(talus=0.02))]
+    jobs, cases = _make(specs, seed0=90)
+    b = B.Batch()
+    ids = [b.add(j) for j in jobs]
+    b.step(7)
+    full = b.bytes_in_use()
+    snaps = {}
+    for k in (1, 2):
+        steps_before = b.status(ids[k])[0]
+        snaps[k] = b.evict(ids[k])
+        assert b.status(ids[k]) == (steps_before, False)
+    assert b.bytes_in_use() == full - B.job_bytes(jobs[1]) - B.job_bytes(jobs[2])
+    b.step(9)  # the others advance; the evicted two do not
+    assert b.status(ids[1])[0] == 7 and b.status(ids[2])[0] == 7
+    for k in (2, 1):
+        b.restore(ids[k], snaps[k])
+    assert b.bytes_in_use() == full
+    while any(not b.status(i)[1] for i in ids):
+        b.step(6)
+    b.synchronize()
+    torch.cuda.synchronize()
+    _verify(cases)
+    b.close()
+
+
 def test_staggered_admission(gpu):
     """Jobs admitted at different rounds (as the served form admits them)
     still each see their own step sequence."""
