@@ -7,9 +7,11 @@
  * Every row of z is loaded once per warp (lanes 0 and 31 also load the
  * column just outside the warp) and the west / east neighbours come from
  * warp shuffles, so a cell costs two coalesced loads per 32 cells instead
- * of nine loads.  The loads of SW_P rows (z, talus, bedrock) are issued
- * before any of them is used, which keeps enough bytes in flight to cover
- * the HBM latency.  Cell rule and border copies as the reference kernel
+ * of nine loads.  The loads of P rows (z, talus, bedrock; a template
+ * parameter) are issued before any of them is used, which keeps enough
+ * bytes in flight to cover the HBM latency: the plain kernels take 8 (4
+ * row pairs), the batched form's persistent kernel fewer, as its
+ * occupancy hides the latency instead.  Cell rule and border copies as the reference kernel
  * (HighMap/src/gpu_opencl/kernels/thermal.cl:26-100, Jacobi form; border
  * copies _common_index.cl:106-132).
  */
@@ -40,8 +42,9 @@ struct TalusExchange
 };
 
 /* Columns wx .. wx+31 (lane = column; columns past nx only feed the
- * shuffles), output rows y0 .. y1-1.  The whole warp must call it. */
-template <bool TMAP, class R>
+ * shuffles), output rows y0 .. y1-1, the loads of P rows in flight
+ * together.  The whole warp must call it. */
+template <bool TMAP, class R, int P = SW_P>
 __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
                                                    float *__restrict__ b,
                                                    int nx,
@@ -62,7 +65,7 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
   /* lanes 0 and 31 also load the column west / east of the warp */
   const int  hx = lane == 0 ? max(wx - 1, 0) : (lane == 31 ? min(wx + 32, nx - 1) : gxc);
 
-  float vc[SW_P + 2], vl[SW_P + 2], vr[SW_P + 2];
+  float vc[P + 2], vl[P + 2], vr[P + 2];
   {
     const float *r0 = a + (size_t)max(y0 - 1, 0) * nx, *r1 = a + (size_t)y0 * nx;
     vc[0] = __ldg(r0 + gxc);
@@ -77,11 +80,11 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
       vl[q] = lane == 0 ? vl[q] : up;
     }
   }
-  for (int j0 = y0; j0 < y1; j0 += SW_P)
+  for (int j0 = y0; j0 < y1; j0 += P)
   {
-    float tl[SW_P], bd[SW_P];
+    float tl[P], bd[P];
 #pragma unroll
-    for (int q = 0; q < SW_P; q++)
+    for (int q = 0; q < P; q++)
     {
       const float *r = a + (size_t)min(j0 + 1 + q, ny - 1) * nx;
       vc[q + 2] = __ldg(r + gxc);
@@ -91,14 +94,14 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
       bd[q] = R::EXTRA ? __ldg(bedrock + o) : 0.f;
     }
 #pragma unroll
-    for (int q = 2; q < SW_P + 2; q++)
+    for (int q = 2; q < P + 2; q++)
     {
       const float up = __shfl_up_sync(0xffffffffu, vc[q], 1), dn = __shfl_down_sync(0xffffffffu, vc[q], 1);
       vr[q] = lane == 31 ? vl[q] : dn;
       vl[q] = lane == 0 ? vl[q] : up;
     }
 #pragma unroll
-    for (int q = 0; q < SW_P; q++)
+    for (int q = 0; q < P; q++)
     {
       const int j = j0 + q;
       if (!live || j >= y1) continue;
@@ -113,12 +116,12 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
                       bd[q], first != 0, param);
       b[(size_t)j * nx + gx] = out;
     }
-    vc[0] = vc[SW_P];
-    vl[0] = vl[SW_P];
-    vr[0] = vr[SW_P];
-    vc[1] = vc[SW_P + 1];
-    vl[1] = vl[SW_P + 1];
-    vr[1] = vr[SW_P + 1];
+    vc[0] = vc[P];
+    vl[0] = vl[P];
+    vr[0] = vr[P];
+    vc[1] = vc[P + 1];
+    vl[1] = vl[P + 1];
+    vr[1] = vr[P + 1];
   }
 }
 
@@ -130,7 +133,7 @@ __device__ __forceinline__ void thermal_sweep_warp(const float *__restrict__ a,
  * grids; identical bits to thermal_sweep_warp. */
 constexpr int S2_P = 4; /* rows whose loads are issued together */
 
-template <bool TMAP, class R>
+template <bool TMAP, class R, int P = S2_P>
 __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
                                                     float *__restrict__ b,
                                                     int nx,
@@ -152,7 +155,7 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
   const int  hx = lane == 0 ? max(wx - 1, 0) : (lane == 31 ? min(wx + 64, nx - 1) : gxc);
 
   /* per row: the pair (x, y), the west neighbour of x and the east one of y */
-  float vx[S2_P + 2], vy[S2_P + 2], vw[S2_P + 2], ve[S2_P + 2];
+  float vx[P + 2], vy[P + 2], vw[P + 2], ve[P + 2];
   const bool halo_lane = lane == 0 || lane == 31;
   auto load = [&](int r, int q) {
     const float *row = a + (size_t)r * nx;
@@ -171,11 +174,11 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
   load(y0, 1);
   exchange(0);
   exchange(1);
-  for (int j0 = y0; j0 < y1; j0 += S2_P)
+  for (int j0 = y0; j0 < y1; j0 += P)
   {
-    float2 tl[S2_P], bd[S2_P];
+    float2 tl[P], bd[P];
 #pragma unroll
-    for (int q = 0; q < S2_P; q++)
+    for (int q = 0; q < P; q++)
     {
       load(min(j0 + 1 + q, ny - 1), q + 2);
       const size_t o = (size_t)min(j0 + q, ny - 1) * nx + gxc;
@@ -183,13 +186,13 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
       bd[q] = R::EXTRA ? __ldg(reinterpret_cast<const float2 *>(bedrock + o)) : make_float2(0.f, 0.f);
     }
 #pragma unroll
-    for (int q = 2; q < S2_P + 2; q++) exchange(q);
+    for (int q = 2; q < P + 2; q++) exchange(q);
     /* a warp whose columns and rows are all interior: no border tests
      * (10 % of the step at 4096^2) */
-    if (wx > 0 && wx + 64 < nx && j0 > 0 && j0 + S2_P < ny - 1 && j0 + S2_P <= y1)
+    if (wx > 0 && wx + 64 < nx && j0 > 0 && j0 + P < ny - 1 && j0 + P <= y1)
     {
 #pragma unroll
-      for (int q = 0; q < S2_P; q++)
+      for (int q = 0; q < P; q++)
       {
         float2 out;
         out.x = R::cell(vx[q + 1], vw[q + 1], vx[q + 2], vx[q], vy[q + 1], vw[q], vw[q + 2], vy[q], vy[q + 2],
@@ -202,7 +205,7 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
     else
     {
 #pragma unroll
-      for (int q = 0; q < S2_P; q++)
+      for (int q = 0; q < P; q++)
       {
         const int j = j0 + q;
         if (!live || j >= y1) continue;
@@ -223,14 +226,14 @@ __device__ __forceinline__ void thermal_sweep2_warp(const float *__restrict__ a,
         *reinterpret_cast<float2 *>(b + (size_t)j * nx + gx) = out;
       }
     }
-    vx[0] = vx[S2_P];
-    vy[0] = vy[S2_P];
-    vw[0] = vw[S2_P];
-    ve[0] = ve[S2_P];
-    vx[1] = vx[S2_P + 1];
-    vy[1] = vy[S2_P + 1];
-    vw[1] = vw[S2_P + 1];
-    ve[1] = ve[S2_P + 1];
+    vx[0] = vx[P];
+    vy[0] = vy[P];
+    vw[0] = vw[P];
+    ve[0] = ve[P];
+    vx[1] = vx[P + 1];
+    vy[1] = vy[P + 1];
+    vw[1] = vw[P + 1];
+    ve[1] = ve[P + 1];
   }
 }
 

@@ -94,6 +94,10 @@ __device__ __forceinline__ unsigned long long global_ns()
  * has, false after HM_TMA_WAIT_NS or HM_TMA_SPIN_LIMIT polls */
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
 {
+  /* first poll (suspended up to the hint): the phase has usually completed
+   * by its end, and the clock is not read */
+  if (HM_TMA_SUSPEND_NS ? mbar_try_wait_suspend(bar, parity, HM_TMA_SUSPEND_NS) : mbar_try_wait(bar, parity))
+    return true;
   const unsigned long long t0 = global_ns();
   for (unsigned i = 0; i < HM_TMA_SPIN_LIMIT; i++)
   {

@@ -108,6 +108,7 @@ struct FweSmem
     AdvStage adv;
   };
   uint64_t bar;
+  uint64_t bar2; /* k_vp_step_tma: the second group of boxes */
 };
 static_assert(sizeof(AdvStage) <= sizeof(float) * 4 * FT_H1 * FW, "advect-in staging fits the new-flux arrays");
 
@@ -144,8 +145,14 @@ struct AdvMaps
 
 /* bytes the seven TMA boxes deliver */
 constexpr unsigned FWE_TMA_BYTES = 4u * 40u * (2u * FT_H2 + 5u * FT_H1);
-/* bytes the nine boxes of k_vp_step_tma deliver */
+/* bytes the nine boxes of k_vp_step_tma deliver: group A (the previous
+ * step's u, v and s1, and the stored depth), on which the advection and
+ * the depth pass run while group B (z and the four old fluxes) is still
+ * arriving */
 constexpr unsigned STEP_TMA_BYTES = 4u * 40u * (2u * FT_H2 + 6u * FT_H1 + FS_H);
+constexpr unsigned STEP_TMA_BYTES_A = 4u * 40u * (FT_H2 + 2u * FT_H1 + FS_H);
+constexpr unsigned STEP_TMA_BYTES_B = 4u * 40u * (FT_H2 + 4u * FT_H1);
+static_assert(STEP_TMA_BYTES_A + STEP_TMA_BYTES_B == STEP_TMA_BYTES, "the two groups are the nine boxes");
 
 /* cp.async staging: z, d on the halo-2 region; s and old fluxes on the
  * halo-1 region; loads clamped to the grid, so every raw neighbour read is
@@ -288,37 +295,57 @@ __device__ __forceinline__ bool fwe_stage_tma(const FweMaps &maps, int nx, int n
   return true;
 }
 
-/* TMA staging of k_vp_step_tma: z and d (region 2), the old fluxes
- * (region 1), the previous step's u and v (region 1) and s1 (rows y0-4 ..
- * y0+19), then the clamp-to-edge rebuild of z, d and the fluxes on edge
- * tiles.  The sediment needs none: it is advected at clamped cells, and u,
- * v and s1 are only read at in-grid cells.  Returns false, uniformly across
- * the CTA, if the loads did not complete in time. */
-__device__ __forceinline__ bool fwe_stage_tma_step(const FweMaps &maps, const AdvMaps &am, int nx, int ny, int x0,
-                                                   int y0, FweSmem &sm, unsigned extra_tx)
+/* TMA staging of k_vp_step_tma in two groups on two barriers.  Group A:
+ * the previous step's u and v (region 1), its s1 (rows y0-4 .. y0+19) and
+ * the stored depth d (region 2), waited for here.  Group B: z (region 2)
+ * and the old fluxes (region 1), waited for by fwe_wait_tma_step_b after
+ * the advection and the depth pass have run on group A, so those overlap
+ * its arrival.  Returns false, uniformly across the CTA, if group A did
+ * not complete in time; group B's loads are then given their own windows
+ * to land before the CTA leaves. */
+__device__ __forceinline__ bool fwe_stage_tma_step(const FweMaps &maps, const AdvMaps &am, int x0, int y0,
+                                                   FweSmem &sm, unsigned extra_tx)
 {
   const int tid = threadIdx.x;
   if (tid == 0)
   {
     mbar_init(&sm.bar, 1);
+    mbar_init(&sm.bar2, 1);
     mbar_fence_init();
   }
   __syncthreads();
   if (tid == 0)
   {
-    mbar_arrive_expect_tx(&sm.bar, STEP_TMA_BYTES + extra_tx);
-    tma_load_2d(&sm.z[0][0], &maps.z, x0 - 4, y0 - 2, &sm.bar);
-    tma_load_2d(&sm.d[0][0], &maps.d, x0 - 4, y0 - 2, &sm.bar);
-    tma_load_2d(&sm.fo[0][0][0], &maps.fl, x0 - 4, y0 - 1, &sm.bar);
-    tma_load_2d(&sm.fo[1][0][0], &maps.fr, x0 - 4, y0 - 1, &sm.bar);
-    tma_load_2d(&sm.fo[2][0][0], &maps.ft, x0 - 4, y0 - 1, &sm.bar);
-    tma_load_2d(&sm.fo[3][0][0], &maps.fb, x0 - 4, y0 - 1, &sm.bar);
+    mbar_arrive_expect_tx(&sm.bar, STEP_TMA_BYTES_A + extra_tx);
     tma_load_2d(&sm.adv.u[0][0], &am.u, x0 - 4, y0 - 1, &sm.bar);
     tma_load_2d(&sm.adv.v[0][0], &am.v, x0 - 4, y0 - 1, &sm.bar);
     tma_load_2d(&sm.adv.s1[0][0], &am.s1, x0 - 4, y0 - 4, &sm.bar);
+    tma_load_2d(&sm.d[0][0], &maps.d, x0 - 4, y0 - 2, &sm.bar);
+    mbar_arrive_expect_tx(&sm.bar2, STEP_TMA_BYTES_B);
+    tma_load_2d(&sm.z[0][0], &maps.z, x0 - 4, y0 - 2, &sm.bar2);
+    tma_load_2d(&sm.fo[0][0][0], &maps.fl, x0 - 4, y0 - 1, &sm.bar2);
+    tma_load_2d(&sm.fo[1][0][0], &maps.fr, x0 - 4, y0 - 1, &sm.bar2);
+    tma_load_2d(&sm.fo[2][0][0], &maps.ft, x0 - 4, y0 - 1, &sm.bar2);
+    tma_load_2d(&sm.fo[3][0][0], &maps.fb, x0 - 4, y0 - 1, &sm.bar2);
   }
   bool ok = mbar_wait_bounded(&sm.bar, 0);
   if (!ok) ok = mbar_wait_bounded(&sm.bar, 0); /* loads still in flight: give them a second window */
+  if (__syncthreads_and(ok)) return true;
+  if (!mbar_wait_bounded(&sm.bar2, 0)) mbar_wait_bounded(&sm.bar2, 0);
+  return false;
+}
+
+/* Group B of k_vp_step_tma's boxes (bounded wait), then the clamp-to-edge
+ * rebuild of z, d and the old fluxes on edge tiles.  It runs after the
+ * depth pass, so the rebuild copies depths already brought to the start
+ * of the step, which are the depths of the clamped cells.  The sediment
+ * needs no rebuild: it is advected at clamped cells, and u, v and s1 are
+ * only read at in-grid cells.  false, uniformly across the CTA, if the
+ * group did not complete in time. */
+__device__ __forceinline__ bool fwe_wait_tma_step_b(int nx, int ny, int x0, int y0, FweSmem &sm)
+{
+  bool ok = mbar_wait_bounded(&sm.bar2, 0);
+  if (!ok) ok = mbar_wait_bounded(&sm.bar2, 0);
   if (!__syncthreads_and(ok)) return false;
   fwe_fix_edges<false>(nx, ny, x0, y0, sm);
   return true;
@@ -452,10 +479,20 @@ __device__ __forceinline__ void st_pair(float *p, size_t k, float a, float b, bo
  * cell is unchanged.  INNER: the tile and its 2-cell halo lie inside the
  * grid and the outputs take pair stores (fwe_inner_tile), so every edge
  * clamp and store-width test below is known to be the identity / true and
- * drops out; the cells' values are the same either way. */
-template <bool MAINTAIN, int F, bool INNER = false>
+ * drops out; the cells' values are the same either way.  mid() runs
+ * between the depth pass and the flow pass (uniformly across the CTA); if
+ * it returns false the tile computes and stores nothing (a staging
+ * timeout) but still takes part in the volume sum. */
+/* fwe_compute's hook between the depth pass and the flow pass: nothing
+ * to wait for */
+struct NoMid
+{
+  __device__ bool operator()() const { return true; }
+};
+
+template <bool MAINTAIN, int F, bool INNER = false, class Mid = NoMid>
 __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, VpScalars *sc, double *partials,
-                                            int bx, int by, int nbx, int nby, FweSmem &sm)
+                                            int bx, int by, int nbx, int nby, FweSmem &sm, Mid mid = Mid())
 {
   static_assert(FT_TX == 32 && FT_TY == 16 && FT_NT == 256, "one cell pair per thread in the water pass");
   constexpr bool GEN = (F & FWE_GENERIC) != 0;
@@ -499,140 +536,143 @@ __device__ __forceinline__ void fwe_compute(const FweIo &io, const VpConst &c, V
   }
   __syncthreads();
 
-  /* flow pass on region 1 (columns x0-1 .. x0+32 = smem 3 .. 36, rows
-   * y0-1 .. y0+16): items 0 .. 287 are the 16 pairs (smem 4 .. 35) of each
-   * of the 18 rows, items 288 .. 323 the two ring columns 3 and 36 */
-  auto flow1 = [&](float zc, float dc, float zw, float dw, float ze, float de, float zs, float ds, float zn,
-                   float dn, float &fl, float &fr, float &ft, float &fb) {
-    if (diffusion)
-    {
-      if (pl_one) flow_cell<true, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
-      else flow_cell<true, false>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
-    }
-    else
-    {
-      if (pl_one) flow_cell<false, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
-      else flow_cell<false, false>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
-    }
-  };
-  for (int e = tid; e < 16 * FT_H1 + 2 * FT_H1; e += FT_NT)
+  double part = 0.0;
+  if (mid())
   {
-    if (e < 16 * FT_H1)
-    {
-      const int    l = e >> 4, cc = 4 + 2 * (e & 15), q = l + 1;
-      const float2 zc = lds2(&sm.z[q][cc]), dc = lds2(&sm.d[q][cc]);
-      const float2 zn = lds2(&sm.z[q - 1][cc]), dn = lds2(&sm.d[q - 1][cc]);
-      const float2 zs = lds2(&sm.z[q + 1][cc]), ds = lds2(&sm.d[q + 1][cc]);
-      const float  zw = sm.z[q][cc - 1], dw = sm.d[q][cc - 1], ze = sm.z[q][cc + 2], de = sm.d[q][cc + 2];
-      float2       fl = lds2(&sm.fo[0][l][cc]), fr = lds2(&sm.fo[1][l][cc]), ft = lds2(&sm.fo[2][l][cc]),
-             fb = lds2(&sm.fo[3][l][cc]);
-      flow1(zc.x, dc.x, zw, dw, zc.y, dc.y, zs.x, ds.x, zn.x, dn.x, fl.x, fr.x, ft.x, fb.x);
-      flow1(zc.y, dc.y, zc.x, dc.x, ze, de, zs.y, ds.y, zn.y, dn.y, fl.y, fr.y, ft.y, fb.y);
-      sts2(&sm.fn[0][l][cc], fl.x, fl.y);
-      sts2(&sm.fn[1][l][cc], fr.x, fr.y);
-      sts2(&sm.fn[2][l][cc], ft.x, ft.y);
-      sts2(&sm.fn[3][l][cc], fb.x, fb.y);
-    }
-    else
-    {
-      const int r = e - 16 * FT_H1, l = r >> 1, cc = (r & 1) ? 36 : 3, q = l + 1;
-      float     fl = sm.fo[0][l][cc], fr = sm.fo[1][l][cc], ft = sm.fo[2][l][cc], fb = sm.fo[3][l][cc];
-      flow1(sm.z[q][cc], sm.d[q][cc], sm.z[q][cc - 1], sm.d[q][cc - 1], sm.z[q][cc + 1], sm.d[q][cc + 1],
-            sm.z[q + 1][cc], sm.d[q + 1][cc], sm.z[q - 1][cc], sm.d[q - 1][cc], fl, fr, ft, fb);
-      sm.fn[0][l][cc] = fl;
-      sm.fn[1][l][cc] = fr;
-      sm.fn[2][l][cc] = ft;
-      sm.fn[3][l][cc] = fb;
-    }
-  }
-  __syncthreads();
-
-  /* water and erosion on the tile: thread t takes row t / 16 and the pair
-   * of tile columns 2 (t % 16), 2 (t % 16) + 1 */
-  double    part = 0.0;
-  const int ty = tid >> 4, pk = tid & 15;
-  const int gy = y0 + ty, gx = x0 + 2 * pk;
-  const int cc = 4 + 2 * pk; /* smem column of the first cell */
-  if (INNER || (gx < nx && gy < ny))
-  {
-    const bool second = INNER || gx + 1 < nx;
-    const int  l = ty + 1, q = ty + 2;
-    /* flux neighbours: rows and columns clamped to the grid (new fluxes are
-     * derived: outside the grid they are the edge cell's own values) */
-    const int  ln = INNER ? ty : clampi(gy - 1, 0, ny - 1) - (y0 - 1);
-    const int  ls = INNER ? ty + 2 : clampi(gy + 1, 0, ny - 1) - (y0 - 1);
-    const int  cw0 = INNER || gx > 0 ? cc - 1 : cc;          /* west of the first cell  */
-    const int  ce0 = second ? cc + 1 : cc;                   /* east of the first cell  */
-    const int  ce1 = INNER || gx + 2 < nx ? cc + 2 : cc + 1; /* east of the second cell */
-    const float2 flc = lds2(&sm.fn[0][l][cc]), frc = lds2(&sm.fn[1][l][cc]), ftc = lds2(&sm.fn[2][l][cc]),
-                 fbc = lds2(&sm.fn[3][l][cc]);
-    const float2 ftn = lds2(&sm.fn[2][ln][cc]), fbs = lds2(&sm.fn[3][ls][cc]);
-    const float  frw0 = sm.fn[1][l][cw0], fle0 = sm.fn[0][l][ce0], fle1 = sm.fn[0][l][ce1];
-    const float2 d1 = lds2(&sm.d[q][cc]);
-    float        d2a, ua, va, d2b, ub, vb;
-    if (pl_one)
-    {
-      water_cell<true>(c, d1.x, flc.x, frc.x, ftc.x, fbc.x, frw0, fle0, ftn.x, fbs.x, d2a, ua, va);
-      water_cell<true>(c, d1.y, flc.y, frc.y, ftc.y, fbc.y, frc.x, fle1, ftn.y, fbs.y, d2b, ub, vb);
-    }
-    else
-    {
-      water_cell<false>(c, d1.x, flc.x, frc.x, ftc.x, fbc.x, frw0, fle0, ftn.x, fbs.x, d2a, ua, va);
-      water_cell<false>(c, d1.y, flc.y, frc.y, ftc.y, fbc.y, frc.x, fle1, ftn.y, fbs.y, d2b, ub, vb);
-    }
-    const size_t k = (size_t)gy * nx + gx;
-    const bool   vec = INNER || io.vec != 0;
-    if (FLOW_ONLY)
-    {
-      /* flow_simulation: the depth after the water pass is the next step's
-       * depth as it is (no evaporation, no erosion; the terrain is fixed) */
-      st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
-      st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
-      st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
-      st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
-      st_pair(io.out.d, k, d2a, d2b, second, vec);
-      (void)ua, (void)ub, (void)va, (void)vb;
-    }
-    else
-    {
-      const float dea = fmul(d2a, c.keep), deb = fmul(d2b, c.keep);
-      /* what the water pass produced, stored before the erosion arithmetic
-       * so its registers are free there (the stores go through generic
-       * pointers, so the compiler keeps them after the shared-memory loads
-       * that follow them in the source: their order decides what stays
-       * live; 48 registers without spills, 2.5 % faster than storing after
-       * erosion) */
-      st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
-      st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
-      st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
-      st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
-      st_pair(io.out.d, k, dea, deb, second, vec);
-      st_pair(io.u, k, ua, ub, second, vec);
-      st_pair(io.v, k, va, vb, second, vec);
-      if (io.u_out)
+    /* flow pass on region 1 (columns x0-1 .. x0+32 = smem 3 .. 36, rows
+     * y0-1 .. y0+16): items 0 .. 287 are the 16 pairs (smem 4 .. 35) of each
+     * of the 18 rows, items 288 .. 323 the two ring columns 3 and 36 */
+    auto flow1 = [&](float zc, float dc, float zw, float dw, float ze, float de, float zs, float ds, float zn,
+                     float dn, float &fl, float &fr, float &ft, float &fb) {
+      if (diffusion)
       {
-        st_pair(io.u_out, k, ua, ub, second, vec);
-        st_pair(io.v_out, k, va, vb, second, vec);
-      }
-      const float2 zc = lds2(&sm.z[q][cc]), zn = lds2(&sm.z[q - 1][cc]), zs = lds2(&sm.z[q + 1][cc]);
-      const float  zw = sm.z[q][cc - 1], ze = sm.z[q][cc + 2];
-      const float2 s0 = lds2(&sm.s[l][cc]), sn = lds2(&sm.s[l - 1][cc]), ss = lds2(&sm.s[l + 1][cc]);
-      const float  sw = sm.s[l][cc - 1], se = sm.s[l][cc + 2];
-      float        zoa, soa, zob, sob;
-      if (kexp_one)
-      {
-        erosion_cell<true>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
-        erosion_cell<true>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+        if (pl_one) flow_cell<true, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
+        else flow_cell<true, false>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
       }
       else
       {
-        erosion_cell<false>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
-        erosion_cell<false>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+        if (pl_one) flow_cell<false, true>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
+        else flow_cell<false, false>(c, zc, dc, zw, dw, ze, de, zs, ds, zn, dn, fl, fr, ft, fb);
       }
-      st_pair(io.out.z, k, zoa, zob, second, vec);
-      st_pair(io.s1, k, soa, sob, second, vec);
-      part = (double)dea;
-      if (second) part += (double)deb;
+    };
+    for (int e = tid; e < 16 * FT_H1 + 2 * FT_H1; e += FT_NT)
+    {
+      if (e < 16 * FT_H1)
+      {
+        const int    l = e >> 4, cc = 4 + 2 * (e & 15), q = l + 1;
+        const float2 zc = lds2(&sm.z[q][cc]), dc = lds2(&sm.d[q][cc]);
+        const float2 zn = lds2(&sm.z[q - 1][cc]), dn = lds2(&sm.d[q - 1][cc]);
+        const float2 zs = lds2(&sm.z[q + 1][cc]), ds = lds2(&sm.d[q + 1][cc]);
+        const float  zw = sm.z[q][cc - 1], dw = sm.d[q][cc - 1], ze = sm.z[q][cc + 2], de = sm.d[q][cc + 2];
+        float2       fl = lds2(&sm.fo[0][l][cc]), fr = lds2(&sm.fo[1][l][cc]), ft = lds2(&sm.fo[2][l][cc]),
+               fb = lds2(&sm.fo[3][l][cc]);
+        flow1(zc.x, dc.x, zw, dw, zc.y, dc.y, zs.x, ds.x, zn.x, dn.x, fl.x, fr.x, ft.x, fb.x);
+        flow1(zc.y, dc.y, zc.x, dc.x, ze, de, zs.y, ds.y, zn.y, dn.y, fl.y, fr.y, ft.y, fb.y);
+        sts2(&sm.fn[0][l][cc], fl.x, fl.y);
+        sts2(&sm.fn[1][l][cc], fr.x, fr.y);
+        sts2(&sm.fn[2][l][cc], ft.x, ft.y);
+        sts2(&sm.fn[3][l][cc], fb.x, fb.y);
+      }
+      else
+      {
+        const int r = e - 16 * FT_H1, l = r >> 1, cc = (r & 1) ? 36 : 3, q = l + 1;
+        float     fl = sm.fo[0][l][cc], fr = sm.fo[1][l][cc], ft = sm.fo[2][l][cc], fb = sm.fo[3][l][cc];
+        flow1(sm.z[q][cc], sm.d[q][cc], sm.z[q][cc - 1], sm.d[q][cc - 1], sm.z[q][cc + 1], sm.d[q][cc + 1],
+              sm.z[q + 1][cc], sm.d[q + 1][cc], sm.z[q - 1][cc], sm.d[q - 1][cc], fl, fr, ft, fb);
+        sm.fn[0][l][cc] = fl;
+        sm.fn[1][l][cc] = fr;
+        sm.fn[2][l][cc] = ft;
+        sm.fn[3][l][cc] = fb;
+      }
+    }
+    __syncthreads();
+
+    /* water and erosion on the tile: thread t takes row t / 16 and the pair
+     * of tile columns 2 (t % 16), 2 (t % 16) + 1 */
+    const int ty = tid >> 4, pk = tid & 15;
+    const int gy = y0 + ty, gx = x0 + 2 * pk;
+    const int cc = 4 + 2 * pk; /* smem column of the first cell */
+    if (INNER || (gx < nx && gy < ny))
+    {
+      const bool second = INNER || gx + 1 < nx;
+      const int  l = ty + 1, q = ty + 2;
+      /* flux neighbours: rows and columns clamped to the grid (new fluxes are
+       * derived: outside the grid they are the edge cell's own values) */
+      const int  ln = INNER ? ty : clampi(gy - 1, 0, ny - 1) - (y0 - 1);
+      const int  ls = INNER ? ty + 2 : clampi(gy + 1, 0, ny - 1) - (y0 - 1);
+      const int  cw0 = INNER || gx > 0 ? cc - 1 : cc;          /* west of the first cell  */
+      const int  ce0 = second ? cc + 1 : cc;                   /* east of the first cell  */
+      const int  ce1 = INNER || gx + 2 < nx ? cc + 2 : cc + 1; /* east of the second cell */
+      const float2 flc = lds2(&sm.fn[0][l][cc]), frc = lds2(&sm.fn[1][l][cc]), ftc = lds2(&sm.fn[2][l][cc]),
+                   fbc = lds2(&sm.fn[3][l][cc]);
+      const float2 ftn = lds2(&sm.fn[2][ln][cc]), fbs = lds2(&sm.fn[3][ls][cc]);
+      const float  frw0 = sm.fn[1][l][cw0], fle0 = sm.fn[0][l][ce0], fle1 = sm.fn[0][l][ce1];
+      const float2 d1 = lds2(&sm.d[q][cc]);
+      float        d2a, ua, va, d2b, ub, vb;
+      if (pl_one)
+      {
+        water_cell<true>(c, d1.x, flc.x, frc.x, ftc.x, fbc.x, frw0, fle0, ftn.x, fbs.x, d2a, ua, va);
+        water_cell<true>(c, d1.y, flc.y, frc.y, ftc.y, fbc.y, frc.x, fle1, ftn.y, fbs.y, d2b, ub, vb);
+      }
+      else
+      {
+        water_cell<false>(c, d1.x, flc.x, frc.x, ftc.x, fbc.x, frw0, fle0, ftn.x, fbs.x, d2a, ua, va);
+        water_cell<false>(c, d1.y, flc.y, frc.y, ftc.y, fbc.y, frc.x, fle1, ftn.y, fbs.y, d2b, ub, vb);
+      }
+      const size_t k = (size_t)gy * nx + gx;
+      const bool   vec = INNER || io.vec != 0;
+      if (FLOW_ONLY)
+      {
+        /* flow_simulation: the depth after the water pass is the next step's
+         * depth as it is (no evaporation, no erosion; the terrain is fixed) */
+        st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
+        st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
+        st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
+        st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
+        st_pair(io.out.d, k, d2a, d2b, second, vec);
+        (void)ua, (void)ub, (void)va, (void)vb;
+      }
+      else
+      {
+        const float dea = fmul(d2a, c.keep), deb = fmul(d2b, c.keep);
+        /* what the water pass produced, stored before the erosion arithmetic
+         * so its registers are free there (the stores go through generic
+         * pointers, so the compiler keeps them after the shared-memory loads
+         * that follow them in the source: their order decides what stays
+         * live; 48 registers without spills, 2.5 % faster than storing after
+         * erosion) */
+        st_pair(io.out.fl, k, flc.x, flc.y, second, vec);
+        st_pair(io.out.fr, k, frc.x, frc.y, second, vec);
+        st_pair(io.out.ft, k, ftc.x, ftc.y, second, vec);
+        st_pair(io.out.fb, k, fbc.x, fbc.y, second, vec);
+        st_pair(io.out.d, k, dea, deb, second, vec);
+        st_pair(io.u, k, ua, ub, second, vec);
+        st_pair(io.v, k, va, vb, second, vec);
+        if (io.u_out)
+        {
+          st_pair(io.u_out, k, ua, ub, second, vec);
+          st_pair(io.v_out, k, va, vb, second, vec);
+        }
+        const float2 zc = lds2(&sm.z[q][cc]), zn = lds2(&sm.z[q - 1][cc]), zs = lds2(&sm.z[q + 1][cc]);
+        const float  zw = sm.z[q][cc - 1], ze = sm.z[q][cc + 2];
+        const float2 s0 = lds2(&sm.s[l][cc]), sn = lds2(&sm.s[l - 1][cc]), ss = lds2(&sm.s[l + 1][cc]);
+        const float  sw = sm.s[l][cc - 1], se = sm.s[l][cc + 2];
+        float        zoa, soa, zob, sob;
+        if (kexp_one)
+        {
+          erosion_cell<true>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
+          erosion_cell<true>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+        }
+        else
+        {
+          erosion_cell<false>(c, zc.x, s0.x, zw, zc.y, zn.x, zs.x, sw, s0.y, sn.x, ss.x, d2a, ua, va, zoa, soa);
+          erosion_cell<false>(c, zc.y, s0.y, zc.x, ze, zn.y, zs.y, s0.x, se, sn.y, ss.y, d2b, ub, vb, zob, sob);
+        }
+        st_pair(io.out.z, k, zoa, zob, second, vec);
+        st_pair(io.s1, k, soa, sob, second, vec);
+        part = (double)dea;
+        if (second) part += (double)deb;
+      }
     }
   }
 
@@ -719,8 +759,9 @@ __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
   }
 }
 
-/* The same with the nine input boxes fetched by TMA (am holds the maps of
- * the previous step's u, v and s1).  Timeouts as k_vp_fwe_tma. */
+/* The same with the nine input boxes fetched by TMA in two groups (am
+ * holds the maps of the previous step's u, v and s1).  Timeouts as
+ * k_vp_fwe_tma. */
 template <bool MAINTAIN, int F>
 __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
     k_vp_step_tma(FweIo io, const __grid_constant__ FweMaps maps, const __grid_constant__ AdvMaps am, VpConst c,
@@ -728,7 +769,7 @@ __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
 {
   __shared__ FweSmem sm;
   const int x0 = blockIdx.x * FT_TX, y0 = blockIdx.y * FT_TY;
-  if (!fwe_stage_tma_step(maps, am, c.nx, c.ny, x0, y0, sm, io.tma_extra_tx))
+  if (!fwe_stage_tma_step(maps, am, x0, y0, sm, io.tma_extra_tx))
   {
     if (threadIdx.x == 0) atomicOr(&sc->error, 1u);
     if (MAINTAIN)
@@ -741,15 +782,21 @@ __global__ void __launch_bounds__(FT_NT, fwe_min_blocks(F))
     }
     return;
   }
+  /* group B (z, fluxes) arrives during the advection and the depth pass */
+  auto group_b = [&]() {
+    if (fwe_wait_tma_step_b(c.nx, c.ny, x0, y0, sm)) return true;
+    if (threadIdx.x == 0) atomicOr(&sc->error, 1u);
+    return false;
+  };
   if (fwe_inner_tile(io, c.nx, c.ny, x0, y0))
   {
     advect_region1<true>(c, io.s1_prev, x0, y0, sm);
-    fwe_compute<MAINTAIN, F, true>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+    fwe_compute<MAINTAIN, F, true>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm, group_b);
   }
   else
   {
     advect_region1<false>(c, io.s1_prev, x0, y0, sm);
-    fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm);
+    fwe_compute<MAINTAIN, F>(io, c, sc, partials, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, sm, group_b);
   }
 }
 
