@@ -52,6 +52,15 @@ namespace hm
 
 constexpr int BT = FT_NT;  /* threads per CTA (8 warps)                  */
 constexpr int TH_W = 256;  /* thermal tile: a warp per 32 columns        */
+/* Resident CTAs per SM the round kernel is compiled for, and the rows
+ * whose loads a thermal tile's sweep keeps in flight (one column per lane,
+ * column pairs).  The plain sweeps' 8 and 4 rows need 80 registers here,
+ * three CTAs per SM; with 4 and 2 the kernel fits 64 registers (a few
+ * words spill) and four CTAs, whose extra warps hide the latency instead:
+ * 8 % less time for the round graphs of the 206 jobs under 1024^2 cells of
+ * the batched benchmark's mix. */
+constexpr int BATCH_CTAS_PER_SM = 4;
+constexpr int BATCH_TH_ROWS_1 = 4, BATCH_TH_ROWS_2 = 2;
 
 /* device-side description of one job */
 struct BJob
@@ -117,12 +126,14 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
   {
     const int wx = bx * 2 * TH_W + (threadIdx.x >> 5) * 64;
     if (wx < J.nx) /* whole warp */
-      thermal_sweep2_warp<TMAP, TalusExchange<BED>>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
+      thermal_sweep2_warp<TMAP, TalusExchange<BED>, BATCH_TH_ROWS_2>(
+          J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
     return;
   }
   const int wx = bx * TH_W + (threadIdx.x >> 5) * 32;
   if (wx < J.nx) /* whole warp */
-    thermal_sweep_warp<TMAP, TalusExchange<BED>>(J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
+    thermal_sweep_warp<TMAP, TalusExchange<BED>, BATCH_TH_ROWS_1>(
+        J.tz[par], J.tz[par ^ 1], J.nx, J.ny, J.talus, J.tv, J.bed, 0, wx, y0, y1);
 }
 
 /* One round: every active vpipes tile and thermal tile, taken by
@@ -131,12 +142,11 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
  * eroded sediment into the tile (fwe_stage_cp_async_step, advect_region1).
  * F: FWE_RTOPTS when every active vpipes job has pipe length 1 and
  * discharge exponent 1 (the lean form without fp64 pow), else FWE_GENERIC;
- * both at three CTAs per SM (80 registers: a bound of four spills 484
- * bytes per thread and ran 20 % slower).  Thread 0 takes
- * the CTA's next tile index while the current tile is computed, so the
+ * both compiled for BATCH_CTAS_PER_SM CTAs per SM.  Thread 0 takes the
+ * CTA's next tile index while the current tile is computed, so the
  * atomic's latency is hidden. */
 template <int F>
-__global__ void __launch_bounds__(BT, 3)
+__global__ void __launch_bounds__(BT, BATCH_CTAS_PER_SM)
     k_batch_round(const BJob *__restrict__ jobs,
                   const int4 *__restrict__ vt,
                   int nv,

@@ -144,7 +144,7 @@ int autotune_batch(hm_context *ctx, int side_max, int steps, hm_tune_result *res
     jobs.push_back(j);
   }
   std::vector<TuneEntry> cands;
-  for (int per_sm = 1; per_sm <= 3; per_sm++)
+  for (int per_sm = 1; per_sm <= 4; per_sm++)
     for (int rows : {8, 16, 32}) cands.push_back(TuneEntry{per_sm, 0, rows, 0, 0.f});
   int   best = -1;
   float best_ms = 0.f;
@@ -383,7 +383,7 @@ int hm_autotune_load(const char *path, int *loaded_out)
       hm::g_th[{cx, cy}] = e;
       loaded++;
     }
-    else if (k == "batch" && e.tpb >= 1 && e.tpb <= 3 && (e.rows == 8 || e.rows == 16 || e.rows == 32))
+    else if (k == "batch" && e.tpb >= 1 && e.tpb <= 4 && (e.rows == 8 || e.rows == 16 || e.rows == 32))
     {
       std::lock_guard<std::mutex> lk(hm::g_mu);
       hm::g_batch = e;

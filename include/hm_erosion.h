@@ -721,7 +721,7 @@ int       hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_g
  * two); solves that leave the choice to the library (time_block 0, no
  * hm_vpipes_set_launch override) then use it.  Process-wide; do not run
  * while other threads solve.  kind: HM_JOB_THERMAL or HM_JOB_VPIPES, or
- * HM_TUNE_BATCH: the batched form's persistent CTAs per SM (1..3) and
+ * HM_TUNE_BATCH: the batched form's persistent CTAs per SM (1..4) and
  * thermal tile rows (8, 16, 32), timed over `steps` rounds of a synthetic
  * batch of 16 jobs, half thermal and half vpipes, with sides from 128 up to
  * max(nx, ny); batches created afterwards use the fastest (result: tpb =
