@@ -25,7 +25,13 @@ PARAMS = dict(iterations=3, maintain_water_volume=0, flux_diffusion=0, dt=0.1, k
               k_depose=0.01, evap_rate=0.01, gravity=9.81, rain_per_step=1e-4, initial_water=0.0)
 
 
-def test_tma_wait_runs_out_and_reports_timeout(gpu):
+@pytest.mark.parametrize("iterations, maintain", [(1, 0), (2, 0), (2, 1)])
+def test_tma_wait_runs_out_and_reports_timeout(gpu, iterations, maintain):
+    """One iteration runs only the first step's kernel (k_vp_fwe_tma); two
+    add a later step's kernel (k_vp_step_tma, whose boxes arrive in two
+    groups on two barriers).  With the volume top-up a tile that gave up
+    still adds zero to the grid-wide sum, so the step's last tile finishes
+    the sum instead of waiting for it."""
     # 64 x 40: TMA staging applies (nx a multiple of 4, nx >= 40, ny >= 24)
     z0 = fbm(64, 40, seed=12)
     ctx = gpu.Context(0)
@@ -35,7 +41,7 @@ def test_tma_wait_runs_out_and_reports_timeout(gpu):
         z = z0.copy()
         t = time.perf_counter()
         with pytest.raises(L.HMError) as e:
-            gpu.hydraulic_vpipes(z, ctx=ctx, **dict(PARAMS, iterations=1))
+            gpu.hydraulic_vpipes(z, ctx=ctx, **dict(PARAMS, iterations=iterations, maintain_water_volume=maintain))
         elapsed = time.perf_counter() - t
         assert e.value.status == L.HM_ERR_TIMEOUT
         assert "timed out" in str(e.value)
