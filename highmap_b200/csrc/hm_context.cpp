@@ -112,9 +112,10 @@ int hm_init(void)
   }
   cudaDeviceProp prop;
   HM_CUDA_TRY(cudaGetDeviceProperties(&prop, 0));
-  if (prop.major != 10)
-    return hm::fail(HM_ERR_NO_DEVICE, std::string("device 0 is ") + prop.name +
-                                          ", this library is built for sm_100a only");
+  if (prop.major != 10 || prop.minor != 0)
+    return hm::fail(HM_ERR_NO_DEVICE, std::string("device 0 is ") + prop.name + " (compute capability " +
+                                          std::to_string(prop.major) + "." + std::to_string(prop.minor) +
+                                          "), this library is built for sm_100a only");
   HM_CUDA_TRY(cudaFree(nullptr)); /* create the primary context */
   return HM_OK;
 }
@@ -132,6 +133,13 @@ int hm_context_create(hm_context **ctx, int device)
     return hm::fail(HM_ERR_NO_DEVICE, "no CUDA device is visible");
   }
   if (device < 0 || device >= n) return hm::fail(HM_ERR_INVALID_ARGUMENT, "device index out of range");
+  int major = 0, minor = 0;
+  HM_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  HM_CUDA_TRY(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device));
+  if (major != 10 || minor != 0)
+    return hm::fail(HM_ERR_NO_DEVICE, "device " + std::to_string(device) + " has compute capability " +
+                                          std::to_string(major) + "." + std::to_string(minor) +
+                                          ", this library is built for sm_100a only");
   int st = hm::use_device(device);
   if (st) return st;
   hm_context *c = new (std::nothrow) hm_context();

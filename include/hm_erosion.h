@@ -23,7 +23,10 @@
  * output buffers are left unmodified where the failure is detected before
  * any device work (argument checks), and hm_last_error() describes it.
  * Contexts are not shared between threads; one context serialises its own
- * calls on its stream.
+ * calls on its stream.  The device-pointer calls (hm_*_device) run on the
+ * caller's stream but use their context's workspace, so two of them on one
+ * context must be ordered (the same stream, or an event between streams);
+ * a context per stream lets them overlap.
  */
 #ifndef HM_EROSION_H
 #define HM_EROSION_H
@@ -51,8 +54,9 @@ typedef struct hm_context hm_context;
 
 /* Replaces hmap::gpu::init_opencl() (HighMap/include/highmap/opencl/
  * gpu_opencl.hpp:166, HighMap/src/gpu_opencl/gpu_opencl.cpp:32-134):
- * returns HM_OK when a CUDA device of compute capability 10.x is ready and
- * the kernels of this library can run on it. */
+ * returns HM_OK when device 0 is of compute capability 10.0 (the library
+ * holds sm_100a code only, which runs on no other capability) and a
+ * context can be made on it. */
 int hm_init(void);
 
 /* Context: a CUDA stream for the host-pointer calls and a grow-only device
