@@ -8,9 +8,10 @@
  * B200 on their own, so here every admitted job's grid is cut into tiles
  * and the tiles of all jobs form packed lists:
  *   vpipes tiles  : 32 x 16 tiles of a step (hm_vpipes_tiled.cuh,
- *                   cp.async staging): the first step's flow / water /
- *                   erosion, and for every later step the previous step's
- *                   advection folded into the same tile;
+ *                   cp.async staging, in 16-byte copies where the tile's
+ *                   boxes lie inside an aligned grid): the first step's
+ *                   flow / water / erosion, and for every later step the
+ *                   previous step's advection folded into the same tile;
  *   thermal tiles : th_rows rows of 512 columns, a warp per 64 (column
  *                   pairs, for even rows on aligned grids) or of 256
  *                   columns, a warp per 32 (hm_thermal_sweep.cuh).
@@ -84,6 +85,7 @@ struct BJob
   VpConst      c;
   int          maintain, diffusion, pl_one, kexp_one;
   int          vec; /* pair stores (even nx, 8-byte aligned outputs) */
+  int          stage16; /* 16-byte staging copies (nx % 4 == 0, 16-byte aligned grids) */
   const float *rain;
   float       *u_out, *v_out;
   VpScalars   *sc;
@@ -115,6 +117,7 @@ __device__ __forceinline__ void job_io(const BJob &J, int step, FweIo &io)
   if (io.u_out && !io.v_out) io.v_out = io.v;
   if (io.v_out && !io.u_out) io.u_out = io.u;
   io.vec = J.vec;
+  io.stage16 = J.stage16;
   io.flow_only = 0;
 }
 
@@ -189,6 +192,8 @@ __global__ void __launch_bounds__(BT, BATCH_CTAS_PER_SM)
       const int   step = s_step;
       if (step == 0)
         fwe_stage_cp_async(s_io, J.nx, J.ny, x0, y0, sm);
+      else if (stage16_tile(s_io, J.nx, J.ny, x0, y0))
+        fwe_stage_cp_async16_step(s_io, J.u[(step & 1) ^ 1], J.v[(step & 1) ^ 1], J.nx, x0, y0, sm);
       else
         fwe_stage_cp_async_step(s_io, J.u[(step & 1) ^ 1], J.v[(step & 1) ^ 1], J.nx, J.ny, x0, y0, sm);
       __syncthreads();
@@ -243,6 +248,21 @@ struct HJob
   float    *z0 = nullptr;     /* thermal input copy for the deposition map */
 };
 
+/* a vpipes job's grids allow 16-byte staging copies (rows a multiple of 4
+ * floats, every staged grid 16-byte aligned) */
+int stage16_ok(const hm::BJob &d)
+{
+  auto al16 = [](const void *q) { return ((uintptr_t)q & 15u) == 0; };
+  if (d.nx % 4 != 0) return 0;
+  for (const hm::VpFields &f : d.cp)
+    for (const void *q : {(const void *)f.z, (const void *)f.d, (const void *)f.fl, (const void *)f.fr,
+                          (const void *)f.ft, (const void *)f.fb})
+      if (!al16(q)) return 0;
+  for (int k = 0; k < 2; k++)
+    if (!al16(d.s1[k]) || !al16(d.u[k]) || !al16(d.v[k])) return 0;
+  return 1;
+}
+
 /* the pointer p moved with its block from old_base to new_base, if it
  * points into the bytes-long block */
 template <class T>
@@ -278,6 +298,7 @@ void rebase_job(HJob &h, uintptr_t old_base, char *new_base)
   rebase(d.partials, old_base, n, new_base);
   rebase(d.sc, old_base, n, new_base);
   rebase(h.z0, old_base, n, new_base);
+  if (h.desc.kind == HM_JOB_VPIPES) d.stage16 = stage16_ok(d);
 }
 
 size_t job_bytes(const hm_job &j)
@@ -701,6 +722,7 @@ int hm_batch_add(hm_batch *b, const hm_job *job, int *job_id)
     d.v[1] = base + 18 * na;
     d.vec = job->nx % 2 == 0 && ((uintptr_t)job->z & 7u) == 0 && ((uintptr_t)job->vel_u & 7u) == 0 &&
             ((uintptr_t)job->vel_v & 7u) == 0;
+    d.stage16 = stage16_ok(d);
     d.partials = (double *)(base + 19 * na);
     const size_t tiles = (size_t)d.nbx * d.nby;
     const size_t parts = std::max(tiles, hm::vpipes_init_partials());

@@ -384,6 +384,14 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
     bool        ok = nx % 2 == 0;
     for (const void *q : outs) ok = ok && al8(q);
     io.vec = ok ? 1 : 0;
+    /* 16-byte staging copies: a row length that is a multiple of 4 and
+     * 16-byte aligned inputs */
+    auto al16 = [](const void *q) { return ((uintptr_t)q & 15u) == 0; };
+    const void *ins[] = {A.z, A.d, A.fl, A.fr, A.ft, A.fb, B.z,      B.d,      B.fl,     B.fr,
+                         B.ft, B.fb, s1_buf[0], s1_buf[1], u_buf[0], u_buf[1], v_buf[0], v_buf[1]};
+    bool        ok16 = nx % 4 == 0;
+    for (const void *q : ins) ok16 = ok16 && al16(q);
+    io.stage16 = ok16 ? 1 : 0;
   }
   const dim3 g1((nx + FT_TX - 1) / FT_TX, (ny + FT_TY - 1) / FT_TY);
   const int  row_groups = (ny + ADV_R - 1) / ADV_R;
