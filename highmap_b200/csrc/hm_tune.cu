@@ -5,7 +5,9 @@
  * synthetic terrain of that size (generated on the device: a sum of
  * sinusoids with the value range of a remapped fBm field) and keeps the
  * fastest per size class (nx and ny rounded up to powers of two):
- *   vpipes  : threads per CTA (strip width) x staged advection radius x
+ *   vpipes  : the tiled step kernels at one or two steps per launch
+ *             (temporal-block depth 1, 2), and the streaming kernel's
+ *             threads per CTA (strip width) x staged advection radius x
  *             output rows per CTA (the occupancy / halo / warm-up trade);
  *   thermal : steps per launch (temporal-block depth 1, 2, 4, 8) x rows
  *             per CTA of the blocked kernel;
@@ -245,6 +247,8 @@ int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_re
     const int shapes[][3] = {{0, 0, 0},     {128, 2, 32}, {128, 2, 64}, {128, 2, 128},
                              {256, 2, 64},  {128, 3, 32}, {128, 3, 64}, {256, 3, 64}};
     for (auto &c : shapes) cands.push_back(hm::TuneEntry{c[0], c[1], c[2], 0, 0.f});
+    /* the tiled kernels with two steps per launch (time_block 2) */
+    cands.push_back(hm::TuneEntry{0, 0, 0, 2, 0.f});
   }
   else
   {
@@ -279,7 +283,7 @@ int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_re
       HM_CUDA_TRY(cudaEventRecord(e0, s));
       if (kind == HM_JOB_VPIPES)
       {
-        if (c.tpb == 0) st = hm_vpipes_set_algorithm(HM_VPIPES_TILED);
+        if (c.tpb == 0) st = hm_vpipes_set_algorithm(c.block == 2 ? HM_VPIPES_TILED_TB2 : HM_VPIPES_TILED);
         else if (!(st = hm_vpipes_set_algorithm(HM_VPIPES_STREAMING))) st = hm_vpipes_set_launch(c.tpb, c.radius, c.rows);
         if (st) break;
         st = hm_vpipes_device(ctx, z, nx, ny, &vp, nullptr, nullptr, nullptr, nullptr, nullptr, s);
@@ -371,7 +375,8 @@ int hm_autotune_load(const char *path, int *loaded_out)
       continue;
     std::string k(kind);
     /* keep only shapes the kernels accept */
-    if (k == "vpipes" && (e.tpb == 0 || hm_vpipes_set_launch(e.tpb, e.radius, e.rows) == HM_OK))
+    if (k == "vpipes" && ((e.tpb == 0 && e.block >= 0 && e.block <= 2) ||
+                          (e.tpb != 0 && hm_vpipes_set_launch(e.tpb, e.radius, e.rows) == HM_OK)))
     {
       std::lock_guard<std::mutex> lk(hm::g_mu);
       hm::g_vp[{cx, cy}] = e;

@@ -172,7 +172,7 @@ int vpipes_pick_algo(int nx, int ny)
   if (g_algo_override >= 0) return g_algo_override;
   if (g_cfg_override.tpb) return 1;
   TuneEntry e;
-  if (tuned_vpipes(nx, ny, &e)) return e.tpb ? 1 : 0;
+  if (tuned_vpipes(nx, ny, &e)) return e.tpb ? 1 : (e.block == 2 ? 3 : 0);
   return 0;
 }
 
@@ -355,11 +355,15 @@ bool fwe_maps(const VpFields &f, int nx, int ny, FweMaps *m)
  * between two copies (step k writes copy k % 2 and reads copy (k - 1) % 2),
  * and the last step's advection runs as k_vp_advect after the loop.  Tiles
  * are fetched by TMA where the grid and buffers allow it and allow_tma is
- * set, else by cp.async. */
+ * set, else by cp.async.  time_block 2: without the volume top-up, steps
+ * after the first go in pairs through k_vp_tb2, which writes the pair's
+ * s1, u, v into the copy its first step would have written (the copy of
+ * the step before the pair is still being read), so the copies alternate
+ * once per pair; a step left over at the end runs alone. */
 static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &p, const VpConst &c, VpFields &A,
                               VpFields &B, float *const u_buf[2], float *const v_buf[2], float *const s1_buf[2],
                               const float *rain, float *water_depth, float *sediment, float *vel_u, float *vel_v,
-                              VpScalars *sc, double *partials, bool allow_tma, cudaStream_t s)
+                              VpScalars *sc, double *partials, bool allow_tma, int time_block, cudaStream_t s)
 {
   const size_t n = (size_t)nx * ny;
   FweMaps      maps[2];
@@ -401,6 +405,38 @@ static int vpipes_tiled_steps(float *z, int nx, int ny, const hm_vpipes_params &
   int        buf = 0; /* copy of u, v, s1 the current step writes */
   for (int it = 0; it < p.iterations; it++)
   {
+    if (time_block == 2 && !io.maintain && it > 0 && it + 1 < p.iterations)
+    {
+      const bool last = it + 2 == p.iterations;
+      TbIo       tb;
+      tb.in = VpState{cur->z, cur->d, cur->s, cur->fl, cur->fr, cur->ft, cur->fb};
+      tb.s1_prev = s1_buf[buf ^ 1];
+      tb.u_prev = u_buf[buf ^ 1];
+      tb.v_prev = v_buf[buf ^ 1];
+      tb.rain = rain;
+      tb.out = VpStateOut{nxt->z, nxt->d, nxt->s, nxt->fl, nxt->fr, nxt->ft, nxt->fb, nullptr, nullptr};
+      tb.s1 = s1_buf[buf];
+      tb.u = u_buf[buf];
+      tb.v = v_buf[buf];
+      tb.u_out = last ? vel_u : nullptr;
+      tb.v_out = last ? vel_v : nullptr;
+      tb.diffusion = io.diffusion;
+      tb.pl_one = io.pl_one;
+      tb.kexp_one = io.kexp_one;
+      int rc = launch_vp_tb2(tb, c, s);
+      if (rc) return rc;
+      if (last)
+      {
+        k_vp_advect<ADV_R><<<g2, 256, 0, s>>>(tb.s1, tb.u, tb.v, nxt->s, c);
+        HM_LAUNCH_CHECK("k_vp_advect");
+      }
+      VpFields *t = cur;
+      cur = nxt;
+      nxt = t;
+      buf ^= 1;
+      it++;
+      continue;
+    }
     const bool last = it == p.iterations - 1;
     io.in = VpState{cur->z, cur->d, cur->s, cur->fl, cur->fr, cur->ft, cur->fb};
     io.out = VpStateOut{nxt->z, nxt->d, nxt->s, nxt->fl, nxt->fr, nxt->ft, nxt->fb, nullptr, nullptr};
@@ -506,9 +542,9 @@ int vpipes_core(float *z,
 
   const FusedCfg cfg = vpipes_pick_config(nx, ny);
   const int      algo = vpipes_pick_algo(nx, ny);
-  if (algo == 0 || algo == 2)
+  if (algo == 0 || algo == 2 || algo == 3)
     return vpipes_tiled_steps(z, nx, ny, p, c, A, B, u2, v2, s12, rain, water_depth, sediment, vel_u, vel_v, sc,
-                              partials, algo == 0, s);
+                              partials, algo != 2, algo == 3 ? 2 : 1, s);
   VpStep         st;
   st.rain = rain;
   st.H = cfg.h;
@@ -558,7 +594,7 @@ int vpipes_core(float *z,
 extern "C" int hm_vpipes_set_algorithm(int algo)
 {
   hm::clear_error();
-  if (algo < -1 || algo > 2) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes_set_algorithm: unknown algorithm");
+  if (algo < -1 || algo > 3) return hm::fail(HM_ERR_INVALID_ARGUMENT, "hm_vpipes_set_algorithm: unknown algorithm");
   hm::g_algo_override = algo;
   return HM_OK;
 }

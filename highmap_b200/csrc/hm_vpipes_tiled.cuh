@@ -873,6 +873,20 @@ int launch_step_tma(const FweIo &io, const FweMaps &maps, const AdvMaps &am, con
 int launch_step_cp_async(const FweIo &io, const float *u_prev, const float *v_prev, const VpConst &c, VpScalars *sc,
                          double *partials, dim3 grid, cudaStream_t s);
 
+/* Two steps t, t+1 (t >= 1, no volume top-up) in one launch of k_vp_tb2
+ * (hm_vpipes_tb.cu): the grids it reads and the grids it writes. */
+struct TbIo
+{
+  VpState      in;                        /* state before step t (z, d, fluxes)          */
+  const float *s1_prev, *u_prev, *v_prev; /* step t-1's eroded sediment and velocity      */
+  const float *rain;                      /* nullable                                    */
+  VpStateOut   out;                       /* state after step t+1 (z, d, fluxes)         */
+  float       *s1, *u, *v;                /* step t+1's eroded sediment and velocity      */
+  float       *u_out, *v_out;             /* velocity outputs when t+1 is the last step, nullable */
+  int          diffusion, pl_one, kexp_one;
+};
+int launch_vp_tb2(const TbIo &io, const VpConst &c, cudaStream_t s);
+
 /* tensor maps of one state copy (hm_vpipes.cu); false if the grid or the
  * buffers do not meet the TMA rules (row pitch and bases 16-byte aligned,
  * boxes no larger than the grid) */

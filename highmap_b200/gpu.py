@@ -511,7 +511,7 @@ def vpipes_set_launch(tpb: int = 0, radius: int = 2, rows: int = 128) -> None:
     L.check(L.lib().hm_vpipes_set_launch(int(tpb), int(radius), int(rows)))
 
 
-VPIPES_AUTO, VPIPES_TILED, VPIPES_STREAMING, VPIPES_TILED_CP_ASYNC = -1, 0, 1, 2
+VPIPES_AUTO, VPIPES_TILED, VPIPES_STREAMING, VPIPES_TILED_CP_ASYNC, VPIPES_TILED_TB2 = -1, 0, 1, 2, 3
 
 
 def vpipes_set_algorithm(algo: int = VPIPES_AUTO) -> None:

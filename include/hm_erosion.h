@@ -619,12 +619,16 @@ int hm_vpipes_set_launch(int tpb, int radius, int rows);
  * ny >= 20 and the state buffers are 16-byte aligned, else by cp.async),
  * HM_VPIPES_TILED_CP_ASYNC (the same, always cp.async),
  * HM_VPIPES_STREAMING (all four passes in one kernel streaming down column
- * strips, shaped by hm_vpipes_set_launch), or HM_VPIPES_AUTO (-1: the
- * tuned or built-in choice).  Results do not depend on it. */
+ * strips, shaped by hm_vpipes_set_launch), HM_VPIPES_TILED_TB2 (temporal
+ * blocking: without the water-volume top-up, every pair of steps after the
+ * first in one launch over 32 x 16 tiles that compute the pair's first step
+ * on a 4-cell halo; with the top-up, as HM_VPIPES_TILED), or HM_VPIPES_AUTO
+ * (-1: the tuned or built-in choice).  Results do not depend on it. */
 #define HM_VPIPES_AUTO (-1)
 #define HM_VPIPES_TILED 0
 #define HM_VPIPES_STREAMING 1
 #define HM_VPIPES_TILED_CP_ASYNC 2
+#define HM_VPIPES_TILED_TB2 3
 int hm_vpipes_set_algorithm(int algo);
 
 /* Fault injection for tests of the device-side timeout (no counterpart in
