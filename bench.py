@@ -61,13 +61,15 @@ def _args():
     ap.add_argument("--size", type=int, default=N_SIDE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=["plain", "batch", "serve", "sweep", "extras", "parity"], default="plain",
+    ap.add_argument("--form", choices=["plain", "batch", "serve", "sweep", "extras", "parity", "tblock"],
+                    default="plain",
                     help="plain: the drop-in headline; batch: 256 mixed jobs batched vs plain calls; "
                          "serve: Poisson request stream, continuous batching vs plain FIFO; "
                          "sweep: thermal and vpipes at 1024^2..16384^2, 200 iterations, rates and errors; "
                          "extras: thermal_auto_bedrock, flow_simulation and the sibling talus stencils at 4096^2; "
                          "parity: thermal x500 and vpipes x1000 at 4096^2, GPU vs the reference's kernel text and "
-                         "fp64 on the host cores")
+                         "fp64 on the host cores; tblock: vpipes at one and at two steps per launch (temporal "
+                         "blocking) on the --sizes grids, device-timed, with the autotuner's pick")
     ap.add_argument("--parity-part", choices=["all", "gpu", "host"], default="all",
                     help="parity form: both sides, or only the GPU or host side (sha256 digests link the two)")
     ap.add_argument("--sizes", default="1024,2048,4096,8192,16384", help="grid sides of the sweep form")
@@ -951,6 +953,68 @@ def run_extras(a):
     return 0
 
 
+def run_tblock(a):
+    """Vpipes (the plain drop-in configuration's parameters, 200 iterations)
+    with one step per launch (HM_VPIPES_TILED) and with two
+    (HM_VPIPES_TILED_TB2) on square grids: device time per step,
+    cell-updates/s, algorithmic GB/s against the measured copy bandwidth,
+    whether the two give the same bits, and which the autotuner keeps.  One
+    JSON line per size."""
+    import numpy as np
+    import torch
+
+    from highmap_b200 import gpu as G
+    from highmap_b200 import tune
+    from highmap_b200.inputs import fbm
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if not G.init_opencl():
+        raise RuntimeError("no usable device: " + G.L.lib().hm_last_error().decode())
+    ctx = G.Context(local)
+    dev = torch.device("cuda", local)
+    peak, peak_kind = _peaks()
+    it = SWEEP_ITERS
+    p = G.vpipes_params(**dict(CONFIG2_VPIPES, iterations=it))
+    for k, n in enumerate(int(x) for x in a.sizes.split(",")):
+        z0 = torch.from_numpy(fbm(n, n, seed=10 + k)).to(dev)
+        algos = (("one_step", G.VPIPES_TILED), ("two_steps", G.VPIPES_TILED_TB2))
+        ms = {name: [] for name, _ in algos}
+        res = {}
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        try:
+            for rep in range(3):  # the first pass warms up
+                for name, algo in algos:
+                    G.vpipes_set_algorithm(algo)
+                    z = z0.clone()
+                    sd = torch.empty_like(z)
+                    torch.cuda.synchronize()
+                    e0.record()
+                    G.hydraulic_vpipes_device(z, p, None, None, sd, ctx=ctx)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    if rep:
+                        ms[name].append(e0.elapsed_time(e1) / it)
+                    res[name] = (z.cpu().numpy(), sd.cpu().numpy())
+        finally:
+            G.vpipes_set_algorithm(G.VPIPES_AUTO)
+        same = all(np.array_equal(x, y) for x, y in zip(res["one_step"], res["two_steps"]))
+        tuned = tune.autotune(tune.VPIPES, n, n, steps=20, ctx=ctx)
+        row = {"form": "tblock", "grid": [n, n], "iterations": it, "bit_identical": bool(same),
+               "tuned_time_block": 2 if (tuned["tpb"] == 0 and tuned["time_block"] == 2) else 1,
+               "tuned": tuned, "peak_gbs": peak, "peak_kind": peak_kind}
+        for name, _ in algos:
+            t = min(ms[name])
+            rate = n * n / (t * 1e-3)
+            row[name] = {"ms_per_step": t, "cell_updates_per_s": rate, "algorithmic_gbs": rate * 56 / 1e9,
+                         "frac": rate * 56 / 1e9 / peak}
+        row["two_over_one_time"] = row["two_steps"]["ms_per_step"] / row["one_step"]["ms_per_step"]
+        print(json.dumps(row), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_form(a):
     """The batched or served form on one GPU (rank 0 of a torchrun launch
     runs it; the others exit)."""
@@ -997,6 +1061,8 @@ def main():
         return run_extras(a)
     if a.form == "parity":
         return run_parity(a)
+    if a.form == "tblock":
+        return run_tblock(a)
     if a.form != "plain":
         return run_form(a)
     return run_ours(a)
