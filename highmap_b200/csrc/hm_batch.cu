@@ -61,6 +61,9 @@ constexpr int TH_W = 256;  /* thermal tile: a warp per 32 columns        */
  * 8 % less time for the round graphs of the 206 jobs under 1024^2 cells of
  * the batched benchmark's mix. */
 constexpr int BATCH_CTAS_PER_SM = 4;
+/* built-in launch of the rounds: one CTA per tile (true) or persistent
+ * CTAs taking tiles from a counter (false) */
+constexpr bool BATCH_ONE_TILE = false;
 constexpr int BATCH_TH_ROWS_1 = 4, BATCH_TH_ROWS_2 = 2;
 
 /* device-side description of one job */
@@ -145,10 +148,14 @@ __device__ __forceinline__ void thermal_tile(const BJob &J, int par, int bx, int
  * eroded sediment into the tile (fwe_stage_cp_async_step, advect_region1).
  * F: FWE_RTOPTS when every active vpipes job has pipe length 1 and
  * discharge exponent 1 (the lean form without fp64 pow), else FWE_GENERIC;
- * both compiled for BATCH_CTAS_PER_SM CTAs per SM.  Thread 0 takes the
- * CTA's next tile index while the current tile is computed, so the
- * atomic's latency is hidden. */
-template <int F>
+ * both compiled for BATCH_CTAS_PER_SM CTAs per SM.  PERSIST: thread 0
+ * takes the CTA's next tile index while the current tile is computed, so
+ * the atomic's latency is hidden.  Without it the grid has one CTA per
+ * tile of the round and CTA b takes tile b (counter unused): the block
+ * scheduler starts a tile whenever a CTA slot frees, and a tile's staging
+ * wait overlaps the other resident CTAs' tiles, as in the plain step
+ * kernels. */
+template <int F, bool PERSIST>
 __global__ void __launch_bounds__(BT, BATCH_CTAS_PER_SM)
     k_batch_round(const BJob *__restrict__ jobs,
                   const int4 *__restrict__ vt,
@@ -164,7 +171,7 @@ __global__ void __launch_bounds__(BT, BATCH_CTAS_PER_SM)
   __shared__ FweIo   s_io;
   __shared__ VpConst s_c;
   __shared__ int     s_step;
-  int                next = threadIdx.x == 0 ? (int)atomicAdd(counter, 1u) : 0;
+  int                next = PERSIST ? (threadIdx.x == 0 ? (int)atomicAdd(counter, 1u) : 0) : (int)blockIdx.x;
   for (;;)
   {
     __syncthreads(); /* the previous tile is done with the shared state */
@@ -172,7 +179,8 @@ __global__ void __launch_bounds__(BT, BATCH_CTAS_PER_SM)
     {
       const int t = next;
       s_tile = t;
-      if (t < nv + nt) next = (int)atomicAdd(counter, 1u); /* used by the next iteration */
+      if (!PERSIST) next = nv + nt; /* one tile: the next iteration returns */
+      else if (t < nv + nt) next = (int)atomicAdd(counter, 1u); /* used by the next iteration */
       if (t < nv)
       {
         const BJob &J = jobs[vt[t].x];
@@ -346,6 +354,7 @@ struct hm_batch
   int               grid_cap = 0; /* persistent CTAs of k_batch_round<FWE_RTOPTS>  */
   int               grid_cap_gen = 0; /* persistent CTAs of k_batch_round<FWE_GENERIC> */
   int               th_rows = 16; /* rows of a thermal tile            */
+  bool              one_tile = hm::BATCH_ONE_TILE; /* one CTA per tile instead of persistent CTAs */
   /* device tables */
   hm::BJob         *d_jobs = nullptr;
   size_t            d_jobs_cap = 0;
@@ -529,12 +538,24 @@ int launch_rounds(hm_batch *b, const Plan &pl)
       while (m > 0 && pl.rem[m - 1] <= r) m--;
       const size_t iv = tl.vcum[m], it = tl.tcum[m];
       const int total = (int)(iv + it);
+      if (b->one_tile)
+      {
+        const int grid = std::max(1, total);
+        if (tl.generic)
+          hm::k_batch_round<hm::FWE_GENERIC, false><<<grid, hm::BT, 0, b->stream>>>(
+              b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it, b->round + r, nullptr);
+        else
+          hm::k_batch_round<hm::FWE_RTOPTS, false><<<grid, hm::BT, 0, b->stream>>>(
+              b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it, b->round + r, nullptr);
+        HM_LAUNCH_CHECK("k_batch_round");
+        continue;
+      }
       const int grid = std::max(1, std::min(tl.generic ? b->grid_cap_gen : b->grid_cap, total));
       if (tl.generic)
-        hm::k_batch_round<hm::FWE_GENERIC><<<grid, hm::BT, 0, b->stream>>>(
+        hm::k_batch_round<hm::FWE_GENERIC, true><<<grid, hm::BT, 0, b->stream>>>(
             b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it, b->round + r, b->d_counters + r);
       else
-        hm::k_batch_round<hm::FWE_RTOPTS><<<grid, hm::BT, 0, b->stream>>>(
+        hm::k_batch_round<hm::FWE_RTOPTS, true><<<grid, hm::BT, 0, b->stream>>>(
             b->d_jobs, b->d_tiles, (int)iv, b->d_tiles + nv, (int)it, b->round + r, b->d_counters + r);
       HM_LAUNCH_CHECK("k_batch_round");
     }
@@ -624,15 +645,17 @@ int hm_batch_create(hm_context *ctx, hm_batch **out)
     HM_CUDA_TRY(cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   }
   int per_sm = 0, per_sm_gen = 0, sms = 0;
-  HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hm::k_batch_round<hm::FWE_RTOPTS>, hm::BT, 0));
   HM_CUDA_TRY(
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_gen, hm::k_batch_round<hm::FWE_GENERIC>, hm::BT, 0));
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hm::k_batch_round<hm::FWE_RTOPTS, true>, hm::BT, 0));
+  HM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_gen, hm::k_batch_round<hm::FWE_GENERIC, true>,
+                                                            hm::BT, 0));
   HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-  /* persistent CTAs per SM and thermal tile rows: the tuned choice, or all
-   * CTAs that fit and 16 rows */
+  /* persistent CTAs per SM (0: one CTA per tile) and thermal tile rows:
+   * the tuned choice, or the built-in one and 16 rows */
   hm::TuneEntry te;
   if (hm::tuned_batch(&te))
   {
+    b->one_tile = te.tpb == 0;
     if (te.tpb >= 1)
     {
       per_sm = std::min(per_sm, te.tpb);

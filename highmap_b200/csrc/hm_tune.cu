@@ -11,7 +11,8 @@
  *             output rows per CTA (the occupancy / halo / warm-up trade);
  *   thermal : steps per launch (temporal-block depth 1, 2, 4, 8) x rows
  *             per CTA of the blocked kernel;
- *   batch   : persistent CTAs per SM (occupancy) x rows of a thermal tile
+ *   batch   : persistent CTAs per SM (occupancy; 0 = one CTA per tile of
+ *             the round) x rows of a thermal tile
  *             of the batched form's round kernel, on a synthetic mixed
  *             batch (one entry for the process).
  * The solvers consult the table whenever the caller leaves the choice to
@@ -146,7 +147,8 @@ int autotune_batch(hm_context *ctx, int side_max, int steps, hm_tune_result *res
     jobs.push_back(j);
   }
   std::vector<TuneEntry> cands;
-  for (int per_sm = 1; per_sm <= 4; per_sm++)
+  /* per_sm 0: one CTA per tile of the round instead of persistent CTAs */
+  for (int per_sm = 0; per_sm <= 4; per_sm++)
     for (int rows : {8, 16, 32}) cands.push_back(TuneEntry{per_sm, 0, rows, 0, 0.f});
   int   best = -1;
   float best_ms = 0.f;
@@ -388,7 +390,7 @@ int hm_autotune_load(const char *path, int *loaded_out)
       hm::g_th[{cx, cy}] = e;
       loaded++;
     }
-    else if (k == "batch" && e.tpb >= 1 && e.tpb <= 4 && (e.rows == 8 || e.rows == 16 || e.rows == 32))
+    else if (k == "batch" && e.tpb >= 0 && e.tpb <= 4 && (e.rows == 8 || e.rows == 16 || e.rows == 32))
     {
       std::lock_guard<std::mutex> lk(hm::g_mu);
       hm::g_batch = e;

@@ -729,16 +729,19 @@ int       hm_batch_run(hm_context *ctx, const hm_job *jobs, int njobs, int use_g
  * two); solves that leave the choice to the library (time_block 0, no
  * hm_vpipes_set_launch override) then use it.  Process-wide; do not run
  * while other threads solve.  kind: HM_JOB_THERMAL or HM_JOB_VPIPES, or
- * HM_TUNE_BATCH: the batched form's persistent CTAs per SM (1..4) and
- * thermal tile rows (8, 16, 32), timed over `steps` rounds of a synthetic
- * batch of 16 jobs, half thermal and half vpipes, with sides from 128 up to
- * max(nx, ny); batches created afterwards use the fastest (result: tpb =
- * CTAs per SM, rows = thermal tile rows, ms_per_step = per round). */
+ * HM_TUNE_BATCH: the batched form's round launch (persistent CTAs per SM,
+ * 1..4, or 0: one CTA per tile of the round) and thermal tile rows (8, 16,
+ * 32), timed over `steps` rounds of a synthetic batch of 16 jobs, half
+ * thermal and half vpipes, with sides from 128 up to max(nx, ny); batches
+ * created afterwards use the fastest (result: tpb = CTAs per SM or 0,
+ * rows = thermal tile rows, ms_per_step = per round).  The time_block field
+ * of the result holds the steps per launch of the vpipes tiled kernels for
+ * HM_JOB_VPIPES and of the thermal kernel for HM_JOB_THERMAL. */
 #define HM_TUNE_BATCH 3
 typedef struct hm_tune_result
 {
   int   tpb, radius, rows; /* vpipes launch shape (rows: also thermal's blocked kernel) */
-  int   time_block;        /* thermal steps per launch                               */
+  int   time_block;        /* steps per launch: thermal, or vpipes' tiled kernels (0, 1: one; 2: two) */
   float ms_per_step;
   int   candidates;
 } hm_tune_result;

@@ -103,6 +103,28 @@ def test_batch_run_matches_oracle(gpu, use_graph):
     _verify(cases)
 
 
+@pytest.mark.parametrize("per_sm", [0, 4, 1])
+def test_round_launch_modes(gpu, tmp_path, per_sm):
+    """The rounds launched as one CTA per tile (per_sm 0) or as persistent
+    CTAs (1 or 4 per SM), chosen through a launch-shape table: every job
+    still gives the oracle's bits."""
+    import torch
+    from highmap_b200 import batch as B
+    from highmap_b200 import tune
+    t = tmp_path / "batch.txt"
+    t.write_text("batch 0 0 %d 0 16 0 1.0\n" % per_sm)
+    tune.clear()
+    try:
+        assert tune.load(str(t)) == 1
+        for use_graph in (True, False):
+            jobs, cases = _make(_specs(), seed0=90)
+            B.run(jobs, use_graph=use_graph)
+            torch.cuda.synchronize()
+            _verify(cases)
+    finally:
+        tune.clear()
+
+
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_batch_run_with_large_jobs(gpu, use_graph):
     """Jobs of at least 2^20 cells run through the plain solvers on a side
