@@ -73,6 +73,24 @@ def test_argument_checks_without_device(built_lib):
         assert b"NULL" in lib.hm_last_error(), name
 
 
+def test_step_kernel_selection_without_device(built_lib):
+    """The vpipes step-kernel choice is process-wide host state: every
+    declared algorithm, temporal blocking (two steps per launch) included,
+    is accepted and anything else refused, with no device call."""
+    from highmap_b200 import _lib as L
+    from highmap_b200 import gpu as G
+    lib = L.lib()
+    try:
+        for algo in (G.VPIPES_AUTO, G.VPIPES_TILED, G.VPIPES_STREAMING, G.VPIPES_TILED_CP_ASYNC,
+                     G.VPIPES_TILED_TB2):
+            assert lib.hm_vpipes_set_algorithm(algo) == L.HM_OK, algo
+        for bad in (-2, 4, 99):
+            assert lib.hm_vpipes_set_algorithm(bad) == L.HM_ERR_INVALID_ARGUMENT, bad
+            assert b"unknown algorithm" in lib.hm_last_error()
+    finally:
+        lib.hm_vpipes_set_algorithm(G.VPIPES_AUTO)
+
+
 def test_defaults_match_reference_signature(built_lib):
     """hm_vpipes_default_params carries the defaults of
     HighMap/include/highmap/erosion.hpp:1206-1223."""

@@ -28,6 +28,27 @@ def test_load_skips_invalid_lines(built_lib, tmp_path):
     tune.clear()
 
 
+def test_load_time_block_and_one_tile_entries(built_lib, tmp_path):
+    """Vpipes entries of the tiled kernels keep their steps per launch (0, 1
+    or 2; others are refused), and a batch entry with 0 CTAs per SM (one CTA
+    per tile of a round) is accepted."""
+    from highmap_b200 import tune
+    p = tmp_path / "shapes.txt"
+    p.write_text("vpipes 10 10 0 0 0 2 0.200\n"
+                 "vpipes 11 11 0 0 0 3 0.200\n"         # unsupported steps per launch
+                 "batch 0 0 0 0 32 0 0.300\n")
+    tune.clear()
+    try:
+        assert tune.load(str(p)) == 2
+        out = tmp_path / "out.txt"
+        tune.save(str(out))
+        text = out.read_text()
+        assert "vpipes 10 10 0 0 0 2" in text and "vpipes 11 11" not in text
+        assert "batch 0 0 0 0 32 0" in text
+    finally:
+        tune.clear()
+
+
 @pytest.mark.gpu
 def test_autotune_then_parity(gpu, tmp_path):
     from highmap_b200 import tune
