@@ -192,18 +192,34 @@ __device__ __noinline__ float tb_s1_at(const TbIo io, const VpConst c, int i, in
 
 /* ---- the kernel ------------------------------------------------------ */
 
-/* the cells of the tile's ring of width h that lie inside the grid */
+/* the cells of the tile's ring of width h that lie inside the grid, and
+ * the rounded reciprocal of the row width */
 struct TbRegion
 {
-  int xa, ya, w, cnt;
+  int   xa, ya, w, cnt;
+  float rw;
 };
 
 __device__ __forceinline__ TbRegion tb_region(int x0, int y0, int h, int nx, int ny)
 {
   const int xa = max(0, x0 - h), xb = min(nx - 1, x0 + TB_TX - 1 + h);
   const int ya = max(0, y0 - h), yb = min(ny - 1, y0 + TB_TY - 1 + h);
-  return TbRegion{xa, ya, xb - xa + 1, (xb - xa + 1) * (yb - ya + 1)};
+  const int w = xb - xa + 1;
+  return TbRegion{xa, ya, w, w * (yb - ya + 1), __fdiv_rn(1.f, (float)w)};
 }
+
+/* grid cell of item e of region r: row e / w as (e + 0.5) * RN(1/w)
+ * truncated, exact for every w < 64 and e < 4096 (checked exhaustively;
+ * the regions have w <= 44 and at most 1232 cells) */
+__device__ __forceinline__ void tb_cell(const TbRegion &r, int e, int &gx, int &gy)
+{
+  const int q = (int)__fmul_rn(__fadd_rn((float)e, 0.5f), r.rw);
+  gx = r.xa + (e - q * r.w);
+  gy = r.ya + q;
+}
+
+/* items of the first pass's advection loop whose loads are issued together */
+constexpr int TB_AB = 2;
 
 template <int F>
 __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
@@ -229,28 +245,61 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
               at(gx, min(gy + 1, ny - 1))};
   };
 
-  /* A: step t's z and start depth (h 6), old fluxes and advected sediment (h 5) */
+  /* A: step t's z and start depth (h 6), old fluxes and advected sediment
+   * (h 5); the advection takes TB_AB items at a time so that their
+   * velocity loads, then their tap gathers, are in flight together */
   {
     const TbRegion r = tb_region(x0, y0, TB_H2, nx, ny);
+#pragma unroll 4
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
-      const int    q = e / r.w, gx = r.xa + (e - q * r.w), gy = r.ya + q;
+      int gx, gy;
+      tb_cell(r, e, gx, gy);
       const size_t k = (size_t)gy * nx + gx;
       const int    i = at(gx, gy);
       Z[i] = __ldg(io.in.z + k);
       D[i] = tb_d1(c, io.rain, __ldg(io.in.d + k), k);
     }
     const TbRegion r1 = tb_region(x0, y0, TB_H1, nx, ny);
-    for (int e = tid; e < r1.cnt; e += TB_NT)
+    for (int e0 = tid; e0 < r1.cnt; e0 += TB_AB * TB_NT)
     {
-      const int    q = e / r1.w, gx = r1.xa + (e - q * r1.w), gy = r1.ya + q;
-      const size_t k = (size_t)gy * nx + gx;
-      const int    i = at(gx, gy);
-      FL[i] = __ldg(io.in.fl + k);
-      FR[i] = __ldg(io.in.fr + k);
-      FT[i] = __ldg(io.in.ft + k);
-      FB[i] = __ldg(io.in.fb + k);
-      S[i] = tb_advect(c, io.s1_prev, __ldg(io.u_prev + k), __ldg(io.v_prev + k), gx, gy);
+      int   gx[TB_AB], gy[TB_AB];
+      float uu[TB_AB], vv[TB_AB];
+#pragma unroll
+      for (int q = 0; q < TB_AB; q++)
+      {
+        /* an item past the region repeats the last cell and is not stored */
+        tb_cell(r1, min(e0 + q * TB_NT, r1.cnt - 1), gx[q], gy[q]);
+        const size_t k = (size_t)gy[q] * nx + gx[q];
+        uu[q] = __ldg(io.u_prev + k);
+        vv[q] = __ldg(io.v_prev + k);
+      }
+      Tap   t[TB_AB];
+      float g[TB_AB][4];
+#pragma unroll
+      for (int q = 0; q < TB_AB; q++)
+      {
+        const float x = fsub((float)gx[q], fmul(c.dt, uu[q]));
+        const float y = fsub((float)gy[q], fmul(c.dt, vv[q]));
+        t[q] = linear_tap(x, y, nx, ny);
+        const size_t k0 = (size_t)t[q].j0 * nx, k1 = (size_t)t[q].j1 * nx;
+        g[q][0] = __ldg(io.s1_prev + k0 + t[q].i0);
+        g[q][1] = __ldg(io.s1_prev + k0 + t[q].i1);
+        g[q][2] = __ldg(io.s1_prev + k1 + t[q].i0);
+        g[q][3] = __ldg(io.s1_prev + k1 + t[q].i1);
+      }
+#pragma unroll
+      for (int q = 0; q < TB_AB; q++)
+        if (e0 + q * TB_NT < r1.cnt)
+        {
+          const size_t k = (size_t)gy[q] * nx + gx[q];
+          const int    i = at(gx[q], gy[q]);
+          S[i] = blend(t[q], g[q][0], g[q][1], g[q][2], g[q][3]);
+          FL[i] = __ldg(io.in.fl + k);
+          FR[i] = __ldg(io.in.fr + k);
+          FT[i] = __ldg(io.in.ft + k);
+          FB[i] = __ldg(io.in.fb + k);
+        }
     }
   }
   __syncthreads();
@@ -260,7 +309,8 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
     const TbRegion r = tb_region(x0, y0, TB_H1, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
-      const int q = e / r.w, gx = r.xa + (e - q * r.w), gy = r.ya + q;
+      int gx, gy;
+      tb_cell(r, e, gx, gy);
       const Nb  p = nb(gx, gy);
       float     fl = FL[p.c], fr = FR[p.c], ft = FT[p.c], fb = FB[p.c];
       tb_flow<F>(c, io, Z[p.c], D[p.c], Z[p.w], D[p.w], Z[p.e], D[p.e], Z[p.s], D[p.s], Z[p.n], D[p.n], fl, fr, ft, fb);
@@ -278,7 +328,8 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
     const TbRegion r = tb_region(x0, y0, TB_HX, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
-      const int q = e / r.w, gx = r.xa + (e - q * r.w), gy = r.ya + q;
+      int gx, gy;
+      tb_cell(r, e, gx, gy);
       const Nb  p = nb(gx, gy);
       float     d2, u, v, zo, so;
       tb_water<F>(c, io, D[p.c], FL[p.c], FR[p.c], FT[p.c], FB[p.c], FR[p.w], FL[p.e], FT[p.n], FB[p.s], d2, u, v);
@@ -298,7 +349,8 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
     const TbRegion r = tb_region(x0, y0, 2, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
-      const int q = e / r.w, gx = r.xa + (e - q * r.w), gy = r.ya + q;
+      int gx, gy;
+      tb_cell(r, e, gx, gy);
       const int i = at(gx, gy);
       D[i] = tb_d1(c, io.rain, D[i], (size_t)gy * nx + gx);
     }
@@ -311,7 +363,8 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
     const TbRegion r1 = tb_region(x0, y0, 1, nx, ny);
     for (int e = tid; e < r1.cnt; e += TB_NT)
     {
-      const int   q = e / r1.w, gx = r1.xa + (e - q * r1.w), gy = r1.ya + q;
+      int gx, gy;
+      tb_cell(r1, e, gx, gy);
       const int   i = at(gx, gy);
       const float x = fsub((float)gx, fmul(c.dt, UN[i]));
       const float y = fsub((float)gy, fmul(c.dt, VN[i]));
@@ -327,7 +380,8 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
     const TbRegion r = tb_region(x0, y0, 1, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
-      const int q = e / r.w, gx = r.xa + (e - q * r.w), gy = r.ya + q;
+      int gx, gy;
+      tb_cell(r, e, gx, gy);
       const Nb  p = nb(gx, gy);
       float     fl = FL[p.c], fr = FR[p.c], ft = FT[p.c], fb = FB[p.c];
       tb_flow<F>(c, io, ZN[p.c], D[p.c], ZN[p.w], D[p.w], ZN[p.e], D[p.e], ZN[p.s], D[p.s], ZN[p.n], D[p.n], fl, fr, ft,
@@ -345,7 +399,8 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
     const TbRegion r = tb_region(x0, y0, 0, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
-      const int    q = e / r.w, gx = r.xa + (e - q * r.w), gy = r.ya + q;
+      int gx, gy;
+      tb_cell(r, e, gx, gy);
       const Nb     p = nb(gx, gy);
       const size_t k = (size_t)gy * nx + gx;
       float        d2, u, v, zo, so;
