@@ -274,12 +274,15 @@ int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_re
 
   int       best = -1;
   float     best_ms = 0.f;
-  const int warm = 2;
+  /* one warm-up run, then the best of three timed runs: at small sizes a
+   * run lasts a few hundred microseconds and one timing alone can pick a
+   * slower candidate */
+  const int warm = 1, timed = 3;
   for (size_t k = 0; k < cands.size() && !st; k++)
   {
     const hm::TuneEntry &c = cands[k];
     float                ms = 0.f;
-    for (int rep = 0; rep < warm + 1 && !st; rep++)
+    for (int rep = 0; rep < warm + timed && !st; rep++)
     {
       HM_CUDA_TRY(cudaMemcpyAsync(z, z0, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
       HM_CUDA_TRY(cudaEventRecord(e0, s));
@@ -300,7 +303,9 @@ int hm_autotune(hm_context *ctx, int kind, int nx, int ny, int steps, hm_tune_re
       }
       HM_CUDA_TRY(cudaEventRecord(e1, s));
       HM_CUDA_TRY(cudaEventSynchronize(e1));
-      HM_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      float t = 0.f;
+      HM_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+      if (rep == warm || (rep > warm && t < ms)) ms = t;
     }
     cands[k].ms_per_step = ms / steps;
     if (!st && (best < 0 || ms < best_ms))
