@@ -4,7 +4,8 @@
  * The reference advances one step per round of its four kernels
  * (HighMap/src/erosion/hydraulic_vpipes_gpu.cpp:59-170 around
  * HighMap/src/gpu_opencl/kernels/hydraulic_vpipes.cl:5-211).  k_vp_tb2
- * advances steps t and t + 1 of a 32 x 16 output tile in one CTA: the
+ * advances steps t and t + 1 of an output tile (32 x 16, or 16 x 8 on
+ * small grids) in one CTA: the
  * state of step t is read once from HBM and only the state after step
  * t + 1 is written, half the traffic of two one-step launches, at the cost
  * of computing step t again on a halo that neighbouring tiles also compute.
@@ -41,16 +42,21 @@
 namespace hm
 {
 
-constexpr int TB_TX = 32, TB_TY = 16;   /* output tile                         */
 constexpr int TB_NT = 256;              /* threads per CTA                     */
 constexpr int TB_HX = 4;                /* ring of step t's eroded sediment     */
 constexpr int TB_H1 = TB_HX + 1;        /* ring of step t's flow and advection  */
 constexpr int TB_H2 = TB_HX + 2;        /* ring of step t's z and depth         */
-constexpr int TB_W = TB_TX + 2 * TB_H2; /* shared-memory row: 44 columns        */
-constexpr int TB_H = TB_TY + 2 * TB_H2; /* 28 rows                              */
-constexpr int TB_N = TB_W * TB_H;
-/* shared-memory fields, each TB_W x TB_H floats over columns x0-6 .. x0+37
- * and rows y0-6 .. y0+21 */
+/* Output tile TX x TY: 32 x 16, or 16 x 8 on grids with fewer than two
+ * 32 x 16 tiles per SM, where a launch is one wave and its time is one
+ * CTA's chain of dependent passes (a quarter of the cells per CTA, four
+ * times the CTAs).  Shared-memory fields, each W x H floats over columns
+ * x0-6 .. x0+TX+5 and rows y0-6 .. y0+TY+5. */
+template <int TX, int TY>
+struct TbShape
+{
+  static constexpr int    W = TX + 2 * TB_H2, H = TY + 2 * TB_H2, N = W * H;
+  static constexpr size_t SMEM = 11 * (size_t)N * sizeof(float);
+};
 enum
 {
   TB_Z,   /* z of step t                                        */
@@ -66,7 +72,7 @@ enum
   TB_VN,
   TB_NF
 };
-constexpr size_t TB_SMEM = (size_t)TB_NF * TB_N * sizeof(float);
+static_assert(TB_NF == 11, "TbShape::SMEM holds eleven fields");
 
 /* Kernel option word: TB_DIFF flux diffusion; TB_GEN pipe length and
  * discharge exponent read at run time (without it both are 1, and
@@ -200,10 +206,11 @@ struct TbRegion
   float rw;
 };
 
+template <int TX, int TY>
 __device__ __forceinline__ TbRegion tb_region(int x0, int y0, int h, int nx, int ny)
 {
-  const int xa = max(0, x0 - h), xb = min(nx - 1, x0 + TB_TX - 1 + h);
-  const int ya = max(0, y0 - h), yb = min(ny - 1, y0 + TB_TY - 1 + h);
+  const int xa = max(0, x0 - h), xb = min(nx - 1, x0 + TX - 1 + h);
+  const int ya = max(0, y0 - h), yb = min(ny - 1, y0 + TY - 1 + h);
   const int w = xb - xa + 1;
   return TbRegion{xa, ya, w, w * (yb - ya + 1), __fdiv_rn(1.f, (float)w)};
 }
@@ -221,20 +228,22 @@ __device__ __forceinline__ void tb_cell(const TbRegion &r, int e, int &gx, int &
 /* items of the first pass's advection loop whose loads are issued together */
 constexpr int TB_AB = 2;
 
-template <int F>
+template <int F, int TX, int TY>
 __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
 {
   extern __shared__ __align__(16) float tb_sm[];
-  float *const Z = tb_sm + TB_Z * TB_N, *const D = tb_sm + TB_D * TB_N;
-  float *const FL = tb_sm + TB_FL * TB_N, *const FR = tb_sm + TB_FR * TB_N;
-  float *const FT = tb_sm + TB_FT * TB_N, *const FB = tb_sm + TB_FB * TB_N;
-  float *const S = tb_sm + TB_S * TB_N, *const ZN = tb_sm + TB_ZN * TB_N;
-  float *const S1N = tb_sm + TB_S1N * TB_N, *const UN = tb_sm + TB_UN * TB_N, *const VN = tb_sm + TB_VN * TB_N;
+  using Sh = TbShape<TX, TY>;
+  constexpr int N = Sh::N;
+  float *const  Z = tb_sm + TB_Z * N, *const D = tb_sm + TB_D * N;
+  float *const  FL = tb_sm + TB_FL * N, *const FR = tb_sm + TB_FR * N;
+  float *const  FT = tb_sm + TB_FT * N, *const FB = tb_sm + TB_FB * N;
+  float *const  S = tb_sm + TB_S * N, *const ZN = tb_sm + TB_ZN * N;
+  float *const  S1N = tb_sm + TB_S1N * N, *const UN = tb_sm + TB_UN * N, *const VN = tb_sm + TB_VN * N;
   const int    nx = c.nx, ny = c.ny, tid = threadIdx.x;
-  const int    x0 = blockIdx.x * TB_TX, y0 = blockIdx.y * TB_TY;
+  const int    x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int    ox = x0 - TB_H2, oy = y0 - TB_H2;
   /* shared-memory index of grid cell (gx, gy) of the h <= 6 region */
-  auto at = [&](int gx, int gy) { return (gy - oy) * TB_W + (gx - ox); };
+  auto at = [&](int gx, int gy) { return (gy - oy) * Sh::W + (gx - ox); };
   /* indices of a cell and its clamped neighbours */
   struct Nb
   {
@@ -249,7 +258,7 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
    * (h 5); the advection takes TB_AB items at a time so that their
    * velocity loads, then their tap gathers, are in flight together */
   {
-    const TbRegion r = tb_region(x0, y0, TB_H2, nx, ny);
+    const TbRegion r = tb_region<TX, TY>(x0, y0, TB_H2, nx, ny);
 #pragma unroll 4
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
@@ -260,7 +269,7 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
       Z[i] = __ldg(io.in.z + k);
       D[i] = tb_d1(c, io.rain, __ldg(io.in.d + k), k);
     }
-    const TbRegion r1 = tb_region(x0, y0, TB_H1, nx, ny);
+    const TbRegion r1 = tb_region<TX, TY>(x0, y0, TB_H1, nx, ny);
     for (int e0 = tid; e0 < r1.cnt; e0 += TB_AB * TB_NT)
     {
       int   gx[TB_AB], gy[TB_AB];
@@ -306,7 +315,7 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
 
   /* B: step t's flow (h 5); a cell reads only its own old fluxes */
   {
-    const TbRegion r = tb_region(x0, y0, TB_H1, nx, ny);
+    const TbRegion r = tb_region<TX, TY>(x0, y0, TB_H1, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
       int gx, gy;
@@ -325,7 +334,7 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
   /* C: step t's water and erosion (h 4); the depth slot of a cell takes its
    * evaporated depth (only the cell itself reads its start depth here) */
   {
-    const TbRegion r = tb_region(x0, y0, TB_HX, nx, ny);
+    const TbRegion r = tb_region<TX, TY>(x0, y0, TB_HX, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
       int gx, gy;
@@ -346,7 +355,7 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
 
   /* D: step t+1's start depth (h 2) and advected sediment (h 1) */
   {
-    const TbRegion r = tb_region(x0, y0, 2, nx, ny);
+    const TbRegion r = tb_region<TX, TY>(x0, y0, 2, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
       int gx, gy;
@@ -356,11 +365,11 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
     }
     /* s1_t at grid cell (ti, tj): shared memory inside the h 4 region,
      * else recomputed from step t's state */
-    const int xlo = x0 - TB_HX, xhi = x0 + TB_TX - 1 + TB_HX, ylo = y0 - TB_HX, yhi = y0 + TB_TY - 1 + TB_HX;
+    const int xlo = x0 - TB_HX, xhi = x0 + TX - 1 + TB_HX, ylo = y0 - TB_HX, yhi = y0 + TY - 1 + TB_HX;
     auto      s1t = [&](int ti, int tj) {
       return (ti >= xlo && ti <= xhi && tj >= ylo && tj <= yhi) ? S1N[at(ti, tj)] : tb_s1_at<F>(io, c, ti, tj);
     };
-    const TbRegion r1 = tb_region(x0, y0, 1, nx, ny);
+    const TbRegion r1 = tb_region<TX, TY>(x0, y0, 1, nx, ny);
     for (int e = tid; e < r1.cnt; e += TB_NT)
     {
       int gx, gy;
@@ -377,7 +386,7 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
 
   /* E: step t+1's flow (h 1) on z after step t and the new start depth */
   {
-    const TbRegion r = tb_region(x0, y0, 1, nx, ny);
+    const TbRegion r = tb_region<TX, TY>(x0, y0, 1, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
       int gx, gy;
@@ -396,7 +405,7 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
 
   /* F: step t+1's water and erosion on the tile, written out */
   {
-    const TbRegion r = tb_region(x0, y0, 0, nx, ny);
+    const TbRegion r = tb_region<TX, TY>(x0, y0, 0, nx, ny);
     for (int e = tid; e < r.cnt; e += TB_NT)
     {
       int gx, gy;
@@ -424,24 +433,44 @@ __global__ void __launch_bounds__(TB_NT, 4) k_vp_tb2(TbIo io, VpConst c)
 }
 
 /* Launch k_vp_tb2 for steps t, t+1 (t >= 1, no volume top-up) on stream s. */
-int launch_vp_tb2(const TbIo &io, const VpConst &c, cudaStream_t s)
+template <int TX, int TY>
+static int launch_tb2_shape(const TbIo &io, const VpConst &c, cudaStream_t s)
 {
-  static bool attr_set[64] = {};
-  int         dev = 0;
+  constexpr int SMEM = (int)TbShape<TX, TY>::SMEM;
+  static bool   attr_set[64] = {};
+  int           dev = 0;
   HM_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64 || !attr_set[dev])
   {
-    HM_CUDA_TRY(cudaFuncSetAttribute(k_vp_tb2<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TB_SMEM));
-    HM_CUDA_TRY(cudaFuncSetAttribute(k_vp_tb2<TB_DIFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TB_SMEM));
-    HM_CUDA_TRY(cudaFuncSetAttribute(k_vp_tb2<TB_GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TB_SMEM));
+    HM_CUDA_TRY(cudaFuncSetAttribute(k_vp_tb2<0, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+    HM_CUDA_TRY(cudaFuncSetAttribute(k_vp_tb2<TB_DIFF, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+    HM_CUDA_TRY(cudaFuncSetAttribute(k_vp_tb2<TB_GEN, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
     if (dev >= 0 && dev < 64) attr_set[dev] = true;
   }
-  const dim3 grid((c.nx + TB_TX - 1) / TB_TX, (c.ny + TB_TY - 1) / TB_TY);
-  if (!io.pl_one || !io.kexp_one) k_vp_tb2<TB_GEN><<<grid, TB_NT, TB_SMEM, s>>>(io, c);
-  else if (io.diffusion) k_vp_tb2<TB_DIFF><<<grid, TB_NT, TB_SMEM, s>>>(io, c);
-  else k_vp_tb2<0><<<grid, TB_NT, TB_SMEM, s>>>(io, c);
+  const dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY);
+  if (!io.pl_one || !io.kexp_one) k_vp_tb2<TB_GEN, TX, TY><<<grid, TB_NT, SMEM, s>>>(io, c);
+  else if (io.diffusion) k_vp_tb2<TB_DIFF, TX, TY><<<grid, TB_NT, SMEM, s>>>(io, c);
+  else k_vp_tb2<0, TX, TY><<<grid, TB_NT, SMEM, s>>>(io, c);
   HM_LAUNCH_CHECK("k_vp_tb2");
   return HM_OK;
+}
+
+/* Launch k_vp_tb2 for steps t, t+1 (t >= 1, no volume top-up) on stream s:
+ * 16 x 8 tiles on grids with fewer than two 32 x 16 tiles per SM. */
+int launch_vp_tb2(const TbIo &io, const VpConst &c, cudaStream_t s)
+{
+  static int sms[64] = {};
+  int        dev = 0;
+  HM_CUDA_TRY(cudaGetDevice(&dev));
+  int n_sm = dev >= 0 && dev < 64 ? sms[dev] : 0;
+  if (n_sm == 0)
+  {
+    HM_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    if (dev >= 0 && dev < 64) sms[dev] = n_sm;
+  }
+  const long long big_tiles = (long long)((c.nx + 31) / 32) * ((c.ny + 15) / 16);
+  if (big_tiles < 2LL * n_sm) return launch_tb2_shape<16, 8>(io, c, s);
+  return launch_tb2_shape<32, 16>(io, c, s);
 }
 
 } // namespace hm

@@ -59,7 +59,8 @@ def _compare(got, ref, want, z0, exact):
             assert np.array_equal(g, w), "%s not bit-exact with the oracle: %s" % (n, errs)
 
 
-@pytest.mark.parametrize("shape", [(128, 128), (97, 131), (256, 64), (5, 300), (20, 40), (37, 260)])
+# small grids take 16 x 8 tiles; (333, 650) has enough 32 x 16 tiles for that shape, with ragged edges
+@pytest.mark.parametrize("shape", [(128, 128), (97, 131), (256, 64), (5, 300), (20, 40), (37, 260), (333, 650)])
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_two_step_tiles(gpu, shape, case):
     ny, nx = shape
