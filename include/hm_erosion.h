@@ -621,9 +621,10 @@ int hm_vpipes_set_launch(int tpb, int radius, int rows);
  * HM_VPIPES_STREAMING (all four passes in one kernel streaming down column
  * strips, shaped by hm_vpipes_set_launch), HM_VPIPES_TILED_TB2 (temporal
  * blocking: without the water-volume top-up, every pair of steps after the
- * first in one launch over 32 x 16 tiles that compute the pair's first step
- * on a 4-cell halo; with the top-up, as HM_VPIPES_TILED), or HM_VPIPES_AUTO
- * (-1: the tuned or built-in choice).  Results do not depend on it. */
+ * first in one launch over 32 x 16 tiles, 16 x 8 on small grids, that
+ * compute the pair's first step on a 4-cell halo; with the top-up, as
+ * HM_VPIPES_TILED), or HM_VPIPES_AUTO (-1: the tuned or built-in choice).
+ * Results do not depend on it. */
 #define HM_VPIPES_AUTO (-1)
 #define HM_VPIPES_TILED 0
 #define HM_VPIPES_STREAMING 1
