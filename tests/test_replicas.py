@@ -78,3 +78,14 @@ def test_reference_arm_other_ranks_exit_quietly():
                         "--steps", "1", "--warmup", "3"], capture_output=True, text=True, env=env, timeout=120)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+@pytest.mark.parametrize("form", ["tblock", "sweep"])
+def test_single_gpu_forms_other_ranks_exit_quietly(form):
+    """The forms that measure one GPU run on rank 0 of a torchrun launch;
+    the other ranks exit 0 before any device call."""
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--form", form, "--sizes", "128"],
+                       capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == ""
